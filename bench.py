@@ -1,0 +1,401 @@
+#!/usr/bin/env python
+"""Benchmark: synaptic events/s on the 1M-neuron / 100M-synapse Izhikevich +
+pair-STDP network (BF16 weights, dt 1 ms), one JSON line on rank 0.
+
+A bench "step" is 1000 simulation steps (1 s of simulated time) of that
+network, inputs resident in HBM (state 64 MB + synapses ~1.3 GB, larger than
+the 126 MB L2, so no flush is needed between steps). `value` is device-timed
+with CUDA events on the library's launching stream. `e2e` times complete jobs
+through the C ABI with pinned host buffers: upload of the network and
+initial state, 10,000 simulation steps (the configuration's 10 s), and the
+read-back of the full spike raster and final membrane state.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+N > 1 (torchrun): independent replicas of the network, one per GPU ("replicas
+only": a single network does not shard here); value = all ranks' events /
+max over ranks of the device time.
+`--impl reference` times the CPU restatement of the reference's engine loop
+(C++, FP64, per-synapse state, OpenMP over neurons as rayon does) on this
+host: rank 0 only, each step one simulation step of the same network.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "syn events/s @1M/100M"
+UNIT = "events/s"
+WORKLOAD = ("Izhikevich + pair STDP, 1,000,000 neurons (80% RS / 20% FS), in-degree 100 "
+            "(100M synapses, CSR, BF16 weights, FP32 accumulation), thalamic noise 5/2 N(0,1), "
+            "dt 1 ms; one step = 1000 simulation steps (1 s simulated)")
+
+
+def args_():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--neurons", type=int, default=1_000_000)
+    p.add_argument("--in-degree", type=int, default=100)
+    p.add_argument("--sim-steps", type=int, default=1000, help="simulation steps per bench step")
+    p.add_argument("--e2e-jobs", type=int, default=2)
+    p.add_argument("--cpu-seconds", type=float, default=20.0)
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    return 6650.0, "fallback 6.65 TB/s (no MEASURED_PEAKS.json)"
+
+
+def profile_traffic():
+    """DRAM bytes per launch of the neuron kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "k_neuron_izh_c2_ncu.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("traffic_bytes_per_launch_full_size:"):
+            try:
+                return float(line.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        self.f.flush()
+        rows = []
+        for line in open(self.f.name):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, x in enumerate(r) if x == "Active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows),
+                "sm_max_mhz": max(r[1] for r in rows), "reasons": reasons, "samples": len(rows)}
+
+
+def build_network(n, k, seed):
+    from neuralsim_b200 import configs
+    return configs.izh_c2(n=n, k=k, seed=seed)
+
+
+def step_bytes(n, spikes, events, in_plastic):
+    """Algorithmic HBM bytes of one simulation step:
+    64 N (v,u r/w; a,b,c,d; int64 accumulator read + zero; pre/post traces r/w)
+    + 16 S (row_ptr pair, CSC pointer pair) + 8 E_out (col, bf16 w, LTP write)
+    + 8 E_in,plastic (incoming index, bf16 w read + write)."""
+    return 64.0 * n + 16.0 * spikes + 8.0 * events + 8.0 * in_plastic
+
+
+def neuron_kernel_bytes(n, spikes):
+    """Algorithmic bytes of one neuron-kernel launch: 64 N plus per spike the
+    spike index 4, last-spike step r/w 16, pre-bump trace 4, row_ptr pair 16."""
+    return 64.0 * n + 40.0 * spikes
+
+
+def run_ours(a):
+    import torch
+    from neuralsim_b200 import SimulationEngine
+    from neuralsim_b200 import _abi as A
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local)
+
+    t0 = time.time()
+    net, cfg, drive, _ = build_network(a.neurons, a.in_degree, 44 + rank)
+    cfg.device = local
+    gen_s = time.time() - t0
+    in_deg_plastic = np.zeros(net.n, np.int64)
+    np.add.at(in_deg_plastic, net.col[net.plastic.astype(bool)], 1)
+
+    eng = SimulationEngine(net, cfg, drive)
+    stream = torch.cuda.ExternalStream(eng.stream(), device=local)
+    S = a.sim_steps
+    for _ in range(a.warmup):
+        eng.run(S)
+    c0 = eng.counters()
+    l0 = eng.launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(a.steps):
+            eng.run(S)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    c1 = eng.counters()
+    launches = eng.launch_count() - l0
+    events = c1[3] - c0[3]
+    spikes = c1[1] - c0[1]
+    sim_steps = c1[0] - c0[0]
+    clocks = clk.summary()
+
+    # per-kernel device time (eager steps with events around each kernel)
+    pc0 = eng.counters()
+    prof = eng.profile_steps(200)
+    pc1 = eng.counters()
+    prof_spikes = (pc1[1] - pc0[1]) / 200.0
+
+    # whole-step algorithmic bytes: plastic in-degree of the spikers is
+    # estimated from the mean (80 of 100 incoming synapses are plastic)
+    mean_in_plastic = float(in_deg_plastic.mean())
+    bytes_total = step_bytes(net.n, spikes, events, spikes * mean_in_plastic) if sim_steps else 0.0
+
+    if dist:
+        t = torch.tensor([ms, float(events)], dtype=torch.float64, device=f"cuda:{local}")
+        tm = t.clone()
+        dist.all_reduce(tm[0:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(tm[1:2], op=dist.ReduceOp.SUM)
+        ms_max, events_all = float(tm[0]), float(tm[1])
+    else:
+        ms_max, events_all = ms, float(events)
+
+    # e2e: complete jobs through the C ABI with pinned host buffers
+    e2e = None
+    if not a.no_e2e:
+        e2e = run_e2e(a, net, cfg, drive, local, dist)
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu:
+        cpu = run_cpu_baseline(net, cfg, drive, a.cpu_seconds)
+
+    if rank == 0:
+        peak, peak_src = peaks()
+        nk_ms, nk_launches = prof["neuron"]
+        nk_avg_s = nk_ms / nk_launches / 1e3
+        nk_bytes = neuron_kernel_bytes(net.n, prof_spikes)
+        achieved = nk_bytes / nk_avg_s / 1e9
+        total_prof_ms = sum(v[0] for v in prof.values())
+        traffic = profile_traffic()
+        value = events_all / (ms_max / 1e3)
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_max / a.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded generator, configuration shapes)",
+            "config": {
+                "workload": WORKLOAD, "neurons": net.n, "synapses": net.m,
+                "sim_steps_per_step": S, "weights": "bf16", "accumulation": "int64 fixed point",
+                "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                "l2": "inputs larger than L2 (no flush needed)",
+                "spikes_per_sim_step": spikes / max(sim_steps, 1),
+                "events_per_sim_step": events / max(sim_steps, 1),
+                "sim_time_per_wall_s": (sim_steps * cfg.dt_ms / 1e3) / (ms / 1e3),
+                "network_build_s": round(gen_s, 2),
+            },
+            "roofline": {
+                "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic,
+                "kernel": "k_neuron<IZHIKEVICH,RESET_EACH_STEP>",
+                "bytes_per_launch": nk_bytes, "avg_launch_us": nk_avg_s * 1e6,
+                "peak_source": peak_src,
+                "kernel_share": {k: v[0] / total_prof_ms for k, v in prof.items()},
+                "kernel_avg_us": {k: v[0] / v[1] * 1e3 for k, v in prof.items()},
+            },
+            "step_roofline": {
+                "algorithmic_bytes_per_sim_step": bytes_total / max(sim_steps, 1),
+                "achieved": bytes_total / (ms / 1e3) / 1e9, "unit": "GB/s",
+                "frac": bytes_total / (ms / 1e3) / 1e9 / peak,
+                "formula": "64N + 16S + 8E_out + 8E_in,plastic",
+            },
+            "clocks": clocks,
+            "gpu_launches": launches,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(out), flush=True)
+    eng.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_e2e(a, net, cfg, drive, local, dist):
+    """Whole jobs: pinned host network + state -> device, 10,000 steps,
+    raster + final v back to pinned host memory."""
+    import torch
+    from neuralsim_b200 import SimulationEngine
+    from neuralsim_b200.engine import Network
+    pin = lambda x: torch.from_numpy(np.ascontiguousarray(x)).pin_memory().numpy()
+    pnet = Network(net.model, pin(net.params), pin(net.row_ptr), pin(net.col), pin(net.w),
+                   syn_type=pin(net.syn_type), plastic=pin(net.plastic), v0=pin(net.v0),
+                   u0=pin(net.u0), inhibitory=pin(net.inhibitory))
+    job_steps = 10_000
+    cfg.spike_log_capacity = 200_000_000
+    cfg.spike_log_steps = job_steps
+    h2d = (pnet.params.nbytes + pnet.row_ptr.nbytes + pnet.col.nbytes + pnet.w.nbytes +
+           pnet.syn_type.nbytes + pnet.plastic.nbytes + pnet.v0.nbytes + pnet.u0.nbytes +
+           pnet.inhibitory.nbytes)
+    eng = SimulationEngine(pnet, cfg, drive)   # allocations done once
+    stream = torch.cuda.ExternalStream(eng.stream(), device=local)
+    times, events, d2h = [], [], []
+    for job in range(a.e2e_jobs + 1):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        eng._upload(pnet)
+        c0 = eng.counters()
+        eng.run(job_steps)
+        c1 = eng.counters()
+        idx, off = eng.read_raster(c0[0], job_steps)
+        st = eng.download_state(with_weights=False)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if job == 0:
+            continue  # warm-up job
+        times.append(e0.elapsed_time(e1))
+        events.append(c1[3] - c0[3])
+        d2h.append(idx.nbytes + off.nbytes + st["v"].nbytes)
+    eng.close()
+    ms = sum(times)
+    ev = float(sum(events))
+    if dist:
+        t = torch.tensor([ms, ev], dtype=torch.float64, device=f"cuda:{local}")
+        m_ = t[0:1].clone()
+        s_ = t[1:2].clone()
+        dist.all_reduce(m_, op=dist.ReduceOp.MAX)
+        dist.all_reduce(s_, op=dist.ReduceOp.SUM)
+        ms, ev = float(m_), float(s_)
+    return {"value": ev / (ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(statistics.mean(d2h)),
+            "step": "one job: upload network + initial state, 10,000 simulation steps, "
+                    "read back raster + final v", "jobs": len(times),
+            "ms_per_job": ms / max(len(times), 1)}
+
+
+def run_cpu_baseline(net, cfg, drive, seconds):
+    """The CPU restatement of engine.rs (FP64, per-synapse state) on this
+    host, on the same network, for a bounded number of simulation steps."""
+    from oracle.oracle import LiteralOracle
+    threads = os.cpu_count() or 1
+    lit = LiteralOracle(net, cfg, drive, threads=threads)
+    lit.step(1)  # warm-up
+    e0 = lit.events()
+    t0 = time.perf_counter()
+    steps = 0
+    while steps < 2 or (time.perf_counter() - t0 < seconds and steps < 100):
+        lit.step(1)
+        steps += 1
+    dt = time.perf_counter() - t0
+    ev = lit.events() - e0
+    lit.close()
+    return {"value": ev / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{steps} simulation steps of the same 1M/100M network after 1 warm-up step "
+                      f"({dt:.1f} s); C++ restatement of engine.rs, FP64, per-synapse state, "
+                      "OpenMP over the neuron update only (as rayon); not the Rust binary"}
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle.oracle import LiteralOracle
+    net, cfg, drive, _ = build_network(a.neurons, a.in_degree, 44)
+    threads = os.cpu_count() or 1
+    lit = LiteralOracle(net, cfg, drive, threads=threads)
+    for _ in range(a.warmup):
+        lit.step(1)
+    e0 = lit.events()
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        lit.step(1)
+    dt = time.perf_counter() - t0
+    ev = lit.events() - e0
+    value = ev / dt
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": dt * 1e3 / a.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator, configuration shapes)",
+        "config": {"workload": WORKLOAD.replace("one step = 1000 simulation steps (1 s simulated)",
+                                                "one step = 1 simulation step"),
+                   "neurons": net.n, "synapses": net.m, "sim_steps_per_step": 1},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{a.steps} simulation steps after {a.warmup} warm-up steps; "
+                                   "C++ restatement of engine.rs (the Rust crate does not build "
+                                   "here), FP64, per-synapse state, OpenMP over the neuron update"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    a = args_()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

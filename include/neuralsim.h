@@ -1,0 +1,255 @@
+/*
+ * neuralsim.h — C ABI of the B200 step backend for NeuralSim's per-timestep
+ * hot path (neuron-state update, CSR spike propagation, trace STDP).
+ *
+ * This is the drop-in seam for the reference crate's `GpuBackend`
+ * (src/simulation/gpu_backend.rs:47-1036), which `SimulationEngine::step`
+ * dispatches to at src/simulation/engine.rs:255-258 and which
+ * `SimulationEngine::init_gpu` builds at src/simulation/engine.rs:181-252.
+ *
+ * Conventions
+ *  - Every function returns an ns_status (0 = NS_OK) and never throws or
+ *    aborts across the ABI. ns_last_error() gives the message of the last
+ *    failing call on a handle (the reference's GpuError strings,
+ *    gpu_backend.rs:25-39, map onto NS_ERR_NO_DEVICE / NS_ERR_CUDA).
+ *  - The host owns every pointer it passes in; data is copied. The handle
+ *    owns all device memory and one CUDA stream.
+ *  - One handle is not thread-safe (the reference guards its engine with a
+ *    Mutex, src/simulation/scheduler.rs:23); distinct handles may be driven
+ *    from distinct threads.
+ *  - There is no CPU fallback: without a usable CUDA device ns_create fails
+ *    with NS_ERR_NO_DEVICE.
+ */
+#ifndef NEURALSIM_H
+#define NEURALSIM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t ns_status;
+#define NS_OK                  0
+#define NS_ERR_INVALID_ARG     1
+#define NS_ERR_NULL_HANDLE     2
+#define NS_ERR_CSR             3  /* row_ptr not monotone, col >= n, m mismatch */
+#define NS_ERR_OOM             4
+#define NS_ERR_CUDA            5
+#define NS_ERR_DEVICE_TIMEOUT  6  /* a bounded device-side wait gave up */
+#define NS_ERR_STATE           7  /* call out of order (e.g. step before upload) */
+#define NS_ERR_UNSUPPORTED     8
+#define NS_ERR_NONFINITE       9  /* NaN/Inf in uploaded state or parameters */
+#define NS_ERR_SPIKE_LOG_FULL 10  /* spike log capacity exceeded; stepping went on */
+#define NS_ERR_NO_DEVICE      11
+
+typedef struct ns_handle ns_handle;
+
+/* Neuron models: NeuronModelParams::{Lif, Izhikevich, HodgkinHuxley},
+ * src/neuron/mod.rs:71-94. One model per handle. Per-neuron parameter rows:
+ *   LIF (6): resting, threshold, reset, tau_m, refractory_period, input_resistance
+ *   IZH (4): a, b, c, d
+ *   HH  (7): g_na, g_k, g_l, e_na, e_k, e_l, c_m                               */
+enum ns_model { NS_MODEL_LIF = 0, NS_MODEL_IZHIKEVICH = 1, NS_MODEL_HH = 2 };
+
+/* How synaptic input reaches the neuron.
+ *  DIRECT_DECAY     reference current mode: I += w per event, I *= current_decay
+ *                   at the end of every step (engine.rs:456-471, :609-614).
+ *  DELTA_V          each delivered weight is a voltage kick added right after
+ *                   the model's integration step.
+ *  RESET_EACH_STEP  I = drive + sum of delivered weights, fresh every step.
+ *  CONDUCTANCE_REF  reference conductance mode: per-type conductances decay by
+ *                   exp(-dt/tau), events add w*gmax*mg(V) (|.| for GABA types),
+ *                   I += sum g*(E_rev - V), I never cleared (engine.rs:406-494).
+ *  CONDUCTANCE_FRESH per-target conductances as above, but the synaptic current
+ *                   is recomputed every step: I = sum g*(E_rev - V) + drive.   */
+enum ns_input_mode {
+  NS_INPUT_DIRECT_DECAY = 0,
+  NS_INPUT_DELTA_V = 1,
+  NS_INPUT_RESET_EACH_STEP = 2,
+  NS_INPUT_CONDUCTANCE_REF = 3,
+  NS_INPUT_CONDUCTANCE_FRESH = 4
+};
+
+/* HH integrator: EULER_REF is HodgkinHuxleyNeuron::step (forward-Euler gates,
+ * spike when V >= -55 then V = -70, src/neuron/hodgkin_huxley.rs:46-96);
+ * RUSH_LARSEN integrates the gates exactly for frozen V and reports a spike on
+ * an upward 0 mV crossing without reset.                                      */
+enum ns_hh_integrator { NS_HH_EULER_REF = 0, NS_HH_RUSH_LARSEN = 1 };
+
+enum ns_weight_format { NS_WEIGHT_F32 = 0, NS_WEIGHT_BF16 = 1 };
+
+/* SynapseType, src/synapse/mod.rs:22-28; constants src/synapse/types.rs:15-54. */
+enum ns_syn_type { NS_SYN_AMPA = 0, NS_SYN_GABA = 1, NS_SYN_GABA_B = 2, NS_SYN_NMDA = 3 };
+
+/* Drive (background input), replacing the host-side noise loop of
+ * engine.rs:273-287 with counter-based Philox4x32-10 streams keyed by
+ * (seed, step, neuron), so device and host produce the same numbers.
+ *  REF_UNIFORM   per neuron: with probability p, I += U*amplitude; then with
+ *                probability kick_chance, kick_min..kick_max random neurons
+ *                get I += U*kick_strength (the reference's drive shape).
+ *  POISSON_KICK  with probability p per neuron-step, add amplitude (a voltage
+ *                kick in DELTA_V mode, a current otherwise).
+ *  GAUSS         I += sigma*N(0,1), sigma_exc / sigma_inh by neuron type.
+ *  POISSON_CONDUCTANCE with probability p per neuron-step, add amplitude to
+ *                the neuron's AMPA conductance (conductance modes only).    */
+enum ns_drive_kind {
+  NS_DRIVE_NONE = 0,
+  NS_DRIVE_REF_UNIFORM = 1,
+  NS_DRIVE_POISSON_KICK = 2,
+  NS_DRIVE_GAUSS = 3,
+  NS_DRIVE_POISSON_CONDUCTANCE = 4
+};
+
+typedef struct ns_drive {
+  uint32_t kind;
+  float p;
+  float amplitude;
+  float sigma_exc;
+  float sigma_inh;
+  float kick_chance;
+  float kick_strength;
+  uint32_t kick_min;
+  uint32_t kick_max;
+} ns_drive;
+
+/* Mirrors SimulationConfig (src/config/mod.rs:61-68) + PlasticityConfig /
+ * StdpRule (src/synapse/mod.rs:122-157, src/synapse/plasticity.rs:8-28). */
+typedef struct ns_config {
+  uint32_t model;          /* ns_model */
+  uint32_t input_mode;     /* ns_input_mode */
+  uint32_t hh_integrator;  /* ns_hh_integrator */
+  uint32_t weight_format;  /* ns_weight_format */
+  double dt_ms;
+  uint32_t delay_steps;    /* >= 1; 1 = the reference (delivery at the next update) */
+  int32_t device;          /* CUDA ordinal */
+  uint64_t seed;
+  double current_decay;    /* DIRECT_DECAY factor, 0.92 in the reference */
+  /* pair STDP (StdpRule) */
+  int32_t stdp_enabled;
+  double tau_plus, tau_minus, a_plus, a_minus, w_min, w_max;
+  /* homeostatic scaling (engine.rs:569-606) */
+  int32_t homeostasis_enabled;
+  double homeostatic_target_rate, homeostatic_tau, contribution_tau;
+  /* spike log (the StepResult.spiking_neurons stream, engine.rs:35-41) */
+  uint64_t spike_log_capacity; /* indices held; 0 = no log */
+  uint32_t spike_log_steps;    /* steps held */
+  uint32_t graph_chunk;        /* steps per captured CUDA graph; 0 = 1000 */
+} ns_config;
+
+/* Fills cfg with the reference defaults: LIF, DIRECT_DECAY, dt 0.5 ms
+ * (engine.rs:96), decay 0.92, StdpRule::default, homeostasis 5 Hz / 5000 ms,
+ * contribution_tau 1000 ms, seed 42 (engine.rs:99). */
+void ns_config_default(ns_config* cfg);
+
+/* Neuron SoA (NeuronArray, src/neuron/mod.rs:126-163, in f32 as init_gpu
+ * uploads it, engine.rs:190-238). Unused arrays may be NULL on upload
+ * (defaults: v = model rest, u = 0, refractory = 0, current = 0, gates
+ * 0.05/0.6/0.32, traces 0, last spike never). On download every non-NULL
+ * pointer is filled. */
+typedef struct ns_neuron_soa {
+  uint64_t n;
+  float* v;
+  float* u;
+  int32_t* refractory;
+  float* current;
+  float* hh_m;
+  float* hh_h;
+  float* hh_n;
+  float* params;              /* n * params_per_neuron */
+  uint32_t params_per_neuron; /* 6 LIF, 4 IZH, 7 HH */
+  uint8_t* inhibitory;        /* NeuronType::Inhibitory flag (drive sigma) */
+  uint8_t* is_output;
+  float* pre_trace;           /* per-neuron STDP traces */
+  float* post_trace;
+  int64_t* last_spike_step;   /* -1 = never */
+  /* exact resume: synaptic input already propagated but not yet delivered,
+   * fixed point 2^-40, layout [type][delay slot][n] with 1 type in current
+   * modes and 4 (AMPA, GABA, GABA-B, NMDA) in conductance modes */
+  int64_t* pending_input;
+  float* conductance;         /* [4][n] per-target conductances */
+  double* firing_rate;        /* per-neuron rate estimate (homeostasis) */
+} ns_neuron_soa;
+
+typedef struct ns_step_stats {
+  uint64_t steps_done;        /* total steps since creation / state upload */
+  uint64_t spikes;            /* spikes during this call */
+  uint64_t output_spikes;
+  uint64_t events;            /* synaptic events (sum of out-degree of spikers) */
+  uint64_t last_step_spikes;
+  double sim_time_ms;         /* FP64 device clock (engine.rs:388-389) */
+} ns_step_stats;
+
+/* --- lifecycle: GpuBackend::new, gpu_backend.rs:98-124 ------------------ */
+ns_status ns_create(const ns_config* cfg, ns_handle** out);
+ns_status ns_destroy(ns_handle* h);
+const char* ns_last_error(const ns_handle* h);
+const char* ns_status_string(ns_status s);
+ns_status ns_device_count(int* count);
+
+/* --- uploads: GpuBackend::upload_initial_state / upload_csr,
+ *     gpu_backend.rs:640-688 (called from engine.rs:240-247) --------------- */
+ns_status ns_upload_neurons(ns_handle* h, const ns_neuron_soa* soa);
+/* CSR by source (Network::finalize, src/network/mod.rs:79-106). Synapse
+ * arrays MUST already be in CSR order. syn_type NULL = AMPA for all;
+ * plastic NULL = no plastic synapse. Validated: row_ptr[0]==0, monotone,
+ * row_ptr[n]==m, col<n, weights finite. */
+ns_status ns_upload_csr(ns_handle* h, uint64_t n, uint64_t m, const uint64_t* row_ptr,
+                        const uint32_t* col, const float* w, const uint8_t* syn_type,
+                        const uint8_t* plastic);
+/* Drive: the noise loop of engine.rs:273-287 (host RNG in the reference). */
+ns_status ns_set_drive(ns_handle* h, const ns_drive* d);
+
+/* --- stepping: SimulationEngine::step / simulate_ms, engine.rs:254-680,
+ *     :792-797; GpuBackend::step_neurons + step_spmv, gpu_backend.rs:852-981.
+ *     Runs n_steps on the device (CUDA-graph chunks) and blocks until done. */
+ns_status ns_step(ns_handle* h, uint32_t n_steps, ns_step_stats* out);
+
+/* Spike log: ascending neuron indices per step (StepResult.spiking_neurons).
+ * Copies steps [first_step, first_step+n_steps) of the log; offsets_out has
+ * n_steps+1 entries relative to the first copied index. */
+ns_status ns_read_spikes(ns_handle* h, uint64_t first_step, uint32_t n_steps, uint32_t* idx_out,
+                         uint64_t* offsets_out, uint64_t cap, uint64_t* n_written);
+ns_status ns_clear_spike_log(ns_handle* h);
+/* First step held in the log and number of steps held. */
+ns_status ns_spike_log_range(ns_handle* h, uint64_t* first_step, uint64_t* n_steps);
+
+/* --- state: checkpoint / resume (io/checkpoint.rs keeps the Network only;
+ *     here the device state round-trips exactly, step counter included) --- */
+ns_status ns_download_state(ns_handle* h, ns_neuron_soa* out, float* w_out);
+ns_status ns_upload_state(ns_handle* h, const ns_neuron_soa* in, const float* w_in,
+                          uint64_t step);
+/* Current global step index (the Philox counter and STDP clock). */
+ns_status ns_get_step(ns_handle* h, uint64_t* step);
+/* Per-neuron firing-rate estimate (engine.rs:637-642), FP64 on the device;
+ * maintained only when homeostasis is enabled. */
+ns_status ns_download_rates(ns_handle* h, double* rates_out);
+/* Weight mean / std over all synapses (engine.rs:658-669), on demand. */
+ns_status ns_weight_stats(ns_handle* h, double* mean, double* stddev);
+
+/* --- traversal trace: runs ONE step and records the CSR position of every
+ *     propagation event in traversal order (spikers ascending, each row in
+ *     CSR order). For parity tests of the CSR walk. */
+ns_status ns_step_traced(ns_handle* h, uint64_t* pos_out, uint64_t cap, uint64_t* n_events);
+
+/* Kernel launches issued by this handle since creation (own kernels only). */
+ns_status ns_launch_count(ns_handle* h, uint64_t* launches);
+
+/* Running totals since creation / state upload: out[0] steps, out[1]
+ * spikes, out[2] output spikes, out[3] synaptic events. */
+ns_status ns_counters(ns_handle* h, uint64_t out[4]);
+
+/* The CUDA stream (cudaStream_t) every kernel of this handle is launched on,
+ * so a caller can record its own CUDA events around ns_step. */
+ns_status ns_get_stream(ns_handle* h, void** stream);
+
+/* Runs n_steps eagerly with CUDA events around every kernel; adds the device
+ * time (ms) and the launch count of the neuron, propagation and homeostasis
+ * kernels to kernel_ms[3] / launches[3]. Same numerics as ns_step. */
+ns_status ns_profile_steps(ns_handle* h, uint32_t n_steps, double* kernel_ms, uint64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NEURALSIM_H */

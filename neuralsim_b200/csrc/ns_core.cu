@@ -1,0 +1,1135 @@
+// Host side of the C ABI declared in include/neuralsim.h: handle lifetime,
+// validated uploads, device-side CSR checks and incoming-index build, and the
+// CUDA-graph step loop. Replaces GpuBackend (src/simulation/gpu_backend.rs).
+#include <cuda_runtime.h>
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/neuralsim.h"
+#include "ns_kernels.cuh"
+
+using ns::NsDev;
+
+struct ns_handle {
+  ns_config cfg{};
+  ns_drive drive{};
+  int dev = 0;
+  int sms = 148;
+  cudaStream_t st = nullptr;
+  std::string err;
+  bool have_neurons = false, have_csr = false;
+  uint64_t n = 0, n_pad = 0, m = 0, m_pad = 0;
+  uint32_t ntiles = 0;
+  NsDev d{};
+  ns::Ctl* ctl = nullptr;
+  std::vector<void*> neuron_allocs, csr_allocs, log_allocs;
+  std::map<uint32_t, cudaGraphExec_t> graphs;
+  uint64_t launches = 0;
+  int prop_blocks = 0;
+  int homeo_blocks = 0;
+  int ntypes_acc = 1;
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+ns_status fail(ns_handle* h, ns_status s, const std::string& msg) {
+  if (h) h->err = msg; else g_err = msg;
+  return s;
+}
+
+#define CK(call)                                                                           \
+  do {                                                                                     \
+    cudaError_t e_ = (call);                                                               \
+    if (e_ != cudaSuccess)                                                                 \
+      return fail(h, e_ == cudaErrorMemoryAllocation ? NS_ERR_OOM : NS_ERR_CUDA,           \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                     \
+  } while (0)
+
+template <class T> ns_status dalloc(ns_handle* h, std::vector<void*>& bag, T** p, size_t count) {
+  void* q = nullptr;
+  size_t bytes = std::max<size_t>(count * sizeof(T), 16);
+  cudaError_t e = cudaMalloc(&q, bytes);
+  if (e != cudaSuccess) {
+    return fail(h, e == cudaErrorMemoryAllocation ? NS_ERR_OOM : NS_ERR_CUDA,
+                std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  }
+  e = cudaMemsetAsync(q, 0, bytes, h->st);
+  if (e != cudaSuccess) return fail(h, NS_ERR_CUDA, cudaGetErrorString(e));
+  bag.push_back(q);
+  *p = (T*)q;
+  return NS_OK;
+}
+
+void free_bag(std::vector<void*>& bag) {
+  for (void* p : bag) cudaFree(p);
+  bag.clear();
+}
+
+void drop_graphs(ns_handle* h) {
+  for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second);
+  h->graphs.clear();
+}
+
+uint64_t round_up(uint64_t x, uint64_t a) { return (x + a - 1) / a * a; }
+
+int params_for(uint32_t model) { return model == NS_MODEL_LIF ? 6 : (model == NS_MODEL_IZHIKEVICH ? 4 : 7); }
+
+uint32_t prob_threshold(double p) {
+  if (p <= 0) return 0;
+  double t = p * 4294967296.0;
+  if (t >= 4294967295.0) return 0xffffffffu;
+  return (uint32_t)t;
+}
+
+bool is_fin(double x) { return std::isfinite(x); }
+
+// ---- device kernels used by uploads ----
+__global__ void k_check_rows(const uint64_t* rp, uint64_t n, uint64_t m, unsigned int* bad) {
+  uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  if (rp[j] > rp[j + 1] || rp[j + 1] > m) atomicOr(bad, 1u);
+}
+
+__global__ void k_check_syn(const uint32_t* col, const float* w, const uint8_t* ty, uint64_t m,
+                            uint64_t n, unsigned int* bad) {
+  for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < m;
+       e += (uint64_t)gridDim.x * blockDim.x) {
+    if (col[e] >= n) atomicOr(bad, 2u);
+    float x = w[e];
+    if (!(fabsf(x) < 4194304.0f)) atomicOr(bad, 4u);  // finite and |w| < 2^22
+    if (ty && ty[e] > 3) atomicOr(bad, 8u);
+  }
+}
+
+// per-row classification of plastic flags and synapse types
+__global__ void k_row_flags(const uint64_t* rp, uint64_t n, const uint8_t* pl, const uint8_t* ty,
+                            uint8_t* row_pl, uint8_t* row_ty, unsigned int* mixed) {
+  uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  uint64_t b = rp[j], e = rp[j + 1];
+  uint8_t p0 = 0, t0 = 0;
+  bool pm = false, tm = false;
+  if (e > b) {
+    p0 = pl ? (pl[b] ? 1 : 0) : 0;
+    t0 = ty ? ty[b] : 0;
+    for (uint64_t q = b + 1; q < e; ++q) {
+      if (pl && ((pl[q] ? 1 : 0) != p0)) pm = true;
+      if (ty && ty[q] != t0) tm = true;
+    }
+  }
+  row_pl[j] = pm ? 2 : p0;
+  row_ty[j] = tm ? 255 : t0;
+  if (pm) atomicOr(mixed, 1u);
+  if (tm) atomicOr(mixed, 2u);
+}
+
+__global__ void k_to_bf16(const float* in, uint16_t* out, uint64_t m) {
+  for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < m;
+       e += (uint64_t)gridDim.x * blockDim.x)
+    out[e] = ns::f32_to_bf16_bits(in[e]);
+}
+
+__global__ void k_from_bf16(const uint16_t* in, float* out, uint64_t m) {
+  for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < m;
+       e += (uint64_t)gridDim.x * blockDim.x)
+    out[e] = ns::bf16_bits_to_f32(in[e]);
+}
+
+// keys (target) and values (CSR position) of the synapses to index
+__global__ void k_in_keys(const uint32_t* col, const uint8_t* pl, uint64_t m, uint32_t* keys,
+                          uint32_t* vals, unsigned long long* cnt, int only_plastic) {
+  for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < m;
+       e += (uint64_t)gridDim.x * blockDim.x) {
+    if (only_plastic && !(pl && pl[e])) continue;
+    unsigned long long q = atomicAdd(cnt, 1ull);
+    keys[q] = col[e];
+    vals[q] = (uint32_t)e;
+  }
+}
+
+__global__ void k_count_keys(const uint32_t* keys, uint64_t cnt, uint64_t* deg) {
+  for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < cnt;
+       q += (uint64_t)gridDim.x * blockDim.x)
+    atomicAdd((unsigned long long*)&deg[keys[q]], 1ull);
+}
+
+__global__ void k_in_list(const uint32_t* pos, uint64_t cnt, const uint64_t* rp, uint64_t n,
+                          uint2* out) {
+  for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < cnt;
+       q += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t p = pos[q];
+    uint64_t lo = 0, hi = n;  // largest j with rp[j] <= p
+    while (hi - lo > 1) {
+      uint64_t mid = (lo + hi) >> 1;
+      if (rp[mid] <= p) lo = mid; else hi = mid;
+    }
+    out[q] = make_uint2((uint32_t)lo, (uint32_t)p);
+  }
+}
+
+__global__ void k_weight_sum(const float* w32, const uint16_t* w16, uint64_t m, double mean,
+                             int pass, double* out) {
+  double acc = 0.0;
+  for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < m;
+       e += (uint64_t)gridDim.x * blockDim.x) {
+    double x = w16 ? (double)ns::bf16_bits_to_f32(w16[e]) : (double)w32[e];
+    acc += pass == 0 ? x : (x - mean) * (x - mean);
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(out, acc);
+}
+
+// Builds an incoming index sorted by (target, CSR position): deterministic.
+ns_status build_incoming(ns_handle* h, const uint8_t* d_pl, int only_plastic, uint64_t** out_ptr,
+                         uint32_t** out_pos, uint2** out_list) {
+  const uint64_t n = h->n, m = h->m;
+  uint32_t *keys = nullptr, *vals = nullptr, *keys2 = nullptr, *vals2 = nullptr;
+  unsigned long long* cnt_d = nullptr;
+  std::vector<void*> tmp;
+  ns_status s;
+  if ((s = dalloc(h, tmp, &keys, m)) || (s = dalloc(h, tmp, &vals, m)) ||
+      (s = dalloc(h, tmp, &keys2, m)) || (s = dalloc(h, tmp, &vals2, m)) ||
+      (s = dalloc(h, tmp, &cnt_d, 1))) {
+    free_bag(tmp);
+    return s;
+  }
+  const int grid = h->sms * 8;
+  k_in_keys<<<grid, 256, 0, h->st>>>(h->d.col, d_pl, m, keys, vals, cnt_d, only_plastic);
+  unsigned long long cnt = 0;
+  CK(cudaMemcpyAsync(&cnt, cnt_d, 8, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  uint64_t* ptr = nullptr;
+  if ((s = dalloc(h, h->csr_allocs, &ptr, n + 1))) { free_bag(tmp); return s; }
+  if (cnt > 0) {
+    // sort pairs by (target, position): first by position (already grouped
+    // arbitrarily), then a stable sort by target keeps position order
+    size_t tb = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tb, vals, vals2, keys, keys2, (int64_t)cnt, 0, 32, h->st);
+    void* tstore = nullptr;
+    CK(cudaMalloc(&tstore, tb));
+    tmp.push_back(tstore);
+    cub::DeviceRadixSort::SortPairs(tstore, tb, vals, vals2, keys, keys2, (int64_t)cnt, 0, 32, h->st);
+    // vals2 = sorted positions, keys2 = their targets
+    size_t tb2 = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tb2, keys2, keys, vals2, vals, (int64_t)cnt, 0, 32, h->st);
+    if (tb2 > tb) {
+      void* t2 = nullptr;
+      CK(cudaMalloc(&t2, tb2));
+      tmp.push_back(t2);
+      tstore = t2;
+      tb = tb2;
+    }
+    cub::DeviceRadixSort::SortPairs(tstore, tb, keys2, keys, vals2, vals, (int64_t)cnt, 0, 32, h->st);
+    // keys = targets sorted, vals = positions (ascending within a target)
+    uint64_t* deg = nullptr;
+    if ((s = dalloc(h, tmp, &deg, n + 1))) { free_bag(tmp); return s; }
+    k_count_keys<<<grid, 256, 0, h->st>>>(keys, cnt, deg + 1);
+    size_t tb3 = 0;
+    cub::DeviceScan::InclusiveSum(nullptr, tb3, deg, ptr, (int64_t)(n + 1), h->st);
+    void* t3 = nullptr;
+    CK(cudaMalloc(&t3, tb3));
+    tmp.push_back(t3);
+    cub::DeviceScan::InclusiveSum(t3, tb3, deg, ptr, (int64_t)(n + 1), h->st);
+    if (out_list) {
+      uint2* lst = nullptr;
+      if ((s = dalloc(h, h->csr_allocs, &lst, cnt))) { free_bag(tmp); return s; }
+      k_in_list<<<grid, 256, 0, h->st>>>(vals, cnt, h->d.row_ptr, n, lst);
+      *out_list = lst;
+    }
+    if (out_pos) {
+      uint32_t* pos = nullptr;
+      if ((s = dalloc(h, h->csr_allocs, &pos, cnt))) { free_bag(tmp); return s; }
+      CK(cudaMemcpyAsync(pos, vals, cnt * 4, cudaMemcpyDeviceToDevice, h->st));
+      *out_pos = pos;
+    }
+  } else {
+    if (out_list) *out_list = nullptr;
+    if (out_pos) *out_pos = nullptr;
+  }
+  CK(cudaStreamSynchronize(h->st));
+  free_bag(tmp);
+  *out_ptr = ptr;
+  CK(cudaGetLastError());
+  return NS_OK;
+}
+
+ns_status check_device_status(ns_handle* h) {
+  unsigned int stt = 0;
+  CK(cudaMemcpyAsync(&stt, &h->ctl->status, 4, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  if (stt & ns::kErrLookback)
+    return fail(h, NS_ERR_DEVICE_TIMEOUT, "spike compaction look-back wait gave up");
+  return NS_OK;
+}
+
+// tables exp(-q dt / tau), q = 0..K-1, for the spike-to-spike trace factor
+std::vector<float> trace_table(double tau, double dt) {
+  uint64_t K = (uint64_t)std::ceil(104.0 * tau / dt) + 2;
+  if (K > (1u << 22)) K = 1u << 22;
+  std::vector<float> t(K);
+  for (uint64_t q = 0; q < K; ++q) t[q] = (float)std::exp(-(double)q * dt / tau);
+  return t;
+}
+
+void fill_scalars(ns_handle* h) {
+  NsDev& d = h->d;
+  const ns_config& c = h->cfg;
+  d.n = h->n; d.n_pad = h->n_pad; d.m = h->m;
+  d.D = c.delay_steps; d.ntiles = h->ntiles;
+  d.dt = c.dt_ms; d.dt_f = (float)c.dt_ms;
+  d.decay_I = (float)c.current_decay;
+  d.stdp = c.stdp_enabled ? 1 : 0;
+  d.homeo = c.homeostasis_enabled ? 1 : 0;
+  d.hh_int = (int)c.hh_integrator;
+  d.a_plus = (float)c.a_plus; d.neg_a_minus = (float)(-c.a_minus);
+  d.w_min = (float)c.w_min; d.w_max = (float)c.w_max;
+  d.ep = (float)std::exp(-c.dt_ms / c.tau_plus);
+  d.em = (float)std::exp(-c.dt_ms / c.tau_minus);
+  d.seed = c.seed;
+  const double taus[4] = {2.0, 10.0, 150.0, 100.0};
+  for (int t = 0; t < 4; ++t) d.Gdec[t] = (float)std::exp(-c.dt_ms / taus[t]);
+  d.cd = (float)std::exp(-c.dt_ms / c.contribution_tau);
+  d.one_m_cd = 1.0f - d.cd;
+  d.h_target = c.homeostatic_target_rate;
+  d.h_tau = c.homeostatic_tau;
+  d.h_tau_f = (float)c.homeostatic_tau;
+  d.drive_kind = (int)h->drive.kind;
+  d.drive_p = h->drive.p;
+  d.drive_amp = h->drive.amplitude;
+  d.sig_e = h->drive.sigma_exc; d.sig_i = h->drive.sigma_inh;
+  d.kick_chance = h->drive.kick_chance; d.kick_strength = h->drive.kick_strength;
+  d.kick_min = h->drive.kick_min; d.kick_max = h->drive.kick_max;
+  d.p_thr = prob_threshold((double)h->drive.p);
+  d.ctl = h->ctl;
+}
+
+typedef void (*neuron_fn)(NsDev, uint32_t);
+typedef void (*prop_fn)(NsDev, uint32_t);
+
+neuron_fn pick_neuron(uint32_t model, uint32_t mode) {
+#define NSN(MO, MD) if (model == MO && mode == MD) return ns::k_neuron<MO, MD>;
+  NSN(0, 0) NSN(0, 1) NSN(0, 2) NSN(0, 3) NSN(0, 4)
+  NSN(1, 0) NSN(1, 1) NSN(1, 2) NSN(1, 3) NSN(1, 4)
+  NSN(2, 0) NSN(2, 1) NSN(2, 2) NSN(2, 3) NSN(2, 4)
+#undef NSN
+  return nullptr;
+}
+
+prop_fn pick_prop(uint32_t mode, uint32_t wf) {
+  bool cond = mode == NS_INPUT_CONDUCTANCE_REF || mode == NS_INPUT_CONDUCTANCE_FRESH;
+  bool bf = wf == NS_WEIGHT_BF16;
+  if (cond) return bf ? ns::k_propagate<true, true> : ns::k_propagate<true, false>;
+  return bf ? ns::k_propagate<false, true> : ns::k_propagate<false, false>;
+}
+
+// Enqueues one step (graph-node index j) on the handle's stream.
+void enqueue_step(ns_handle* h, uint32_t j) {
+  neuron_fn nf = pick_neuron(h->cfg.model, h->cfg.input_mode);
+  prop_fn pf = pick_prop(h->cfg.input_mode, h->cfg.weight_format);
+  nf<<<h->ntiles, ns::kThreads, 0, h->st>>>(h->d, j);
+  pf<<<h->prop_blocks, 256, 0, h->st>>>(h->d, j);
+  if (h->cfg.homeostasis_enabled) {
+    if (h->cfg.weight_format == NS_WEIGHT_BF16)
+      ns::k_homeostasis<true><<<h->homeo_blocks, 256, 0, h->st>>>(h->d, j);
+    else
+      ns::k_homeostasis<false><<<h->homeo_blocks, 256, 0, h->st>>>(h->d, j);
+  }
+}
+
+uint64_t launches_per_step(const ns_handle* h) { return 2u + (h->cfg.homeostasis_enabled ? 1u : 0u); }
+
+ns_status get_graph(ns_handle* h, uint32_t S, cudaGraphExec_t* out) {
+  auto it = h->graphs.find(S);
+  if (it != h->graphs.end()) { *out = it->second; return NS_OK; }
+  cudaGraph_t g;
+  CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+  for (uint32_t j = 0; j < S; ++j) enqueue_step(h, j);
+  ns::k_advance<<<1, 1, 0, h->st>>>(h->ctl, S);
+  CK(cudaStreamEndCapture(h->st, &g));
+  cudaGraphExec_t ex;
+  cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return fail(h, NS_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  h->graphs[S] = ex;
+  *out = ex;
+  return NS_OK;
+}
+
+ns_status ready(ns_handle* h) {
+  if (!h->have_neurons || !h->have_csr) return fail(h, NS_ERR_STATE, "upload neurons and CSR first");
+  if (h->n == 0) return fail(h, NS_ERR_STATE, "empty network");
+  return NS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void ns_config_default(ns_config* c) {
+  if (!c) return;
+  std::memset(c, 0, sizeof(*c));
+  c->model = NS_MODEL_LIF;
+  c->input_mode = NS_INPUT_DIRECT_DECAY;
+  c->hh_integrator = NS_HH_EULER_REF;
+  c->weight_format = NS_WEIGHT_F32;
+  c->dt_ms = 0.5;           // engine.rs:96
+  c->delay_steps = 1;
+  c->device = 0;
+  c->seed = 42;             // engine.rs:99
+  c->current_decay = 0.92;  // engine.rs:609-614
+  c->stdp_enabled = 1;      // PlasticityConfig::default, synapse/mod.rs:143-157
+  c->tau_plus = 20.0; c->tau_minus = 20.0;
+  c->a_plus = 0.01; c->a_minus = 0.012;
+  c->w_min = 0.0; c->w_max = 10.0;
+  c->homeostasis_enabled = 1;
+  c->homeostatic_target_rate = 5.0;
+  c->homeostatic_tau = 5000.0;
+  c->contribution_tau = 1000.0;
+  c->spike_log_capacity = 0;
+  c->spike_log_steps = 0;
+  c->graph_chunk = 1000;
+}
+
+const char* ns_status_string(ns_status s) {
+  switch (s) {
+    case NS_OK: return "ok";
+    case NS_ERR_INVALID_ARG: return "invalid argument";
+    case NS_ERR_NULL_HANDLE: return "null handle";
+    case NS_ERR_CSR: return "invalid CSR";
+    case NS_ERR_OOM: return "out of device memory";
+    case NS_ERR_CUDA: return "CUDA error";
+    case NS_ERR_DEVICE_TIMEOUT: return "device wait timed out";
+    case NS_ERR_STATE: return "call out of order";
+    case NS_ERR_UNSUPPORTED: return "unsupported configuration";
+    case NS_ERR_NONFINITE: return "non-finite value";
+    case NS_ERR_SPIKE_LOG_FULL: return "spike log full";
+    case NS_ERR_NO_DEVICE: return "no CUDA device";
+    default: return "unknown status";
+  }
+}
+
+const char* ns_last_error(const ns_handle* h) { return h ? h->err.c_str() : g_err.c_str(); }
+
+ns_status ns_device_count(int* count) {
+  if (!count) return NS_ERR_INVALID_ARG;
+  int c = 0;
+  if (cudaGetDeviceCount(&c) != cudaSuccess) c = 0;
+  *count = c;
+  return NS_OK;
+}
+
+ns_status ns_create(const ns_config* cfg, ns_handle** out) {
+  ns_handle* h = nullptr;
+  if (!cfg || !out) return fail(h, NS_ERR_INVALID_ARG, "null config or out pointer");
+  *out = nullptr;
+  const ns_config& c = *cfg;
+  if (c.model > 2 || c.input_mode > 4 || c.hh_integrator > 1 || c.weight_format > 1)
+    return fail(h, NS_ERR_INVALID_ARG, "unknown model / input mode / integrator / weight format");
+  if (!(c.dt_ms > 0) || !is_fin(c.dt_ms)) return fail(h, NS_ERR_INVALID_ARG, "dt_ms must be > 0");
+  if (c.delay_steps < 1 || c.delay_steps > 4096) return fail(h, NS_ERR_INVALID_ARG, "delay_steps in [1, 4096]");
+  if (c.input_mode == NS_INPUT_CONDUCTANCE_REF && c.delay_steps != 1)
+    return fail(h, NS_ERR_UNSUPPORTED, "reference conductance mode delivers in the same step (delay 1)");
+  if (c.stdp_enabled && (!(c.tau_plus > 0) || !(c.tau_minus > 0) || !is_fin(c.a_plus) ||
+                         !is_fin(c.a_minus) || !(c.w_min <= c.w_max)))
+    return fail(h, NS_ERR_INVALID_ARG, "bad STDP parameters");
+  if (c.homeostasis_enabled && (!(c.homeostatic_tau > 0) || !(c.contribution_tau > 0)))
+    return fail(h, NS_ERR_INVALID_ARG, "bad homeostasis parameters");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(h, NS_ERR_NO_DEVICE, "no CUDA device is visible");
+  if (c.device < 0 || c.device >= ndev) return fail(h, NS_ERR_INVALID_ARG, "device ordinal out of range");
+  h = new ns_handle();
+  h->cfg = c;
+  if (h->cfg.graph_chunk == 0) h->cfg.graph_chunk = 1000;
+  h->dev = c.device;
+  cudaError_t e = cudaSetDevice(h->dev);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, h->dev);
+  if (e != cudaSuccess) {
+    g_err = std::string("device init: ") + cudaGetErrorString(e);
+    delete h;
+    return NS_ERR_NO_DEVICE;
+  }
+  h->prop_blocks = h->sms * 8;
+  h->homeo_blocks = h->sms * 8;
+  e = cudaMalloc(&h->ctl, sizeof(ns::Ctl));
+  if (e == cudaSuccess) e = cudaMemset(h->ctl, 0, sizeof(ns::Ctl));
+  if (e != cudaSuccess) {
+    g_err = std::string("control block: ") + cudaGetErrorString(e);
+    if (h->ctl) cudaFree(h->ctl);
+    cudaStreamDestroy(h->st);
+    delete h;
+    return NS_ERR_OOM;
+  }
+  std::memset(&h->drive, 0, sizeof(h->drive));
+  *out = h;
+  return NS_OK;
+}
+
+ns_status ns_destroy(ns_handle* h) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  cudaSetDevice(h->dev);
+  if (h->st) cudaStreamSynchronize(h->st);
+  drop_graphs(h);
+  free_bag(h->neuron_allocs);
+  free_bag(h->csr_allocs);
+  free_bag(h->log_allocs);
+  if (h->ctl) cudaFree(h->ctl);
+  if (h->st) cudaStreamDestroy(h->st);
+  delete h;
+  return NS_OK;
+}
+
+ns_status ns_set_drive(ns_handle* h, const ns_drive* dr) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  if (!dr) return fail(h, NS_ERR_INVALID_ARG, "null drive");
+  if (dr->kind > 4) return fail(h, NS_ERR_INVALID_ARG, "unknown drive kind");
+  if (!is_fin(dr->p) || !is_fin(dr->amplitude) || !is_fin(dr->sigma_exc) || !is_fin(dr->sigma_inh) ||
+      !is_fin(dr->kick_chance) || !is_fin(dr->kick_strength))
+    return fail(h, NS_ERR_NONFINITE, "non-finite drive parameter");
+  if (dr->kind == NS_DRIVE_REF_UNIFORM && (dr->kick_min > dr->kick_max || dr->kick_max > 32))
+    return fail(h, NS_ERR_INVALID_ARG, "kick_min <= kick_max <= 32 required");
+  if (dr->kind == NS_DRIVE_POISSON_CONDUCTANCE && h->cfg.input_mode != NS_INPUT_CONDUCTANCE_FRESH)
+    return fail(h, NS_ERR_UNSUPPORTED, "conductance drive needs CONDUCTANCE_FRESH input");
+  if (h->have_neurons) CK(cudaStreamSynchronize(h->st));
+  h->drive = *dr;
+  drop_graphs(h);
+  return NS_OK;
+}
+
+static ns_status alloc_dynamic(ns_handle* h);
+
+ns_status ns_upload_neurons(ns_handle* h, const ns_neuron_soa* s) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  if (!s || !s->params) return fail(h, NS_ERR_INVALID_ARG, "null SoA or params");
+  const int ppn = params_for(h->cfg.model);
+  if ((int)s->params_per_neuron != ppn)
+    return fail(h, NS_ERR_INVALID_ARG, "params_per_neuron does not match the model");
+  if (s->n == 0 || s->n > 0xFFFFFFF0ull) return fail(h, NS_ERR_INVALID_ARG, "n out of range");
+  if (h->have_csr && s->n != h->n) return fail(h, NS_ERR_INVALID_ARG, "n differs from the CSR");
+  CK(cudaSetDevice(h->dev));
+  CK(cudaStreamSynchronize(h->st));
+  drop_graphs(h);
+  free_bag(h->neuron_allocs);
+  const uint64_t n = s->n;
+  h->n = n;
+  h->ntiles = (uint32_t)((n + ns::kTile - 1) / ns::kTile);
+  h->n_pad = (uint64_t)h->ntiles * ns::kTile;
+  const uint64_t np = h->n_pad;
+  const uint32_t model = h->cfg.model;
+  // host staging (padded)
+  for (uint64_t q = 0; q < n * (uint64_t)ppn; ++q)
+    if (!is_fin(s->params[q])) return fail(h, NS_ERR_NONFINITE, "non-finite neuron parameter");
+  const int npar = model == NS_MODEL_LIF ? 5 : ppn;
+  std::vector<std::vector<float>> par(npar, std::vector<float>(np, 0.0f));
+  std::vector<int32_t> rsteps(np, 0);
+  std::vector<float> v(np), u(np, 0.0f), I(np, 0.0f), gm(np, 0.05f), gh(np, 0.6f), gn(np, 0.32f);
+  for (uint64_t i = 0; i < n; ++i) {
+    const float* p = s->params + i * ppn;
+    if (model == NS_MODEL_LIF) {
+      par[0][i] = p[0]; par[1][i] = p[1]; par[2][i] = p[2]; par[3][i] = p[3]; par[4][i] = p[5];
+      rsteps[i] = (int32_t)std::round((double)p[4] / h->cfg.dt_ms);  // lif.rs:50
+      if (!(p[3] != 0.0f)) return fail(h, NS_ERR_INVALID_ARG, "tau_m must be nonzero");
+    } else {
+      for (int q = 0; q < ppn; ++q) par[q][i] = p[q];
+      if (model == NS_MODEL_HH && !(p[6] != 0.0f)) return fail(h, NS_ERR_INVALID_ARG, "c_m must be nonzero");
+    }
+    float rest = model == NS_MODEL_LIF ? p[0] : (model == NS_MODEL_IZHIKEVICH ? p[2] : p[5]);
+    v[i] = s->v ? s->v[i] : rest;
+    if (s->u) u[i] = s->u[i];
+    if (s->current) I[i] = s->current[i];
+    if (s->hh_m) gm[i] = s->hh_m[i];
+    if (s->hh_h) gh[i] = s->hh_h[i];
+    if (s->hh_n) gn[i] = s->hh_n[i];
+    if (!is_fin(v[i]) || !is_fin(u[i]) || !is_fin(I[i]) || !is_fin(gm[i]) || !is_fin(gh[i]) || !is_fin(gn[i]))
+      return fail(h, NS_ERR_NONFINITE, "non-finite initial state");
+  }
+  // padded neurons stay quiet: LIF with tau 1, rest 0, huge threshold
+  for (uint64_t i = n; i < np; ++i) {
+    v[i] = 0.0f;
+    if (model == NS_MODEL_LIF) { par[1][i] = 1e30f; par[3][i] = 1.0f; }
+    if (model == NS_MODEL_HH) { par[6][i] = 1.0f; v[i] = -65.0f; }
+  }
+  std::vector<int32_t> refr(np, 0);
+  if (s->refractory) for (uint64_t i = 0; i < n; ++i) refr[i] = s->refractory[i];
+  std::vector<uint8_t> inh(np, 0), outp(np, 0);
+  if (s->inhibitory) for (uint64_t i = 0; i < n; ++i) inh[i] = s->inhibitory[i] ? 1 : 0;
+  if (s->is_output) for (uint64_t i = 0; i < n; ++i) outp[i] = s->is_output[i] ? 1 : 0;
+  std::vector<float> pre(np, 0.0f), post(np, 0.0f);
+  if (s->pre_trace) for (uint64_t i = 0; i < n; ++i) pre[i] = s->pre_trace[i];
+  if (s->post_trace) for (uint64_t i = 0; i < n; ++i) post[i] = s->post_trace[i];
+  std::vector<long long> last(np, -1);
+  if (s->last_spike_step) for (uint64_t i = 0; i < n; ++i) last[i] = s->last_spike_step[i];
+
+  NsDev& d = h->d;
+  ns_status st;
+  auto& B = h->neuron_allocs;
+#define DA(ptr, cnt) if ((st = dalloc(h, B, &(ptr), (cnt)))) return st;
+  DA(d.v, np) DA(d.u, np) DA(d.I, np) DA(d.gm, np) DA(d.gh, np) DA(d.gn, np)
+  DA(d.refr, np) DA(d.refr_steps, np) DA(d.inh, np) DA(d.outp, np)
+  DA(d.pre, np) DA(d.post, np) DA(d.qdec, np) DA(d.last, np) DA(d.rate, np)
+  for (int q = 0; q < 7; ++q) d.par[q] = nullptr;
+  for (int q = 0; q < npar; ++q) DA(d.par[q], np)
+  for (int t = 0; t < 4; ++t) DA(d.G[t], np)
+  DA(d.bitmap, np / 32 + 2) DA(d.spk, np) DA(d.flags, h->ntiles)
+#undef DA
+  auto up = [&](void* dst, const void* src, size_t bytes) {
+    return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->st);
+  };
+  CK(up(d.v, v.data(), np * 4)); CK(up(d.u, u.data(), np * 4)); CK(up(d.I, I.data(), np * 4));
+  CK(up(d.gm, gm.data(), np * 4)); CK(up(d.gh, gh.data(), np * 4)); CK(up(d.gn, gn.data(), np * 4));
+  CK(up(d.refr, refr.data(), np * 4)); CK(up(d.refr_steps, rsteps.data(), np * 4));
+  CK(up(d.inh, inh.data(), np)); CK(up(d.outp, outp.data(), np));
+  CK(up(d.pre, pre.data(), np * 4)); CK(up(d.post, post.data(), np * 4));
+  CK(up(d.last, last.data(), np * 8));
+  for (int q = 0; q < npar; ++q) CK(up(d.par[q], par[q].data(), np * 4));
+  if (s->conductance) {
+    std::vector<float> g(np, 0.0f);
+    for (int t = 0; t < 4; ++t) {
+      for (uint64_t i = 0; i < n; ++i) g[i] = s->conductance[(uint64_t)t * n + i];
+      CK(up(d.G[t], g.data(), np * 4));
+    }
+  }
+  if (s->firing_rate) {
+    std::vector<double> r(np, 0.0);
+    for (uint64_t i = 0; i < n; ++i) r[i] = s->firing_rate[i];
+    CK(up(d.rate, r.data(), np * 8));
+  }
+  CK(cudaStreamSynchronize(h->st));
+  h->have_neurons = true;
+  if (h->have_csr) {
+    ns_status r = alloc_dynamic(h);
+    if (r) return r;
+  }
+  return NS_OK;
+}
+
+// accumulators, contribution, tables, log: need both n and m
+static ns_status alloc_dynamic(ns_handle* h) {
+  free_bag(h->log_allocs);
+  NsDev& d = h->d;
+  const ns_config& c = h->cfg;
+  const bool cond = c.input_mode == NS_INPUT_CONDUCTANCE_REF || c.input_mode == NS_INPUT_CONDUCTANCE_FRESH;
+  h->ntypes_acc = cond ? 4 : 1;
+  ns_status st;
+  auto& B = h->log_allocs;
+  if ((st = dalloc(h, B, &d.acc, (uint64_t)h->ntypes_acc * c.delay_steps * h->n_pad))) return st;
+  d.contrib = nullptr;
+  if (c.homeostasis_enabled && (st = dalloc(h, B, &d.contrib, std::max<uint64_t>(h->m, 1)))) return st;
+  std::vector<float> tp, tm;
+  if (c.stdp_enabled) { tp = trace_table(c.tau_plus, c.dt_ms); tm = trace_table(c.tau_minus, c.dt_ms); }
+  else { tp.assign(1, 0.0f); tm.assign(1, 0.0f); }
+  float *ep = nullptr, *em = nullptr;
+  if ((st = dalloc(h, B, &ep, tp.size())) || (st = dalloc(h, B, &em, tm.size()))) return st;
+  CK(cudaMemcpyAsync(ep, tp.data(), tp.size() * 4, cudaMemcpyHostToDevice, h->st));
+  CK(cudaMemcpyAsync(em, tm.data(), tm.size() * 4, cudaMemcpyHostToDevice, h->st));
+  d.Ep = ep; d.Em = em;
+  d.Kp = (uint32_t)tp.size(); d.Km = (uint32_t)tm.size();
+  d.log_idx = nullptr; d.log_off = nullptr;
+  d.log_cap = c.spike_log_capacity;
+  d.log_steps_cap = c.spike_log_steps;
+  if (c.spike_log_capacity > 0 && c.spike_log_steps > 0) {
+    if ((st = dalloc(h, B, &d.log_idx, c.spike_log_capacity))) return st;
+    if ((st = dalloc(h, B, &d.log_off, (uint64_t)c.spike_log_steps + 1))) return st;
+  }
+  d.trace_pos = nullptr; d.trace_off = nullptr; d.trace_cap = 0;
+  // reset the control block: counters, log, tickets
+  CK(cudaMemsetAsync(h->ctl, 0, sizeof(ns::Ctl), h->st));
+  CK(cudaMemsetAsync(d.flags, 0, (size_t)h->ntiles * 8, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  return NS_OK;
+}
+
+ns_status ns_upload_csr(ns_handle* h, uint64_t n, uint64_t m, const uint64_t* row_ptr,
+                        const uint32_t* col, const float* w, const uint8_t* syn_type,
+                        const uint8_t* plastic) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  if (!row_ptr || (m > 0 && (!col || !w))) return fail(h, NS_ERR_INVALID_ARG, "null CSR array");
+  if (n == 0) return fail(h, NS_ERR_INVALID_ARG, "n must be > 0");
+  if (h->have_neurons && n != h->n) return fail(h, NS_ERR_INVALID_ARG, "n differs from the neuron upload");
+  if (m >= 0xFFFFFFFFull) return fail(h, NS_ERR_UNSUPPORTED, "m must be < 2^32");
+  if (row_ptr[0] != 0 || row_ptr[n] != m) return fail(h, NS_ERR_CSR, "row_ptr[0] must be 0 and row_ptr[n] == m");
+  CK(cudaSetDevice(h->dev));
+  CK(cudaStreamSynchronize(h->st));
+  drop_graphs(h);
+  free_bag(h->csr_allocs);
+  h->have_csr = false;
+  NsDev& d = h->d;
+  h->m = m;
+  h->m_pad = round_up(std::max<uint64_t>(m, 4), 4) + 4;
+  if (!h->have_neurons) {
+    h->n = n;
+    h->ntiles = (uint32_t)((n + ns::kTile - 1) / ns::kTile);
+    h->n_pad = (uint64_t)h->ntiles * ns::kTile;
+  }
+  ns_status st;
+  auto& B = h->csr_allocs;
+  uint64_t* rp = nullptr;
+  uint32_t* cl = nullptr;
+  if ((st = dalloc(h, B, &rp, n + 1)) || (st = dalloc(h, B, &cl, h->m_pad))) return st;
+  CK(cudaMemcpyAsync(rp, row_ptr, (n + 1) * 8, cudaMemcpyHostToDevice, h->st));
+  if (m) CK(cudaMemcpyAsync(cl, col, m * 4, cudaMemcpyHostToDevice, h->st));
+  d.row_ptr = rp; d.col = cl;
+  // temporaries: f32 weights, types, plastic flags
+  std::vector<void*> tmp;
+  float* wt = nullptr;
+  uint8_t *ty = nullptr, *pl = nullptr;
+  unsigned int* bad = nullptr;
+  if ((st = dalloc(h, tmp, &wt, h->m_pad)) || (st = dalloc(h, tmp, &bad, 2))) { free_bag(tmp); return st; }
+  if (m) CK(cudaMemcpyAsync(wt, w, m * 4, cudaMemcpyHostToDevice, h->st));
+  if (syn_type) {
+    if ((st = dalloc(h, tmp, &ty, h->m_pad))) { free_bag(tmp); return st; }
+    if (m) CK(cudaMemcpyAsync(ty, syn_type, m, cudaMemcpyHostToDevice, h->st));
+  }
+  if (plastic) {
+    if ((st = dalloc(h, tmp, &pl, h->m_pad))) { free_bag(tmp); return st; }
+    if (m) CK(cudaMemcpyAsync(pl, plastic, m, cudaMemcpyHostToDevice, h->st));
+  }
+  const int grid = h->sms * 8;
+  k_check_rows<<<(unsigned)((n + 255) / 256), 256, 0, h->st>>>(rp, n, m, bad);
+  if (m) k_check_syn<<<grid, 256, 0, h->st>>>(cl, wt, ty, m, n, bad);
+  unsigned int badh = 0;
+  CK(cudaMemcpyAsync(&badh, bad, 4, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  CK(cudaGetLastError());
+  if (badh) {
+    free_bag(tmp);
+    free_bag(h->csr_allocs);
+    if (badh & 1u) return fail(h, NS_ERR_CSR, "row_ptr is not monotone or exceeds m");
+    if (badh & 2u) return fail(h, NS_ERR_CSR, "column index >= n");
+    if (badh & 4u) return fail(h, NS_ERR_NONFINITE, "weight is not finite or |w| >= 2^22");
+    return fail(h, NS_ERR_CSR, "synapse type > 3");
+  }
+  // weights in storage format
+  d.w32 = nullptr; d.w16 = nullptr;
+  if (h->cfg.weight_format == NS_WEIGHT_BF16) {
+    uint16_t* w16 = nullptr;
+    if ((st = dalloc(h, B, &w16, h->m_pad))) { free_bag(tmp); return st; }
+    if (m) k_to_bf16<<<grid, 256, 0, h->st>>>(wt, w16, m);
+    d.w16 = w16;
+  } else {
+    float* w32 = nullptr;
+    if ((st = dalloc(h, B, &w32, h->m_pad))) { free_bag(tmp); return st; }
+    if (m) CK(cudaMemcpyAsync(w32, wt, m * 4, cudaMemcpyDeviceToDevice, h->st));
+    d.w32 = w32;
+  }
+  // row classification; per-synapse arrays kept only when a row mixes values
+  uint8_t *rpl = nullptr, *rty = nullptr;
+  if ((st = dalloc(h, B, &rpl, n)) || (st = dalloc(h, B, &rty, n))) { free_bag(tmp); return st; }
+  k_row_flags<<<(unsigned)((n + 255) / 256), 256, 0, h->st>>>(rp, n, pl, ty, rpl, rty, bad + 1);
+  unsigned int mixed = 0;
+  CK(cudaMemcpyAsync(&mixed, bad + 1, 4, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  d.row_plastic = rpl; d.row_type = rty;
+  d.plastic = nullptr; d.type = nullptr;
+  if ((mixed & 1u) && pl) {
+    uint8_t* keep = nullptr;
+    if ((st = dalloc(h, B, &keep, h->m_pad))) { free_bag(tmp); return st; }
+    CK(cudaMemcpyAsync(keep, pl, m, cudaMemcpyDeviceToDevice, h->st));
+    d.plastic = keep;
+  }
+  if ((mixed & 2u) && ty) {
+    uint8_t* keep = nullptr;
+    if ((st = dalloc(h, B, &keep, h->m_pad))) { free_bag(tmp); return st; }
+    CK(cudaMemcpyAsync(keep, ty, m, cudaMemcpyDeviceToDevice, h->st));
+    d.type = keep;
+  }
+  // incoming indices: plastic (LTD) and all (homeostasis)
+  d.in_ptr = nullptr; d.in_list = nullptr; d.all_in_ptr = nullptr; d.all_in_pos = nullptr;
+  if (h->cfg.stdp_enabled) {
+    uint64_t* ip = nullptr;
+    uint2* il = nullptr;
+    if ((st = build_incoming(h, pl, 1, &ip, nullptr, &il))) { free_bag(tmp); return st; }
+    d.in_ptr = ip; d.in_list = il;
+  }
+  if (h->cfg.homeostasis_enabled) {
+    uint64_t* ap = nullptr;
+    uint32_t* apos = nullptr;
+    if ((st = build_incoming(h, pl, 0, &ap, &apos, nullptr))) { free_bag(tmp); return st; }
+    d.all_in_ptr = ap; d.all_in_pos = apos;
+  }
+  CK(cudaStreamSynchronize(h->st));
+  free_bag(tmp);
+  CK(cudaGetLastError());
+  h->have_csr = true;
+  if (h->have_neurons) return alloc_dynamic(h);
+  return NS_OK;
+}
+
+ns_status ns_step(ns_handle* h, uint32_t n_steps, ns_step_stats* out) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  ns_status r = ready(h);
+  if (r) return r;
+  CK(cudaSetDevice(h->dev));
+  fill_scalars(h);
+  ns::Ctl before{};
+  CK(cudaMemcpyAsync(&before, h->ctl, sizeof(before), cudaMemcpyDeviceToHost, h->st));
+  const uint32_t S = h->cfg.graph_chunk;
+  uint32_t left = n_steps;
+  if (left >= S) {
+    cudaGraphExec_t ex;
+    if ((r = get_graph(h, S, &ex))) return r;
+    while (left >= S) {
+      CK(cudaGraphLaunch(ex, h->st));
+      h->launches += (uint64_t)S * launches_per_step(h) + 1;
+      left -= S;
+    }
+  }
+  if (left > 0) {
+    for (uint32_t j = 0; j < left; ++j) enqueue_step(h, j);
+    ns::k_advance<<<1, 1, 0, h->st>>>(h->ctl, left);
+    h->launches += (uint64_t)left * launches_per_step(h) + 1;
+    CK(cudaGetLastError());
+  }
+  ns::Ctl after{};
+  CK(cudaMemcpyAsync(&after, h->ctl, sizeof(after), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  if (out) {
+    out->steps_done = after.step_base;
+    out->spikes = after.spikes_total - before.spikes_total;
+    out->output_spikes = after.out_total - before.out_total;
+    out->events = after.events_total - before.events_total;
+    out->last_step_spikes = n_steps ? after.step_spikes[(after.step_base - 1) & 3] : 0;
+    out->sim_time_ms = after.sim_time;
+  }
+  if (after.status & ns::kErrLookback)
+    return fail(h, NS_ERR_DEVICE_TIMEOUT, "spike compaction look-back wait gave up");
+  if ((after.status & ns::kErrLogFull) && !(before.status & ns::kErrLogFull))
+    return fail(h, NS_ERR_SPIKE_LOG_FULL, "spike log capacity exceeded; later steps not logged");
+  return NS_OK;
+}
+
+ns_status ns_step_traced(ns_handle* h, uint64_t* pos_out, uint64_t cap, uint64_t* n_events) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  ns_status r = ready(h);
+  if (r) return r;
+  if (!n_events || (cap && !pos_out)) return fail(h, NS_ERR_INVALID_ARG, "null output");
+  CK(cudaSetDevice(h->dev));
+  fill_scalars(h);
+  std::vector<void*> tmp;
+  unsigned long long *off = nullptr, *pos = nullptr;
+  ns_status st;
+  if ((st = dalloc(h, tmp, &off, h->n_pad + 1)) || (st = dalloc(h, tmp, &pos, std::max<uint64_t>(cap, 1)))) {
+    free_bag(tmp);
+    return st;
+  }
+  NsDev d = h->d;
+  neuron_fn nf = pick_neuron(h->cfg.model, h->cfg.input_mode);
+  prop_fn pf = pick_prop(h->cfg.input_mode, h->cfg.weight_format);
+  nf<<<h->ntiles, ns::kThreads, 0, h->st>>>(d, 0);
+  ns::k_trace_offsets<<<1, 32, 0, h->st>>>(d, off);
+  d.trace_pos = pos; d.trace_off = off; d.trace_cap = cap;
+  pf<<<h->prop_blocks, 256, 0, h->st>>>(d, 0);
+  if (h->cfg.homeostasis_enabled) {
+    if (h->cfg.weight_format == NS_WEIGHT_BF16) ns::k_homeostasis<true><<<h->homeo_blocks, 256, 0, h->st>>>(d, 0);
+    else ns::k_homeostasis<false><<<h->homeo_blocks, 256, 0, h->st>>>(d, 0);
+  }
+  ns::k_advance<<<1, 1, 0, h->st>>>(h->ctl, 1);
+  h->launches += launches_per_step(h) + 2;
+  CK(cudaGetLastError());
+  ns::Ctl after{};
+  CK(cudaMemcpyAsync(&after, h->ctl, sizeof(after), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  const uint32_t cnt = (uint32_t)after.step_spikes[(after.step_base - 1) & 3];
+  unsigned long long total = 0;
+  CK(cudaMemcpyAsync(&total, off + cnt, 8, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  *n_events = total;
+  if (cap) CK(cudaMemcpy(pos_out, pos, std::min<uint64_t>(cap, total) * 8, cudaMemcpyDeviceToHost));
+  free_bag(tmp);
+  return check_device_status(h);
+}
+
+ns_status ns_read_spikes(ns_handle* h, uint64_t first_step, uint32_t n_steps, uint32_t* idx_out,
+                         uint64_t* offsets_out, uint64_t cap, uint64_t* n_written) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  if (!offsets_out || !n_written) return fail(h, NS_ERR_INVALID_ARG, "null output");
+  if (!h->d.log_idx) return fail(h, NS_ERR_STATE, "spike log disabled (spike_log_capacity = 0)");
+  CK(cudaSetDevice(h->dev));
+  ns::Ctl c{};
+  CK(cudaMemcpyAsync(&c, h->ctl, sizeof(c), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  if (first_step < c.log_first || first_step + n_steps > c.log_first + c.log_steps)
+    return fail(h, NS_ERR_INVALID_ARG, "requested steps are not in the log");
+  const uint64_t s0 = first_step - c.log_first;
+  std::vector<unsigned long long> off(n_steps + 1);
+  CK(cudaMemcpy(off.data(), h->d.log_off + s0, (n_steps + 1) * 8, cudaMemcpyDeviceToHost));
+  const uint64_t total = off[n_steps] - off[0];
+  for (uint32_t q = 0; q <= n_steps; ++q) offsets_out[q] = off[q] - off[0];
+  *n_written = total;
+  if (total > cap) return fail(h, NS_ERR_INVALID_ARG, "idx_out capacity too small");
+  if (total) {
+    if (!idx_out) return fail(h, NS_ERR_INVALID_ARG, "null idx_out");
+    CK(cudaMemcpy(idx_out, h->d.log_idx + off[0], total * 4, cudaMemcpyDeviceToHost));
+  }
+  return NS_OK;
+}
+
+ns_status ns_clear_spike_log(ns_handle* h) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  CK(cudaSetDevice(h->dev));
+  CK(cudaStreamSynchronize(h->st));
+  ns::Ctl c{};
+  CK(cudaMemcpy(&c, h->ctl, sizeof(c), cudaMemcpyDeviceToHost));
+  c.log_size = 0; c.log_steps = 0; c.log_first = 0;
+  c.status &= ~ns::kErrLogFull;
+  CK(cudaMemcpy(h->ctl, &c, sizeof(c), cudaMemcpyHostToDevice));
+  return NS_OK;
+}
+
+ns_status ns_spike_log_range(ns_handle* h, uint64_t* first_step, uint64_t* n_steps) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  if (!first_step || !n_steps) return fail(h, NS_ERR_INVALID_ARG, "null output");
+  CK(cudaSetDevice(h->dev));
+  ns::Ctl c{};
+  CK(cudaMemcpyAsync(&c, h->ctl, sizeof(c), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  *first_step = c.log_first;
+  *n_steps = c.log_steps;
+  return NS_OK;
+}
+
+ns_status ns_get_step(ns_handle* h, uint64_t* step) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  if (!step) return fail(h, NS_ERR_INVALID_ARG, "null output");
+  CK(cudaSetDevice(h->dev));
+  unsigned long long s = 0;
+  CK(cudaMemcpyAsync(&s, &h->ctl->step_base, 8, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  *step = s;
+  return NS_OK;
+}
+
+ns_status ns_download_state(ns_handle* h, ns_neuron_soa* o, float* w_out) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  if (!o) return fail(h, NS_ERR_INVALID_ARG, "null output");
+  ns_status r = ready(h);
+  if (r) return r;
+  CK(cudaSetDevice(h->dev));
+  CK(cudaStreamSynchronize(h->st));
+  const uint64_t n = h->n;
+  NsDev& d = h->d;
+  auto dn = [&](void* dst, const void* src, size_t bytes) {
+    return cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost);
+  };
+  o->n = n;
+  if (o->v) CK(dn(o->v, d.v, n * 4));
+  if (o->u) CK(dn(o->u, d.u, n * 4));
+  if (o->refractory) CK(dn(o->refractory, d.refr, n * 4));
+  if (o->current) CK(dn(o->current, d.I, n * 4));
+  if (o->hh_m) CK(dn(o->hh_m, d.gm, n * 4));
+  if (o->hh_h) CK(dn(o->hh_h, d.gh, n * 4));
+  if (o->hh_n) CK(dn(o->hh_n, d.gn, n * 4));
+  if (o->inhibitory) CK(dn(o->inhibitory, d.inh, n));
+  if (o->is_output) CK(dn(o->is_output, d.outp, n));
+  if (o->pre_trace) CK(dn(o->pre_trace, d.pre, n * 4));
+  if (o->post_trace) CK(dn(o->post_trace, d.post, n * 4));
+  if (o->last_spike_step) CK(dn(o->last_spike_step, d.last, n * 8));
+  if (o->firing_rate) CK(dn(o->firing_rate, d.rate, n * 8));
+  if (o->conductance)
+    for (int t = 0; t < 4; ++t) CK(dn(o->conductance + (uint64_t)t * n, d.G[t], n * 4));
+  if (o->pending_input) {
+    const uint64_t rows = (uint64_t)h->ntypes_acc * h->cfg.delay_steps;
+    for (uint64_t q = 0; q < rows; ++q) CK(dn(o->pending_input + q * n, d.acc + q * h->n_pad, n * 8));
+  }
+  if (o->params) {
+    const int ppn = params_for(h->cfg.model);
+    const int npar = h->cfg.model == NS_MODEL_LIF ? 5 : ppn;
+    std::vector<std::vector<float>> par(npar, std::vector<float>(n));
+    for (int q = 0; q < npar; ++q) CK(dn(par[q].data(), d.par[q], n * 4));
+    std::vector<int32_t> rs(n);
+    CK(dn(rs.data(), d.refr_steps, n * 4));
+    for (uint64_t i = 0; i < n; ++i) {
+      float* p = o->params + i * ppn;
+      if (h->cfg.model == NS_MODEL_LIF) {
+        p[0] = par[0][i]; p[1] = par[1][i]; p[2] = par[2][i]; p[3] = par[3][i];
+        p[4] = (float)(rs[i] * h->cfg.dt_ms); p[5] = par[4][i];
+      } else {
+        for (int q = 0; q < ppn; ++q) p[q] = par[q][i];
+      }
+    }
+  }
+  if (w_out && h->m) {
+    if (d.w16) {
+      float* tmpw = nullptr;
+      CK(cudaMalloc(&tmpw, h->m * 4));
+      k_from_bf16<<<h->sms * 8, 256, 0, h->st>>>(d.w16, tmpw, h->m);
+      CK(cudaStreamSynchronize(h->st));
+      cudaError_t e = cudaMemcpy(w_out, tmpw, h->m * 4, cudaMemcpyDeviceToHost);
+      cudaFree(tmpw);
+      CK(e);
+    } else {
+      CK(dn(w_out, d.w32, h->m * 4));
+    }
+  }
+  return NS_OK;
+}
+
+ns_status ns_upload_state(ns_handle* h, const ns_neuron_soa* in, const float* w_in, uint64_t step) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  if (!in) return fail(h, NS_ERR_INVALID_ARG, "null state");
+  ns_status r = ready(h);
+  if (r) return r;
+  if (in->n != h->n) return fail(h, NS_ERR_INVALID_ARG, "state n differs from the network");
+  CK(cudaSetDevice(h->dev));
+  CK(cudaStreamSynchronize(h->st));
+  const uint64_t n = h->n;
+  NsDev& d = h->d;
+  auto upl = [&](void* dst, const void* src, size_t bytes) {
+    return cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
+  };
+  if (in->v) CK(upl(d.v, in->v, n * 4));
+  if (in->u) CK(upl(d.u, in->u, n * 4));
+  if (in->refractory) CK(upl(d.refr, in->refractory, n * 4));
+  if (in->current) CK(upl(d.I, in->current, n * 4));
+  if (in->hh_m) CK(upl(d.gm, in->hh_m, n * 4));
+  if (in->hh_h) CK(upl(d.gh, in->hh_h, n * 4));
+  if (in->hh_n) CK(upl(d.gn, in->hh_n, n * 4));
+  if (in->pre_trace) CK(upl(d.pre, in->pre_trace, n * 4));
+  if (in->post_trace) CK(upl(d.post, in->post_trace, n * 4));
+  if (in->last_spike_step) CK(upl(d.last, in->last_spike_step, n * 8));
+  if (in->firing_rate) CK(upl(d.rate, in->firing_rate, n * 8));
+  if (in->conductance)
+    for (int t = 0; t < 4; ++t) CK(upl(d.G[t], in->conductance + (uint64_t)t * n, n * 4));
+  if (in->pending_input) {
+    const uint64_t rows = (uint64_t)h->ntypes_acc * h->cfg.delay_steps;
+    for (uint64_t q = 0; q < rows; ++q) CK(upl(d.acc + q * h->n_pad, in->pending_input + q * n, n * 8));
+  }
+  if (w_in && h->m) {
+    float* tmpw = nullptr;
+    CK(cudaMalloc(&tmpw, h->m * 4));
+    cudaError_t e = cudaMemcpy(tmpw, w_in, h->m * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+      if (d.w16) k_to_bf16<<<h->sms * 8, 256, 0, h->st>>>(tmpw, d.w16, h->m);
+      else e = cudaMemcpyAsync(d.w32, tmpw, h->m * 4, cudaMemcpyDeviceToDevice, h->st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+    }
+    cudaFree(tmpw);
+    CK(e);
+  }
+  ns::Ctl c{};
+  c.step_base = step;
+  c.sim_time = (double)step * h->cfg.dt_ms;
+  CK(cudaMemcpy(h->ctl, &c, sizeof(c), cudaMemcpyHostToDevice));
+  CK(cudaMemset(d.flags, 0, (size_t)h->ntiles * 8));
+  return NS_OK;
+}
+
+ns_status ns_download_rates(ns_handle* h, double* rates_out) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  if (!rates_out) return fail(h, NS_ERR_INVALID_ARG, "null output");
+  ns_status r = ready(h);
+  if (r) return r;
+  CK(cudaSetDevice(h->dev));
+  CK(cudaStreamSynchronize(h->st));
+  CK(cudaMemcpy(rates_out, h->d.rate, h->n * 8, cudaMemcpyDeviceToHost));
+  return NS_OK;
+}
+
+ns_status ns_weight_stats(ns_handle* h, double* mean, double* stddev) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  if (!mean || !stddev) return fail(h, NS_ERR_INVALID_ARG, "null output");
+  ns_status r = ready(h);
+  if (r) return r;
+  if (h->m == 0) { *mean = 0; *stddev = 0; return NS_OK; }
+  CK(cudaSetDevice(h->dev));
+  double* acc = nullptr;
+  CK(cudaMalloc(&acc, 16));
+  CK(cudaMemsetAsync(acc, 0, 16, h->st));
+  k_weight_sum<<<h->sms * 8, 256, 0, h->st>>>(h->d.w32, h->d.w16, h->m, 0.0, 0, acc);
+  double s = 0;
+  cudaError_t e = cudaMemcpyAsync(&s, acc, 8, cudaMemcpyDeviceToHost, h->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+  const double mu = s / (double)h->m;
+  if (e == cudaSuccess) {
+    k_weight_sum<<<h->sms * 8, 256, 0, h->st>>>(h->d.w32, h->d.w16, h->m, mu, 1, acc + 1);
+    e = cudaMemcpyAsync(&s, acc + 1, 8, cudaMemcpyDeviceToHost, h->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+  }
+  cudaFree(acc);
+  CK(e);
+  h->launches += 2;
+  *mean = mu;
+  *stddev = std::sqrt(s / (double)h->m);
+  return NS_OK;
+}
+
+ns_status ns_counters(ns_handle* h, uint64_t out[4]) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  if (!out) return fail(h, NS_ERR_INVALID_ARG, "null output");
+  CK(cudaSetDevice(h->dev));
+  ns::Ctl c{};
+  CK(cudaMemcpyAsync(&c, h->ctl, sizeof(c), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  out[0] = c.step_base; out[1] = c.spikes_total; out[2] = c.out_total; out[3] = c.events_total;
+  return NS_OK;
+}
+
+ns_status ns_get_stream(ns_handle* h, void** stream) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  if (!stream) return fail(h, NS_ERR_INVALID_ARG, "null output");
+  *stream = (void*)h->st;
+  return NS_OK;
+}
+
+ns_status ns_profile_steps(ns_handle* h, uint32_t n_steps, double* kernel_ms, uint64_t* launches) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  if (!kernel_ms || !launches) return fail(h, NS_ERR_INVALID_ARG, "null output");
+  ns_status r = ready(h);
+  if (r) return r;
+  CK(cudaSetDevice(h->dev));
+  fill_scalars(h);
+  neuron_fn nf = pick_neuron(h->cfg.model, h->cfg.input_mode);
+  prop_fn pf = pick_prop(h->cfg.input_mode, h->cfg.weight_format);
+  const int nk = h->cfg.homeostasis_enabled ? 3 : 2;
+  std::vector<cudaEvent_t> ev((size_t)n_steps * nk * 2);
+  for (auto& e : ev) CK(cudaEventCreate(&e));
+  for (uint32_t j = 0; j < n_steps; ++j) {
+    cudaEvent_t* e = &ev[(size_t)j * nk * 2];
+    CK(cudaEventRecord(e[0], h->st));
+    nf<<<h->ntiles, ns::kThreads, 0, h->st>>>(h->d, j);
+    CK(cudaEventRecord(e[1], h->st));
+    CK(cudaEventRecord(e[2], h->st));
+    pf<<<h->prop_blocks, 256, 0, h->st>>>(h->d, j);
+    CK(cudaEventRecord(e[3], h->st));
+    if (nk == 3) {
+      CK(cudaEventRecord(e[4], h->st));
+      if (h->cfg.weight_format == NS_WEIGHT_BF16)
+        ns::k_homeostasis<true><<<h->homeo_blocks, 256, 0, h->st>>>(h->d, j);
+      else
+        ns::k_homeostasis<false><<<h->homeo_blocks, 256, 0, h->st>>>(h->d, j);
+      CK(cudaEventRecord(e[5], h->st));
+    }
+  }
+  ns::k_advance<<<1, 1, 0, h->st>>>(h->ctl, n_steps);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(h->st));
+  for (uint32_t j = 0; j < n_steps; ++j)
+    for (int q = 0; q < nk; ++q) {
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, ev[((size_t)j * nk + q) * 2], ev[((size_t)j * nk + q) * 2 + 1]));
+      kernel_ms[q] += ms;
+      launches[q] += 1;
+    }
+  for (auto& e : ev) cudaEventDestroy(e);
+  h->launches += (uint64_t)n_steps * nk + 1;
+  return check_device_status(h);
+}
+
+ns_status ns_launch_count(ns_handle* h, uint64_t* launches) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  if (!launches) return fail(h, NS_ERR_INVALID_ARG, "null output");
+  *launches = h->launches;
+  return NS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,347 @@
+"""Python host mirror of the reference crate's simulation API, backed by the
+device through the C ABI.
+
+`Network` carries what `neural_sim::network::Network` holds for the hot path
+(src/network/mod.rs:36-48): the neuron SoA (src/neuron/mod.rs:126-163) and the
+CSR synapse arrays. `SimulationEngine` mirrors `SimulationEngine`
+(src/simulation/engine.rs:43-823): `step()` returns the spiking neurons of one
+step like `StepResult` (engine.rs:35-41), `simulate_ms` is engine.rs:792-797,
+`stats()` is engine.rs:799-801. Every call goes through libneuralsim.so.
+"""
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _abi as A
+
+PARAMS_PER_NEURON = {A.MODEL_LIF: 6, A.MODEL_IZHIKEVICH: 4, A.MODEL_HH: 7}
+
+
+def _ptr(a):
+    return None if a is None else C.c_void_p(a.ctypes.data)
+
+
+@dataclass
+class Network:
+    """Neuron SoA + CSR-by-source synapses (synapse arrays in CSR order)."""
+    model: int
+    params: np.ndarray            # (n, ppn) float32
+    row_ptr: np.ndarray           # (n+1,) uint64
+    col: np.ndarray               # (m,) uint32
+    w: np.ndarray                 # (m,) float32
+    syn_type: np.ndarray = None   # (m,) uint8
+    plastic: np.ndarray = None    # (m,) uint8
+    v0: np.ndarray = None
+    u0: np.ndarray = None
+    m0: np.ndarray = None
+    h0: np.ndarray = None
+    n0: np.ndarray = None
+    inhibitory: np.ndarray = None
+    is_output: np.ndarray = None
+    name: str = "NeuralSim Network"
+
+    @property
+    def n(self):
+        return int(self.params.shape[0])
+
+    @property
+    def m(self):
+        return int(self.col.shape[0])
+
+    def __post_init__(self):
+        self.params = np.ascontiguousarray(self.params, dtype=np.float32)
+        self.row_ptr = np.ascontiguousarray(self.row_ptr, dtype=np.uint64)
+        self.col = np.ascontiguousarray(self.col, dtype=np.uint32)
+        self.w = np.ascontiguousarray(self.w, dtype=np.float32)
+        for name in ("syn_type", "plastic", "inhibitory", "is_output"):
+            a = getattr(self, name)
+            if a is not None:
+                setattr(self, name, np.ascontiguousarray(a, dtype=np.uint8))
+        for name in ("v0", "u0", "m0", "h0", "n0"):
+            a = getattr(self, name)
+            if a is not None:
+                setattr(self, name, np.ascontiguousarray(a, dtype=np.float32))
+
+
+@dataclass
+class SimConfig:
+    """Mirrors SimulationConfig + PlasticityConfig (src/config/mod.rs:61-68,
+    src/synapse/mod.rs:122-157) plus the semantics switches of this backend."""
+    model: int = A.MODEL_LIF
+    input_mode: int = A.INPUT_DIRECT_DECAY
+    hh_integrator: int = A.HH_EULER_REF
+    weight_format: int = A.WEIGHT_F32
+    dt_ms: float = 0.5
+    delay_steps: int = 1
+    device: int = 0
+    seed: int = 42
+    current_decay: float = 0.92
+    stdp_enabled: bool = True
+    tau_plus: float = 20.0
+    tau_minus: float = 20.0
+    a_plus: float = 0.01
+    a_minus: float = 0.012
+    w_min: float = 0.0
+    w_max: float = 10.0
+    homeostasis_enabled: bool = True
+    homeostatic_target_rate: float = 5.0
+    homeostatic_tau: float = 5000.0
+    contribution_tau: float = 1000.0
+    spike_log_capacity: int = 0
+    spike_log_steps: int = 0
+    graph_chunk: int = 1000
+
+    def to_c(self):
+        c = A.NsConfig()
+        for name, _ in A.NsConfig._fields_:
+            setattr(c, name, type(getattr(c, name))(getattr(self, name)))
+        return c
+
+
+@dataclass
+class Drive:
+    kind: int = A.DRIVE_NONE
+    p: float = 0.0
+    amplitude: float = 0.0
+    sigma_exc: float = 0.0
+    sigma_inh: float = 0.0
+    kick_chance: float = 0.0
+    kick_strength: float = 0.0
+    kick_min: int = 0
+    kick_max: int = 0
+
+    def to_c(self):
+        d = A.NsDrive()
+        for name, _ in A.NsDrive._fields_:
+            setattr(d, name, getattr(self, name))
+        return d
+
+    @staticmethod
+    def reference_default():
+        """The reference engine's drive (engine.rs:100-103, :273-287)."""
+        return Drive(A.DRIVE_REF_UNIFORM, p=0.3, amplitude=8.0, kick_chance=0.01,
+                     kick_strength=20.0, kick_min=5, kick_max=30)
+
+
+@dataclass
+class StepResult:
+    spike_count: int
+    output_spike_count: int
+    spiking_neurons: np.ndarray = field(default_factory=lambda: np.zeros(0, np.uint32))
+
+
+class SimulationEngine:
+    """Device-backed engine. One instance owns one ns_handle (not thread-safe,
+    like the Mutex-guarded reference engine, src/simulation/scheduler.rs:23)."""
+
+    def __init__(self, network: Network, config: SimConfig = None, drive: Drive = None):
+        self.lib = A.load()
+        self.config = config or SimConfig(model=network.model)
+        if self.config.model != network.model:
+            raise ValueError("config.model differs from network.model")
+        self.network = network
+        self._h = C.c_void_p()
+        cfg = self.config.to_c()
+        st = self.lib.ns_create(C.byref(cfg), C.byref(self._h))
+        if st != A.NS_OK:
+            raise A.NsError(st, (self.lib.ns_last_error(None) or b"").decode())
+        try:
+            self._upload(network)
+            self.set_drive(drive or Drive())
+        except Exception:
+            self.close()
+            raise
+        self._stats_total = {"spikes": 0, "output_spikes": 0, "events": 0}
+
+    # -- uploads (init_gpu, engine.rs:181-252) --
+    def _upload(self, net: Network):
+        soa = A.NsNeuronSoa()
+        soa.n = net.n
+        soa.params = _ptr(net.params)
+        soa.params_per_neuron = PARAMS_PER_NEURON[net.model]
+        soa.v = _ptr(net.v0)
+        soa.u = _ptr(net.u0)
+        soa.hh_m = _ptr(net.m0)
+        soa.hh_h = _ptr(net.h0)
+        soa.hh_n = _ptr(net.n0)
+        soa.inhibitory = _ptr(net.inhibitory)
+        soa.is_output = _ptr(net.is_output)
+        self._check(self.lib.ns_upload_neurons(self._h, C.byref(soa)))
+        self._check(self.lib.ns_upload_csr(
+            self._h, net.n, net.m, _ptr(net.row_ptr), _ptr(net.col), _ptr(net.w),
+            _ptr(net.syn_type), _ptr(net.plastic)))
+
+    def _check(self, st):
+        A.check(st, self._h)
+
+    def set_drive(self, drive: Drive):
+        self.drive = drive
+        d = drive.to_c()
+        self._check(self.lib.ns_set_drive(self._h, C.byref(d)))
+
+    # -- stepping --
+    def run(self, n_steps: int) -> A.NsStepStats:
+        out = A.NsStepStats()
+        self._check(self.lib.ns_step(self._h, int(n_steps), C.byref(out)))
+        self._stats_total["spikes"] += out.spikes
+        self._stats_total["output_spikes"] += out.output_spikes
+        self._stats_total["events"] += out.events
+        return out
+
+    def step(self) -> StepResult:
+        """One step; returns the ascending spiking neuron list when the spike
+        log is enabled (spike_log_capacity > 0), else only the counts."""
+        k = self.current_step()
+        out = self.run(1)
+        spikes = np.zeros(0, np.uint32)
+        if self.config.spike_log_capacity > 0:
+            spikes = self.read_spikes(k, 1)[0]
+        return StepResult(int(out.spikes), int(out.output_spikes), spikes)
+
+    def simulate_ms(self, duration_ms: float):
+        steps = int(duration_ms / self.config.dt_ms)
+        if steps:
+            self.run(steps)
+
+    def current_step(self) -> int:
+        s = C.c_uint64()
+        self._check(self.lib.ns_get_step(self._h, C.byref(s)))
+        return int(s.value)
+
+    def stats(self) -> dict:
+        out = dict(self._stats_total)
+        out["steps"] = self.current_step()
+        out["sim_time_ms"] = out["steps"] * self.config.dt_ms
+        return out
+
+    def weight_stats(self):
+        mu, sd = C.c_double(), C.c_double()
+        self._check(self.lib.ns_weight_stats(self._h, C.byref(mu), C.byref(sd)))
+        return mu.value, sd.value
+
+    # -- spike log --
+    def log_range(self):
+        a, b = C.c_uint64(), C.c_uint64()
+        self._check(self.lib.ns_spike_log_range(self._h, C.byref(a), C.byref(b)))
+        return int(a.value), int(b.value)
+
+    def read_spikes(self, first_step: int, n_steps: int):
+        """List of ascending uint32 arrays, one per step."""
+        idx, off = self.read_raster(first_step, n_steps)
+        return [idx[int(off[q]):int(off[q + 1])] for q in range(n_steps)]
+
+    def read_raster(self, first_step: int, n_steps: int):
+        """(idx, offsets) flat form of the spike log."""
+        off = np.zeros(n_steps + 1, np.uint64)
+        nw = C.c_uint64()
+        st = self.lib.ns_read_spikes(self._h, first_step, n_steps, None, _ptr(off), 0, C.byref(nw))
+        total = int(nw.value)
+        if st != A.NS_OK and total == 0:
+            self._check(st)
+        idx = np.zeros(max(total, 1), np.uint32)
+        self._check(self.lib.ns_read_spikes(self._h, first_step, n_steps, _ptr(idx), _ptr(off),
+                                            total, C.byref(nw)))
+        return idx[:total], off
+
+    def clear_spike_log(self):
+        self._check(self.lib.ns_clear_spike_log(self._h))
+
+    # -- state --
+    def download_state(self, with_weights=True):
+        n = self.network.n
+        ppn = PARAMS_PER_NEURON[self.config.model]
+        cond = self.config.input_mode in (A.INPUT_CONDUCTANCE_REF, A.INPUT_CONDUCTANCE_FRESH)
+        ntypes = 4 if cond else 1
+        st = {
+            "v": np.zeros(n, np.float32), "u": np.zeros(n, np.float32),
+            "refractory": np.zeros(n, np.int32), "current": np.zeros(n, np.float32),
+            "hh_m": np.zeros(n, np.float32), "hh_h": np.zeros(n, np.float32),
+            "hh_n": np.zeros(n, np.float32), "params": np.zeros((n, ppn), np.float32),
+            "inhibitory": np.zeros(n, np.uint8), "is_output": np.zeros(n, np.uint8),
+            "pre_trace": np.zeros(n, np.float32), "post_trace": np.zeros(n, np.float32),
+            "last_spike_step": np.zeros(n, np.int64),
+            "pending_input": np.zeros(ntypes * self.config.delay_steps * n, np.int64),
+            "conductance": np.zeros(4 * n, np.float32), "firing_rate": np.zeros(n, np.float64),
+        }
+        soa = A.NsNeuronSoa()
+        for name, arr in st.items():
+            setattr(soa, name, _ptr(arr))
+        soa.params_per_neuron = ppn
+        w = np.zeros(max(self.network.m, 1), np.float32) if with_weights else None
+        self._check(self.lib.ns_download_state(self._h, C.byref(soa), _ptr(w)))
+        if with_weights:
+            st["w"] = w[:self.network.m]
+        return st
+
+    def upload_state(self, st: dict, step: int):
+        soa = A.NsNeuronSoa()
+        soa.n = self.network.n
+        for name in ("v", "u", "refractory", "current", "hh_m", "hh_h", "hh_n", "pre_trace",
+                     "post_trace", "last_spike_step", "pending_input", "conductance",
+                     "firing_rate"):
+            if name in st:
+                setattr(soa, name, _ptr(st[name]))
+        soa.params_per_neuron = PARAMS_PER_NEURON[self.config.model]
+        self._check(self.lib.ns_upload_state(self._h, C.byref(soa), _ptr(st.get("w")), int(step)))
+
+    def rates(self):
+        r = np.zeros(self.network.n, np.float64)
+        self._check(self.lib.ns_download_rates(self._h, _ptr(r)))
+        return r
+
+    def step_traced(self, cap: int):
+        pos = np.zeros(max(cap, 1), np.uint64)
+        ne = C.c_uint64()
+        self._check(self.lib.ns_step_traced(self._h, _ptr(pos), cap, C.byref(ne)))
+        return pos[:min(cap, int(ne.value))], int(ne.value)
+
+    def counters(self):
+        """(steps, spikes, output_spikes, events) running totals on the device."""
+        c = (C.c_uint64 * 4)()
+        self._check(self.lib.ns_counters(self._h, c))
+        return tuple(int(x) for x in c)
+
+    def stream(self):
+        """cudaStream_t of this handle (as an int)."""
+        p = C.c_void_p()
+        self._check(self.lib.ns_get_stream(self._h, C.byref(p)))
+        return int(p.value or 0)
+
+    def profile_steps(self, n_steps: int):
+        """Per-kernel device time over n_steps eager steps:
+        {"neuron": (ms_total, launches), "propagate": ..., "homeostasis": ...}"""
+        ms = (C.c_double * 3)()
+        ln = (C.c_uint64 * 3)()
+        self._check(self.lib.ns_profile_steps(self._h, int(n_steps), ms, ln))
+        names = ("neuron", "propagate", "homeostasis")
+        return {names[q]: (ms[q], int(ln[q])) for q in range(3) if ln[q]}
+
+    def launch_count(self):
+        c = C.c_uint64()
+        self._check(self.lib.ns_launch_count(self._h, C.byref(c)))
+        return int(c.value)
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            self.lib.ns_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def device_count():
+    lib = A.load()
+    c = C.c_int()
+    lib.ns_device_count(C.byref(c))
+    return c.value
