@@ -133,12 +133,12 @@ def build_network(n, k, seed):
     return configs.izh_c2(n=n, k=k, seed=seed)
 
 
-def step_bytes(n, spikes, events, in_plastic):
-    """Algorithmic HBM bytes of one simulation step:
-    64 N (v,u r/w; a,b,c,d; int64 accumulator read + zero; pre/post traces r/w)
-    + 16 S (row_ptr pair, CSC pointer pair) + 8 E_out (col, bf16 w, LTP write)
-    + 8 E_in,plastic (incoming index, bf16 w read + write)."""
-    return 64.0 * n + 16.0 * spikes + 8.0 * events + 8.0 * in_plastic
+def step_bytes(n, sim_steps, spikes, events, in_plastic):
+    """Algorithmic HBM bytes of sim_steps simulation steps:
+    64 N per step (v,u r/w; a,b,c,d; int64 accumulator read + zero; pre/post
+    traces r/w) + 16 S (row_ptr pair, CSC pointer pair) + 8 E_out (col, bf16 w,
+    LTP write) + 8 E_in,plastic (incoming index, bf16 w read + write)."""
+    return 64.0 * n * sim_steps + 16.0 * spikes + 8.0 * events + 8.0 * in_plastic
 
 
 def neuron_kernel_bytes(n, spikes):
@@ -206,7 +206,7 @@ def run_ours(a):
     # whole-step algorithmic bytes: plastic in-degree of the spikers is
     # estimated from the mean (80 of 100 incoming synapses are plastic)
     mean_in_plastic = float(in_deg_plastic.mean())
-    bytes_total = step_bytes(net.n, spikes, events, spikes * mean_in_plastic) if sim_steps else 0.0
+    bytes_total = step_bytes(net.n, sim_steps, spikes, events, spikes * mean_in_plastic)
 
     if dist:
         t = torch.tensor([ms, float(events)], dtype=torch.float64, device=f"cuda:{local}")

@@ -81,6 +81,14 @@ void drop_graphs(ns_handle* h) {
 
 uint64_t round_up(uint64_t x, uint64_t a) { return (x + a - 1) / a * a; }
 
+// Every copy is ordered on the handle's own (non-blocking) stream: a legacy
+// cudaMemcpy would not order against kernels on that stream.
+cudaError_t copy_sync(ns_handle* h, void* dst, const void* src, size_t bytes, cudaMemcpyKind kind) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, kind, h->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+  return e;
+}
+
 int params_for(uint32_t model) { return model == NS_MODEL_LIF ? 6 : (model == NS_MODEL_IZHIKEVICH ? 4 : 7); }
 
 uint32_t prob_threshold(double p) {
@@ -266,8 +274,7 @@ ns_status check_device_status(ns_handle* h) {
   unsigned int stt = 0;
   CK(cudaMemcpyAsync(&stt, &h->ctl->status, 4, cudaMemcpyDeviceToHost, h->st));
   CK(cudaStreamSynchronize(h->st));
-  if (stt & ns::kErrLookback)
-    return fail(h, NS_ERR_DEVICE_TIMEOUT, "spike compaction look-back wait gave up");
+  (void)stt;
   return NS_OK;
 }
 
@@ -459,8 +466,17 @@ ns_status ns_create(const ns_config* cfg, ns_handle** out) {
     delete h;
     return NS_ERR_NO_DEVICE;
   }
-  h->prop_blocks = h->sms * 8;
-  h->homeo_blocks = h->sms * 8;
+  {
+    // grid-stride kernels get exactly the resident capacity of the device
+    int nb = 0;
+    prop_fn pf = pick_prop(c.input_mode, c.weight_format);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pf, 256, 0) != cudaSuccess || nb < 1) nb = 4;
+    h->prop_blocks = h->sms * nb;
+    nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ns::k_homeostasis<true>, 256, 0) != cudaSuccess || nb < 1) nb = 4;
+    h->homeo_blocks = h->sms * nb;
+    cudaGetLastError();
+  }
   e = cudaMalloc(&h->ctl, sizeof(ns::Ctl));
   if (e == cudaSuccess) e = cudaMemset(h->ctl, 0, sizeof(ns::Ctl));
   if (e != cudaSuccess) {
@@ -580,7 +596,7 @@ ns_status ns_upload_neurons(ns_handle* h, const ns_neuron_soa* s) {
   for (int q = 0; q < 7; ++q) d.par[q] = nullptr;
   for (int q = 0; q < npar; ++q) DA(d.par[q], np)
   for (int t = 0; t < 4; ++t) DA(d.G[t], np)
-  DA(d.bitmap, np / 32 + 2) DA(d.spk, np) DA(d.flags, h->ntiles)
+  DA(d.bitmap, np / 32 + 2) DA(d.spk, np) DA(d.tile_cnt, h->ntiles + 1) DA(d.tile_off, h->ntiles + 1)
 #undef DA
   auto up = [&](void* dst, const void* src, size_t bytes) {
     return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->st);
@@ -644,7 +660,6 @@ static ns_status alloc_dynamic(ns_handle* h) {
   d.trace_pos = nullptr; d.trace_off = nullptr; d.trace_cap = 0;
   // reset the control block: counters, log, tickets
   CK(cudaMemsetAsync(h->ctl, 0, sizeof(ns::Ctl), h->st));
-  CK(cudaMemsetAsync(d.flags, 0, (size_t)h->ntiles * 8, h->st));
   CK(cudaStreamSynchronize(h->st));
   return NS_OK;
 }
@@ -801,8 +816,6 @@ ns_status ns_step(ns_handle* h, uint32_t n_steps, ns_step_stats* out) {
     out->last_step_spikes = n_steps ? after.step_spikes[(after.step_base - 1) & 3] : 0;
     out->sim_time_ms = after.sim_time;
   }
-  if (after.status & ns::kErrLookback)
-    return fail(h, NS_ERR_DEVICE_TIMEOUT, "spike compaction look-back wait gave up");
   if ((after.status & ns::kErrLogFull) && !(before.status & ns::kErrLogFull))
     return fail(h, NS_ERR_SPIKE_LOG_FULL, "spike log capacity exceeded; later steps not logged");
   return NS_OK;
@@ -844,7 +857,7 @@ ns_status ns_step_traced(ns_handle* h, uint64_t* pos_out, uint64_t cap, uint64_t
   CK(cudaMemcpyAsync(&total, off + cnt, 8, cudaMemcpyDeviceToHost, h->st));
   CK(cudaStreamSynchronize(h->st));
   *n_events = total;
-  if (cap) CK(cudaMemcpy(pos_out, pos, std::min<uint64_t>(cap, total) * 8, cudaMemcpyDeviceToHost));
+  if (cap) CK(copy_sync(h, pos_out, pos, std::min<uint64_t>(cap, total) * 8, cudaMemcpyDeviceToHost));
   free_bag(tmp);
   return check_device_status(h);
 }
@@ -862,14 +875,14 @@ ns_status ns_read_spikes(ns_handle* h, uint64_t first_step, uint32_t n_steps, ui
     return fail(h, NS_ERR_INVALID_ARG, "requested steps are not in the log");
   const uint64_t s0 = first_step - c.log_first;
   std::vector<unsigned long long> off(n_steps + 1);
-  CK(cudaMemcpy(off.data(), h->d.log_off + s0, (n_steps + 1) * 8, cudaMemcpyDeviceToHost));
+  CK(copy_sync(h, off.data(), h->d.log_off + s0, (n_steps + 1) * 8, cudaMemcpyDeviceToHost));
   const uint64_t total = off[n_steps] - off[0];
   for (uint32_t q = 0; q <= n_steps; ++q) offsets_out[q] = off[q] - off[0];
   *n_written = total;
   if (total > cap) return fail(h, NS_ERR_INVALID_ARG, "idx_out capacity too small");
   if (total) {
     if (!idx_out) return fail(h, NS_ERR_INVALID_ARG, "null idx_out");
-    CK(cudaMemcpy(idx_out, h->d.log_idx + off[0], total * 4, cudaMemcpyDeviceToHost));
+    CK(copy_sync(h, idx_out, h->d.log_idx + off[0], total * 4, cudaMemcpyDeviceToHost));
   }
   return NS_OK;
 }
@@ -879,10 +892,10 @@ ns_status ns_clear_spike_log(ns_handle* h) {
   CK(cudaSetDevice(h->dev));
   CK(cudaStreamSynchronize(h->st));
   ns::Ctl c{};
-  CK(cudaMemcpy(&c, h->ctl, sizeof(c), cudaMemcpyDeviceToHost));
+  CK(copy_sync(h, &c, h->ctl, sizeof(c), cudaMemcpyDeviceToHost));
   c.log_size = 0; c.log_steps = 0; c.log_first = 0;
   c.status &= ~ns::kErrLogFull;
-  CK(cudaMemcpy(h->ctl, &c, sizeof(c), cudaMemcpyHostToDevice));
+  CK(copy_sync(h, h->ctl, &c, sizeof(c), cudaMemcpyHostToDevice));
   return NS_OK;
 }
 
@@ -919,7 +932,7 @@ ns_status ns_download_state(ns_handle* h, ns_neuron_soa* o, float* w_out) {
   const uint64_t n = h->n;
   NsDev& d = h->d;
   auto dn = [&](void* dst, const void* src, size_t bytes) {
-    return cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost);
+    return copy_sync(h, dst, src, bytes, cudaMemcpyDeviceToHost);
   };
   o->n = n;
   if (o->v) CK(dn(o->v, d.v, n * 4));
@@ -964,7 +977,7 @@ ns_status ns_download_state(ns_handle* h, ns_neuron_soa* o, float* w_out) {
       CK(cudaMalloc(&tmpw, h->m * 4));
       k_from_bf16<<<h->sms * 8, 256, 0, h->st>>>(d.w16, tmpw, h->m);
       CK(cudaStreamSynchronize(h->st));
-      cudaError_t e = cudaMemcpy(w_out, tmpw, h->m * 4, cudaMemcpyDeviceToHost);
+      cudaError_t e = copy_sync(h, w_out, tmpw, h->m * 4, cudaMemcpyDeviceToHost);
       cudaFree(tmpw);
       CK(e);
     } else {
@@ -985,7 +998,7 @@ ns_status ns_upload_state(ns_handle* h, const ns_neuron_soa* in, const float* w_
   const uint64_t n = h->n;
   NsDev& d = h->d;
   auto upl = [&](void* dst, const void* src, size_t bytes) {
-    return cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
+    return copy_sync(h, dst, src, bytes, cudaMemcpyHostToDevice);
   };
   if (in->v) CK(upl(d.v, in->v, n * 4));
   if (in->u) CK(upl(d.u, in->u, n * 4));
@@ -1007,7 +1020,7 @@ ns_status ns_upload_state(ns_handle* h, const ns_neuron_soa* in, const float* w_
   if (w_in && h->m) {
     float* tmpw = nullptr;
     CK(cudaMalloc(&tmpw, h->m * 4));
-    cudaError_t e = cudaMemcpy(tmpw, w_in, h->m * 4, cudaMemcpyHostToDevice);
+    cudaError_t e = copy_sync(h, tmpw, w_in, h->m * 4, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) {
       if (d.w16) k_to_bf16<<<h->sms * 8, 256, 0, h->st>>>(tmpw, d.w16, h->m);
       else e = cudaMemcpyAsync(d.w32, tmpw, h->m * 4, cudaMemcpyDeviceToDevice, h->st);
@@ -1019,8 +1032,8 @@ ns_status ns_upload_state(ns_handle* h, const ns_neuron_soa* in, const float* w_
   ns::Ctl c{};
   c.step_base = step;
   c.sim_time = (double)step * h->cfg.dt_ms;
-  CK(cudaMemcpy(h->ctl, &c, sizeof(c), cudaMemcpyHostToDevice));
-  CK(cudaMemset(d.flags, 0, (size_t)h->ntiles * 8));
+  CK(cudaMemcpyAsync(h->ctl, &c, sizeof(c), cudaMemcpyHostToDevice, h->st));
+  CK(cudaStreamSynchronize(h->st));
   return NS_OK;
 }
 
@@ -1031,7 +1044,7 @@ ns_status ns_download_rates(ns_handle* h, double* rates_out) {
   if (r) return r;
   CK(cudaSetDevice(h->dev));
   CK(cudaStreamSynchronize(h->st));
-  CK(cudaMemcpy(rates_out, h->d.rate, h->n * 8, cudaMemcpyDeviceToHost));
+  CK(copy_sync(h, rates_out, h->d.rate, h->n * 8, cudaMemcpyDeviceToHost));
   return NS_OK;
 }
 

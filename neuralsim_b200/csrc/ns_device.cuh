@@ -107,6 +107,32 @@ __host__ __device__ __forceinline__ void sincos_2pi(float u, float* sn, float* c
   }
 }
 
+// e^x for the homeostatic scale factor: Cody-Waite reduction x = n ln2 + r
+// (ln2 split into a 16-bit head and a tail so n*ln2_hi is exact), e^r by its
+// Taylor series to r^7 on |r| <= ln2/2, then scaling by 2^n in the exponent.
+__host__ __device__ __forceinline__ float exp_f(float x) {
+  if (x > 88.0f) x = 88.0f;
+  if (x < -87.0f) x = -87.0f;
+  const float nf = floorf(x * 1.44269504f + 0.5f);
+  float r = x - nf * 0.693145752f;
+  r = r - nf * 1.42860677e-06f;
+  float p = 1.98412698e-04f;
+  p = 1.38888889e-03f + r * p;
+  p = 8.33333333e-03f + r * p;
+  p = 4.16666667e-02f + r * p;
+  p = 1.66666667e-01f + r * p;
+  p = 0.5f + r * p;
+  p = 1.0f + r * p;
+  p = 1.0f + r * p;
+  const uint32_t eb = (uint32_t)((int)nf + 127) << 23;
+#ifdef __CUDA_ARCH__
+  const float sc = __uint_as_float(eb);
+#else
+  float sc; __builtin_memcpy(&sc, &eb, 4);
+#endif
+  return p * sc;
+}
+
 // Fixed point for synaptic sums: 2^40 per unit (mV or current unit). Integer
 // addition is associative, so the sum is independent of event order.
 __device__ __forceinline__ long long to_fix(float w) { return __float2ll_rn(w * 0x1p40f); }

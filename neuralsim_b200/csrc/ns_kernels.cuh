@@ -20,21 +20,23 @@
 namespace ns {
 
 constexpr int kThreads = 256;              // neuron kernel block
-constexpr int kTile = 1024;                // neurons per tile (2 pairs per thread)
+constexpr int kPairs = 4;                  // neuron pairs per thread
+constexpr int kTile = kThreads * 2 * kPairs;  // 2048 neurons per tile
 constexpr int kWarps = kThreads / 32;
-constexpr uint32_t kSpinLimit = 1u << 22;  // bounded look-back wait
+static_assert(kPairs * kWarps <= 32, "one warp scans the per-group counts");
+constexpr uint32_t kSmemTiles = 4096;       // tile offsets kept in shared memory up to this
 
 // device status bits (host maps them to ns_status)
-constexpr uint32_t kErrLookback = 1u;
 constexpr uint32_t kErrLogFull = 2u;
 
 struct Ctl {
   unsigned long long step_base;   // global step of graph node 0
-  unsigned int ticket[2];
+  unsigned int tiles_done;        // neuron-kernel tiles finished this step
   unsigned int status;
-  unsigned int pad;
+  unsigned int log_ok[4];         // step k's spikes went to the log (k & 3)
   unsigned long long spikes_total, out_total, events_total;
   unsigned long long step_spikes[4];
+  unsigned long long spk_acc[4];  // per-step spike count accumulators
   double sim_time;
   unsigned long long log_size;    // indices held
   unsigned long long log_steps;   // steps held
@@ -84,9 +86,10 @@ struct NsDev {
   const uint32_t* all_in_pos;
   float* contrib;
   unsigned long long* acc;         // [type][slot][n_pad]
-  uint32_t* spk;                   // this step's ordered spike list
+  uint32_t* spk;                   // this step's spikes, tile-local ordered lists
   uint32_t* bitmap;                // n_pad / 32 words
-  unsigned long long* flags;       // look-back flags per tile
+  uint32_t* tile_cnt;              // spikes per tile this step
+  uint32_t* tile_off;              // exclusive scan of tile_cnt (large networks)
   Ctl* ctl;
   const float *Ep, *Em;
   uint32_t* log_idx;
@@ -102,8 +105,46 @@ __device__ __forceinline__ bool bit_of(const uint32_t* bm, uint32_t i) {
   return (bm[i >> 5] >> (i & 31)) & 1u;
 }
 
-__device__ __forceinline__ unsigned long long flag_pack(uint32_t tag, uint32_t st, uint32_t val) {
-  return ((unsigned long long)tag << 34) | ((unsigned long long)st << 32) | val;
+// exclusive scan of n values by one 256-thread block (chunks of 1024), result
+// in out[0..n]; returns the total
+__device__ uint32_t block_scan_u32(const uint32_t* in, uint32_t* out, uint32_t n) {
+  __shared__ uint32_t s_w[8];
+  __shared__ uint32_t s_carry;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) s_carry = 0;
+  __syncthreads();
+  for (uint32_t b0 = 0; b0 < n; b0 += 1024) {
+    uint32_t v[4], loc = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const uint32_t idx = b0 + 4u * tid + q;
+      v[q] = idx < n ? in[idx] : 0u;
+      loc += v[q];
+    }
+    uint32_t inc = loc;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += y;
+    }
+    if (lane == 31) s_w[warp] = inc;
+    __syncthreads();
+    uint32_t wpre = 0;
+    for (int q = 0; q < warp; ++q) wpre += s_w[q];
+    uint32_t run = s_carry + wpre + inc - loc;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const uint32_t idx = b0 + 4u * tid + q;
+      if (idx < n) out[idx] = run;
+      run += v[q];
+    }
+    __syncthreads();
+    if (tid == 255) s_carry = run;
+    __syncthreads();
+  }
+  if (tid == 0) out[n] = s_carry;
+  __syncthreads();
+  return s_carry;
 }
 
 // ---------------------------------------------------------------------------
@@ -208,40 +249,32 @@ __device__ __forceinline__ bool model_step(const NsDev& d, NState& s, const floa
 }
 
 // ---------------------------------------------------------------------------
-// Kernel 1: fused neuron update + trace update + ordered compaction.
-// Thread t of tile T owns the neuron pairs (T*1024 + r*512 + 2t, +1), r = 0,1,
+// Kernel 1: fused drive + neuron update + trace decay + ordered compaction.
+// Thread t of tile T owns the neuron pairs (T*2048 + r*512 + 2t, +1), r < 4,
 // so every state array is read with 8-byte coalesced loads and one Philox
-// draw feeds the Gaussian drive of both neurons of a pair.
+// draw feeds the Gaussian drive of both neurons of a pair. All loads of a pair
+// are issued before any store. Each tile writes its spikes, ascending, to its
+// own slice of the spike buffer (warp ballots + a 32-entry scan), so no tile
+// waits for another; the last tile to finish does the step's bookkeeping.
 // ---------------------------------------------------------------------------
 template <int MODEL, int MODE>
 __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
-  __shared__ uint32_t s_tile;
-  __shared__ uint32_t s_off[2 * kWarps];
-  __shared__ uint32_t s_excl, s_total_tile;
+  __shared__ uint32_t s_off[kPairs * kWarps];
+  __shared__ uint32_t s_me[kPairs * kWarps], s_mo[kPairs * kWarps];
+  __shared__ uint32_t s_total;
   __shared__ Kick s_kick[32];
   __shared__ int s_nk;
-  __shared__ unsigned long long s_events;
-  __shared__ uint32_t s_outs;
-  __shared__ unsigned long long s_log_base;
-  __shared__ int s_logging;
+  __shared__ int s_last;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint64_t k = d.ctl->step_base + jstep;
   const uint32_t slot = (uint32_t)(k % d.D);
   constexpr bool COND = (MODE == 3 || MODE == 4);
   constexpr int NT = COND ? 4 : 1;
+  constexpr int NP = MODEL == 0 ? 5 : (MODEL == 1 ? 4 : 7);
 
-  if (tid == 0) {
-    s_tile = atomicAdd(&d.ctl->ticket[k & 1], 1u);
-    // log bookkeeping is advanced by the last tile of this step only after
-    // every tile has published its flag, so read it before publishing
-    s_log_base = d.ctl->log_size;
-    s_logging = (d.log_idx != nullptr && d.ctl->log_steps < d.log_steps_cap &&
-                 !(d.ctl->status & kErrLogFull)) ? 1 : 0;
-    s_events = 0ull;
-    s_outs = 0u;
-    s_nk = 0;
-  }
+  if (tid == 0) s_nk = 0;
+  __syncthreads();
   if (d.drive_kind == 1 && warp == 1) {
     // reference-shaped global kicks (engine.rs:280-287): lane j computes kick j
     U4 x = draw(d.seed, 0, k, kStreamKicks);
@@ -259,94 +292,94 @@ __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
     if (lane == 0) s_nk = cnt;
   }
   __syncthreads();
-  const uint32_t tile = s_tile;
-  if (tid == 0 && tile == d.ntiles - 1) d.ctl->ticket[k & 1] = 0u;  // every ticket is taken
+  const uint32_t tile = blockIdx.x;
   const uint64_t base = (uint64_t)tile * kTile;
   const int nk = s_nk;
 
-  bool spk[2][2];
-  uint32_t rank[2][2];
-  uint64_t idx0[2];
-
-#pragma unroll
-  for (int r = 0; r < 2; ++r) {
+#pragma unroll 1
+  for (int r = 0; r < kPairs; ++r) {
     const uint64_t i0 = base + (uint64_t)r * 512 + 2 * (uint64_t)tid;
-    idx0[r] = i0;
+    // ---- every load of the pair ----
     NState st[2];
-    float2 v2 = *reinterpret_cast<const float2*>(d.v + i0);
+    const float2 v2 = *reinterpret_cast<const float2*>(d.v + i0);
     st[0].v = v2.x; st[1].v = v2.y;
     if (MODEL == 1) {
-      float2 u2 = *reinterpret_cast<const float2*>(d.u + i0);
+      const float2 u2 = *reinterpret_cast<const float2*>(d.u + i0);
       st[0].u = u2.x; st[1].u = u2.y;
     }
     if (MODEL == 0) {
-      int2 r2 = *reinterpret_cast<const int2*>(d.refr + i0);
+      const int2 r2 = *reinterpret_cast<const int2*>(d.refr + i0);
       st[0].refr = r2.x; st[1].refr = r2.y;
     }
     if (MODEL == 2) {
-      float2 a = *reinterpret_cast<const float2*>(d.gm + i0);
-      float2 b = *reinterpret_cast<const float2*>(d.gh + i0);
-      float2 c = *reinterpret_cast<const float2*>(d.gn + i0);
+      const float2 a = *reinterpret_cast<const float2*>(d.gm + i0);
+      const float2 b = *reinterpret_cast<const float2*>(d.gh + i0);
+      const float2 c = *reinterpret_cast<const float2*>(d.gn + i0);
       st[0].m = a.x; st[1].m = a.y; st[0].h = b.x; st[1].h = b.y; st[0].n = c.x; st[1].n = c.y;
     }
     if (MODE == 0 || MODE == 3) {
-      float2 c = *reinterpret_cast<const float2*>(d.I + i0);
+      const float2 c = *reinterpret_cast<const float2*>(d.I + i0);
       st[0].I = c.x; st[1].I = c.y;
     }
-    constexpr int NP = MODEL == 0 ? 5 : (MODEL == 1 ? 4 : 7);
     float par[2][7];
 #pragma unroll
     for (int q = 0; q < NP; ++q) {
-      float2 pv = *reinterpret_cast<const float2*>(d.par[q] + i0);
+      const float2 pv = *reinterpret_cast<const float2*>(d.par[q] + i0);
       par[0][q] = pv.x; par[1][q] = pv.y;
     }
     int rs[2] = {0, 0};
     if (MODEL == 0) {
-      int2 r2 = *reinterpret_cast<const int2*>(d.refr_steps + i0);
+      const int2 r2 = *reinterpret_cast<const int2*>(d.refr_steps + i0);
       rs[0] = r2.x; rs[1] = r2.y;
     }
-    // delivered synaptic input for this step (read and clear the slot)
-    float S[NT][2];
+    longlong2 accv[NT];
 #pragma unroll
-    for (int t = 0; t < NT; ++t) {
-      unsigned long long* ap = d.acc + ((uint64_t)t * d.D + slot) * d.n_pad + i0;
-      longlong2 a2 = *reinterpret_cast<const longlong2*>(ap);
-      S[t][0] = from_fix(a2.x);
-      S[t][1] = from_fix(a2.y);
-      *reinterpret_cast<longlong2*>(ap) = make_longlong2(0, 0);
-    }
+    for (int t = 0; t < NT; ++t)
+      accv[t] = *reinterpret_cast<const longlong2*>(d.acc + ((uint64_t)t * d.D + slot) * d.n_pad + i0);
     float G[4][2];
     if (COND) {
 #pragma unroll
       for (int t = 0; t < 4; ++t) {
-        float2 g2 = *reinterpret_cast<const float2*>(d.G[t] + i0);
+        const float2 g2 = *reinterpret_cast<const float2*>(d.G[t] + i0);
         G[t][0] = g2.x; G[t][1] = g2.y;
       }
     }
-    // drive draws: one Philox per pair
-    U4 x = make_drive_draw(d, i0, k);
+    float2 p2 = make_float2(0.f, 0.f), q2 = make_float2(0.f, 0.f);
+    if (d.stdp) {
+      p2 = *reinterpret_cast<const float2*>(d.pre + i0);
+      q2 = *reinterpret_cast<const float2*>(d.post + i0);
+    }
+    uchar2 ih = make_uchar2(0, 0);
+    if (d.drive_kind == 3) ih = *reinterpret_cast<const uchar2*>(d.inh + i0);
+    // ---- delivered synaptic input for this step (the slot is cleared) ----
+    float S[NT][2];
+#pragma unroll
+    for (int t = 0; t < NT; ++t) {
+      S[t][0] = from_fix(accv[t].x);
+      S[t][1] = from_fix(accv[t].y);
+      *reinterpret_cast<longlong2*>(d.acc + ((uint64_t)t * d.D + slot) * d.n_pad + i0) =
+          make_longlong2(0, 0);
+    }
+    // ---- drive draws: one Philox per pair ----
+    const U4 x = make_drive_draw(d, i0, k);
     float z[2] = {0.f, 0.f};
     if (d.drive_kind == 3) {
-      float u1 = unif_open(x.x), u2 = unif(x.y);
-      float l = ln_f(u1);
-      float rr = sqrtf(-2.0f * l);
+      const float u1 = unif_open(x.x), u2 = unif(x.y);
+      const float l = ln_f(u1);
+      const float rr = sqrtf(-2.0f * l);
       float sn, cs;
       sincos_2pi(u2, &sn, &cs);
       z[0] = rr * cs;
       z[1] = rr * sn;
     }
-    uint8_t inhv[2] = {0, 0};
-    if (d.drive_kind == 3) {
-      uchar2 ih = *reinterpret_cast<const uchar2*>(d.inh + i0);
-      inhv[0] = ih.x; inhv[1] = ih.y;
-    }
+    const uint8_t inhv[2] = {ih.x, ih.y};
+    bool spk[2];
 #pragma unroll
     for (int e = 0; e < 2; ++e) {
       const uint64_t i = i0 + e;
-      // drive value of this neuron (per-neuron draws for the non-Gaussian kinds)
       float addI = 0.f, kick = 0.f, addg = 0.f;
       if (d.drive_kind == 1 || d.drive_kind == 2 || d.drive_kind == 4) {
-        U4 y = (e == 0) ? x : draw(d.seed, (uint32_t)i, k, kStreamDrive);
+        const U4 y = (e == 0) ? x : draw(d.seed, (uint32_t)i, k, kStreamDrive);
         if (d.drive_kind == 1) {
           if (unif(y.x) < d.drive_p) addI = unif(y.y) * d.drive_amp;
         } else if (d.drive_kind == 2) {
@@ -383,38 +416,23 @@ __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
       for (int q = 0; q < nk; ++q)
         if (s_kick[q].target == (uint32_t)i) Iv = Iv + s_kick[q].amt;
       kk = kk + kick;
-      bool s = model_step<MODEL>(d, st[e], par[e], rs[e], Iv, kk, MODE == 1);
+      bool sp = model_step<MODEL>(d, st[e], par[e], rs[e], Iv, kk, MODE == 1);
       st[e].I = Iv;
-      s = s && (i < d.n);
-      spk[r][e] = s;
+      spk[e] = sp && (i < d.n);
     }
-    // traces (per-neuron pre/post; double decay on a spike as in StdpTrace,
-    // src/synapse/plasticity.rs:144-159)
+    // ---- traces: per-step decay here; the spike-time bump (double decay of
+    // StdpTrace, src/synapse/plasticity.rs:144-159) is done by the spiker's
+    // own row walk in k_propagate. qdec keeps the decayed, pre-bump post
+    // trace that LTP of a synapse whose target also spiked must see.
     if (d.stdp) {
-      float2 p2 = *reinterpret_cast<const float2*>(d.pre + i0);
-      float2 q2 = *reinterpret_cast<const float2*>(d.post + i0);
-      float pv[2] = {p2.x * d.ep, p2.y * d.ep};
-      float qv[2] = {q2.x * d.em, q2.y * d.em};
-#pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        if (spk[r][e]) {
-          const uint64_t i = i0 + e;
-          long long lst = d.last[i];
-          long long dk = lst < 0 ? -1 : (long long)k - lst;
-          float fp = (dk >= 0 && (unsigned long long)dk < d.Kp) ? d.Ep[dk] : 0.0f;
-          float fm = (dk >= 0 && (unsigned long long)dk < d.Km) ? d.Em[dk] : 0.0f;
-          d.qdec[i] = qv[e];
-          pv[e] = pv[e] * fp + 1.0f;
-          qv[e] = qv[e] * fm + 1.0f;
-        }
-      }
-      *reinterpret_cast<float2*>(d.pre + i0) = make_float2(pv[0], pv[1]);
-      *reinterpret_cast<float2*>(d.post + i0) = make_float2(qv[0], qv[1]);
+      const float pv0 = p2.x * d.ep, pv1 = p2.y * d.ep;
+      const float qv0 = q2.x * d.em, qv1 = q2.y * d.em;
+      *reinterpret_cast<float2*>(d.pre + i0) = make_float2(pv0, pv1);
+      *reinterpret_cast<float2*>(d.post + i0) = make_float2(qv0, qv1);
+      if (spk[0]) d.qdec[i0] = qv0;
+      if (spk[1]) d.qdec[i0 + 1] = qv1;
     }
-#pragma unroll
-    for (int e = 0; e < 2; ++e)
-      if (spk[r][e]) d.last[i0 + e] = (long long)k;
-    // write back state
+    // ---- write back state ----
     *reinterpret_cast<float2*>(d.v + i0) = make_float2(st[0].v, st[1].v);
     if (MODEL == 1) *reinterpret_cast<float2*>(d.u + i0) = make_float2(st[0].u, st[1].u);
     if (MODEL == 0) *reinterpret_cast<int2*>(d.refr + i0) = make_int2(st[0].refr, st[1].refr);
@@ -430,16 +448,16 @@ __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
       for (int t = 0; t < 4; ++t)
         *reinterpret_cast<float2*>(d.G[t] + i0) = make_float2(G[t][0], G[t][1]);
     }
-    // warp ballots: ascending order inside the warp is (lane, parity)
-    const unsigned me = __ballot_sync(0xffffffffu, spk[r][0]);
-    const unsigned mo = __ballot_sync(0xffffffffu, spk[r][1]);
-    const unsigned lt = (1u << lane) - 1u;
-    const uint32_t pre_cnt = __popc(me & lt) + __popc(mo & lt);
-    rank[r][0] = pre_cnt;
-    rank[r][1] = pre_cnt + (spk[r][0] ? 1u : 0u);
-    if (lane == 0) s_off[r * kWarps + warp] = __popc(me) + __popc(mo);
+    // ---- warp ballots: ascending order inside the warp is (lane, parity) ----
+    const unsigned me = __ballot_sync(0xffffffffu, spk[0]);
+    const unsigned mo = __ballot_sync(0xffffffffu, spk[1]);
+    if (lane == 0) {
+      s_off[r * kWarps + warp] = __popc(me) + __popc(mo);
+      s_me[r * kWarps + warp] = me;
+      s_mo[r * kWarps + warp] = mo;
+    }
     // spike bitmap: bit 2l / 2l+1 of the half-warp's word
-    const uint32_t b2 = (spk[r][0] ? 1u : 0u) | (spk[r][1] ? 2u : 0u);
+    const uint32_t b2 = (spk[0] ? 1u : 0u) | (spk[1] ? 2u : 0u);
     const uint32_t lo = __reduce_or_sync(0xffffffffu, lane < 16 ? (b2 << (2 * lane)) : 0u);
     const uint32_t hi = __reduce_or_sync(0xffffffffu, lane >= 16 ? (b2 << (2 * (lane - 16))) : 0u);
     if (lane == 0) {
@@ -448,93 +466,66 @@ __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
     }
   }
   __syncthreads();
-  if (tid == 0) {
-    uint32_t run = 0;
+  if (warp == 0) {
+    // tile-local exclusive offsets of the kPairs x kWarps (r, warp) groups
+    const uint32_t c = lane < kPairs * kWarps ? s_off[lane] : 0u;
+    uint32_t incl = c;
 #pragma unroll
-    for (int q = 0; q < 2 * kWarps; ++q) {
-      uint32_t c = s_off[q];
-      s_off[q] = run;
-      run += c;
+    for (int o = 1; o < kPairs * kWarps; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
     }
-    s_total_tile = run;
+    if (lane < kPairs * kWarps) s_off[lane] = incl - c;
+    if (lane == kPairs * kWarps - 1) {
+      s_total = incl;
+      d.tile_cnt[tile] = incl;
+    }
+  }
+  __syncthreads();
+  const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+  for (int r = 0; r < kPairs; ++r) {
+    const unsigned me = s_me[r * kWarps + warp], mo = s_mo[r * kWarps + warp];
+    const bool s0 = (me >> lane) & 1u, s1 = (mo >> lane) & 1u;
+    const uint32_t pre_cnt = __popc(me & lt) + __popc(mo & lt);
+    const uint32_t i0 = (uint32_t)(base + (uint64_t)r * 512 + 2 * (uint64_t)tid);
+    const uint32_t o = s_off[r * kWarps + warp] + pre_cnt;
+    if (s0) d.spk[base + o] = i0;
+    if (s1) d.spk[base + o + (s0 ? 1u : 0u)] = i0 + 1;
+  }
+  // last tile of the step: counters, FP64 clock, spike-log bookkeeping
+  if (tid == 0) {
+    if (s_total) atomicAdd(&d.ctl->spk_acc[k & 3], (unsigned long long)s_total);
     __threadfence();
-    // decoupled look-back over tiles in ticket order (bounded wait)
-    const uint32_t tag = (uint32_t)(k % 0x3FFFFFFFull) + 1u;
-    volatile unsigned long long* fl = d.flags;
-    uint32_t excl = 0;
-    if (tile == 0) {
-      fl[0] = flag_pack(tag, 2u, run);
-    } else {
-      fl[tile] = flag_pack(tag, 1u, run);
-      int64_t p = (int64_t)tile - 1;
-      uint32_t spins = 0;
-      while (p >= 0) {
-        unsigned long long f = fl[p];
-        uint32_t ft = (uint32_t)(f >> 34), fs = (uint32_t)(f >> 32) & 3u;
-        if (ft == tag && fs != 0u) {
-          excl += (uint32_t)f;
-          if (fs == 2u) break;
-          --p;
-        } else if (++spins > kSpinLimit) {
-          atomicOr(&d.ctl->status, kErrLookback);
-          break;
-        }
-      }
-      fl[tile] = flag_pack(tag, 2u, excl + run);
-    }
-    s_excl = excl;
+    const unsigned done = atomicAdd(&d.ctl->tiles_done, 1u);
+    s_last = (done == d.ntiles - 1) ? 1 : 0;
   }
   __syncthreads();
-  const uint32_t excl = s_excl;
-  const unsigned long long log_base = s_log_base;
-  const bool logging = s_logging != 0;
-  unsigned long long ev = 0;
-  uint32_t outs = 0;
-#pragma unroll
-  for (int r = 0; r < 2; ++r) {
-#pragma unroll
-    for (int e = 0; e < 2; ++e) {
-      if (spk[r][e]) {
-        const uint32_t i = (uint32_t)(idx0[r] + e);
-        const uint32_t pos = excl + s_off[r * kWarps + warp] + rank[r][e];
-        d.spk[pos] = i;
-        if (logging && log_base + pos < d.log_cap) d.log_idx[log_base + pos] = i;
-        ev += d.row_ptr[i + 1] - d.row_ptr[i];
-        if (d.outp[i]) ++outs;
-      }
-    }
-  }
-  // block sums of events and output spikes
-  for (int o = 16; o > 0; o >>= 1) {
-    ev += __shfl_down_sync(0xffffffffu, ev, o);
-    outs += __shfl_down_sync(0xffffffffu, outs, o);
-  }
-  if (lane == 0 && (ev | outs)) {
-    atomicAdd(&s_events, ev);
-    atomicAdd(&s_outs, outs);
-  }
-  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  if (d.ntiles > kSmemTiles) block_scan_u32(d.tile_cnt, d.tile_off, d.ntiles);
   if (tid == 0) {
-    if (s_events) atomicAdd(&d.ctl->events_total, s_events);
-    if (s_outs) atomicAdd(&d.ctl->out_total, (unsigned long long)s_outs);
-    if (tile == d.ntiles - 1) {
-      // the last tile in order holds the inclusive total of this step
-      const uint32_t total = excl + s_total_tile;
-      d.ctl->step_spikes[k & 3] = total;
-      d.ctl->spikes_total += total;
-      d.ctl->sim_time += d.dt;  // FP64 clock, engine.rs:388-389
-      if (logging) {
-        if (log_base + total <= d.log_cap) {
-          const unsigned long long s = d.ctl->log_steps;
-          if (s == 0) d.ctl->log_first = k;
-          d.log_off[s + 1] = log_base + total;
-          d.ctl->log_size = log_base + total;
-          d.ctl->log_steps = s + 1;
-        } else {
-          atomicOr(&d.ctl->status, kErrLogFull);
-        }
+    Ctl* c = d.ctl;
+    const unsigned long long total = atomicAdd(&c->spk_acc[k & 3], 0ull);
+    c->spk_acc[(k + 2) & 3] = 0ull;
+    c->tiles_done = 0u;
+    c->step_spikes[k & 3] = total;
+    c->spikes_total += total;
+    c->sim_time += d.dt;  // FP64 clock, engine.rs:388-389
+    unsigned ok = 0u;
+    if (d.log_idx != nullptr && c->log_steps < d.log_steps_cap && !(c->status & kErrLogFull)) {
+      if (c->log_size + total <= d.log_cap) {
+        const unsigned long long s = c->log_steps;
+        if (s == 0) c->log_first = k;
+        d.log_off[s + 1] = c->log_size + total;
+        c->log_size += total;
+        c->log_steps = s + 1;
+        ok = 1u;
+      } else {
+        atomicOr(&c->status, kErrLogFull);
       }
     }
+    c->log_ok[k & 3] = ok;
   }
 }
 
@@ -560,22 +551,58 @@ __device__ __forceinline__ void load_w4(const NsDev& d, bool bf16, uint64_t e0, 
 
 template <bool COND, bool BF16>
 __global__ void __launch_bounds__(256) k_propagate(NsDev d, uint32_t jstep) {
+  __shared__ uint32_t s_toff[kSmemTiles + 1];
+  __shared__ unsigned long long s_ev;
+  __shared__ uint32_t s_out;
   const int lane = threadIdx.x & 31;
   const uint64_t k = d.ctl->step_base + jstep;
   const uint32_t slot = (uint32_t)(k % d.D);
   const uint32_t cnt = (uint32_t)d.ctl->step_spikes[k & 3];
   const bool STDP = d.stdp != 0;
   const bool HOMEO = d.homeo != 0;
+  const bool small = d.ntiles <= kSmemTiles;
+  if (threadIdx.x == 0) { s_ev = 0ull; s_out = 0u; }
+  if (small && cnt) block_scan_u32(d.tile_cnt, s_toff, d.ntiles);
+  __syncthreads();
+  const uint32_t* toff = small ? s_toff : d.tile_off;
+  const bool log_ok = d.ctl->log_ok[k & 3] != 0u;
+  const unsigned long long log_base = log_ok ? d.ctl->log_size - cnt : 0ull;
   const uint32_t items = STDP ? 2u * cnt : cnt;
   const uint32_t wglob = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const uint32_t nw = gridDim.x * (blockDim.x >> 5);
+  unsigned long long ev = 0ull;
+  uint32_t outs = 0u;
   for (uint32_t item = wglob; item < items; item += nw) {
+    const uint32_t rank = item < cnt ? item : item - cnt;
+    // tile holding the rank-th spike: largest t with toff[t] <= rank
+    uint32_t lo = 0, hi = d.ntiles;
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (toff[mid] <= rank) lo = mid; else hi = mid;
+    }
+    const uint32_t j = __ldg(d.spk + (uint64_t)lo * kTile + (rank - toff[lo]));
     if (item < cnt) {
-      const uint32_t j = __ldg(d.spk + item);
       const uint64_t beg = __ldg(d.row_ptr + j), end = __ldg(d.row_ptr + j + 1);
       const uint8_t rp = STDP ? __ldg(d.row_plastic + j) : 0;
       const uint8_t rt = COND ? __ldg(d.row_type + j) : 0;
-      const float pj = (STDP && rp) ? d.pre[j] : 0.0f;
+      // spike bookkeeping of neuron j: log, last spike step, trace bump
+      float pj = 0.0f;
+      if (lane == 0) {
+        if (log_ok) d.log_idx[log_base + item] = j;
+        ev += end - beg;
+        outs += d.outp[j] ? 1u : 0u;
+        const long long lst = d.last[j];
+        d.last[j] = (long long)k;
+        if (STDP) {
+          const long long dk = lst < 0 ? -1 : (long long)k - lst;
+          const float fp = (dk >= 0 && (unsigned long long)dk < d.Kp) ? d.Ep[dk] : 0.0f;
+          const float fm = (dk >= 0 && (unsigned long long)dk < d.Km) ? d.Em[dk] : 0.0f;
+          pj = d.pre[j] * fp + 1.0f;
+          d.pre[j] = pj;
+          d.post[j] = d.qdec[j] * fm + 1.0f;
+        }
+      }
+      pj = __shfl_sync(0xffffffffu, pj, 0);
       const unsigned long long tbase = d.trace_pos ? d.trace_off[item] : 0ull;
       for (uint64_t b = beg & ~3ull; b < end; b += 128) {
         const uint64_t e0 = b + 4ull * lane;
@@ -648,22 +675,51 @@ __global__ void __launch_bounds__(256) k_propagate(NsDev d, uint32_t jstep) {
           }
         }
       }
-    } else if (STDP) {
-      const uint32_t i = __ldg(d.spk + (item - cnt));
+    } else {
+      const uint32_t i = j;
       const uint64_t b = __ldg(d.in_ptr + i), e = __ldg(d.in_ptr + i + 1);
-      for (uint64_t q = b + lane; q < e; q += 32) {
-        const uint2 sp = __ldg(d.in_list + q);
-        if (bit_of(d.bitmap, sp.x)) continue;  // handled by the source's row walk
-        const float pre = d.pre[sp.x];
-        if (BF16) {
-          const float w = bf16_bits_to_f32(d.w16[sp.y]);
-          d.w16[sp.y] = f32_to_bf16_bits(clampw(w + d.neg_a_minus * pre, d.w_min, d.w_max));
-        } else {
-          const float w = d.w32[sp.y];
-          d.w32[sp.y] = clampw(w + d.neg_a_minus * pre, d.w_min, d.w_max);
+      for (uint64_t q0 = b; q0 < e; q0 += 128) {
+        // issue every load of up to four entries per lane before any use
+        uint2 sp[4];
+        bool act[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const uint64_t q = q0 + lane + 32u * u;
+          act[u] = q < e;
+          sp[u] = act[u] ? __ldg(d.in_list + q) : make_uint2(0u, 0u);
+        }
+        float pre[4], wv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          // synapses whose source spiked are handled by the source's row walk
+          act[u] = act[u] && !bit_of(d.bitmap, sp[u].x);
+          pre[u] = act[u] ? d.pre[sp[u].x] : 0.0f;
+          if (BF16) wv[u] = act[u] ? bf16_bits_to_f32(d.w16[sp[u].y]) : 0.0f;
+          else wv[u] = act[u] ? d.w32[sp[u].y] : 0.0f;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          if (!act[u]) continue;
+          const float w1 = clampw(wv[u] + d.neg_a_minus * pre[u], d.w_min, d.w_max);
+          if (BF16) d.w16[sp[u].y] = f32_to_bf16_bits(w1);
+          else d.w32[sp[u].y] = w1;
         }
       }
     }
+  }
+  // block sums of synaptic events and output spikes
+  for (int o = 16; o > 0; o >>= 1) {
+    ev += __shfl_down_sync(0xffffffffu, ev, o);
+    outs += __shfl_down_sync(0xffffffffu, outs, o);
+  }
+  if (lane == 0 && (ev | outs)) {
+    atomicAdd(&s_ev, ev);
+    atomicAdd(&s_out, outs);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (s_ev) atomicAdd(&d.ctl->events_total, s_ev);
+    if (s_out) atomicAdd(&d.ctl->out_total, (unsigned long long)s_out);
   }
 }
 
@@ -674,26 +730,25 @@ __global__ void __launch_bounds__(256) k_propagate(NsDev d, uint32_t jstep) {
 // ---------------------------------------------------------------------------
 template <bool BF16>
 __global__ void __launch_bounds__(256) k_homeostasis(NsDev d, uint32_t jstep) {
-  const int lane = threadIdx.x & 31;
-  const uint32_t wglob = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const uint32_t nw = gridDim.x * (blockDim.x >> 5);
   (void)jstep;
-  for (uint64_t i = wglob; i < d.n; i += nw) {
+  // one thread per target; sums in ascending CSR position, as the reference
+  // walks synapses_by_target (engine.rs:86-92)
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < d.n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
     const double rate = d.rate[i];
     const double err = rate - d.h_target;
     const uint64_t b = d.all_in_ptr[i], e = d.all_in_ptr[i + 1];
     double sum = 0.0;
-    for (uint64_t q = b + lane; q < e; q += 32) sum += (double)d.contrib[d.all_in_pos[q]];
-    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    for (uint64_t q = b; q < e; ++q) sum += (double)d.contrib[d.all_in_pos[q]];
     const uint64_t cnt = e - b;
     if (cnt > 0 && sum >= 1e-12) {
       const double mean = sum / (double)cnt;
       const float nerr = (float)(-err);
-      for (uint64_t q = b + lane; q < e; q += 32) {
+      for (uint64_t q = b; q < e; ++q) {
         const uint32_t s = d.all_in_pos[q];
         const float rel = (float)((double)d.contrib[s] / mean);
         const float arg = nerr * rel * d.dt_f / d.h_tau_f;
-        const float scale = expf(arg);
+        const float scale = exp_f(arg);
         if (BF16) {
           const float w = bf16_bits_to_f32(d.w16[s]) * scale;
           d.w16[s] = f32_to_bf16_bits(clampw(w, 0.0f, 10.0f));
@@ -702,27 +757,28 @@ __global__ void __launch_bounds__(256) k_homeostasis(NsDev d, uint32_t jstep) {
         }
       }
     }
-    if (lane == 0) {
-      const double inst = bit_of(d.bitmap, (uint32_t)i) ? 1000.0 / d.dt : 0.0;
-      d.rate[i] = rate + (inst - rate) * d.dt / 100.0;
-    }
+    const double inst = bit_of(d.bitmap, (uint32_t)i) ? 1000.0 / d.dt : 0.0;
+    d.rate[i] = rate + (inst - rate) * d.dt / 100.0;
   }
 }
 
 __global__ void k_advance(Ctl* ctl, uint32_t steps) { ctl->step_base += steps; }
 
-// exclusive scan of out-degrees of this step's spikers (traced step only)
+// exclusive scan of out-degrees of this step's spikers in ascending order
+// (traced step only): walks the tile-local lists in tile order
 __global__ void k_trace_offsets(NsDev d, unsigned long long* off) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  const uint64_t k = d.ctl->step_base;
-  const uint32_t cnt = (uint32_t)d.ctl->step_spikes[k & 3];
   unsigned long long run = 0;
-  for (uint32_t q = 0; q < cnt; ++q) {
-    off[q] = run;
-    const uint32_t j = d.spk[q];
-    run += d.row_ptr[j + 1] - d.row_ptr[j];
+  uint32_t q = 0;
+  for (uint32_t t = 0; t < d.ntiles; ++t) {
+    const uint32_t c = d.tile_cnt[t];
+    for (uint32_t l = 0; l < c; ++l) {
+      off[q++] = run;
+      const uint32_t j = d.spk[(uint64_t)t * kTile + l];
+      run += d.row_ptr[j + 1] - d.row_ptr[j];
+    }
   }
-  off[cnt] = run;
+  off[q] = run;
 }
 
 }  // namespace ns

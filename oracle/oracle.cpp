@@ -105,6 +105,30 @@ inline void own_sincos2pi(float u, float* sn, float* cs) {
   }
 }
 
+// e^x in float for the homeostatic scale: Cody-Waite reduction with a
+// 16-bit head of ln2, Taylor series of e^r to r^7, scaling by 2^n.
+inline float own_expf(float x) {
+  if (x > 88.0f) x = 88.0f;
+  if (x < -87.0f) x = -87.0f;
+  const float nf = std::floor(x * 1.44269504f + 0.5f);
+  float r = x - nf * 0.693145752f;
+  r = r - nf * 1.42860677e-06f;
+  float p = 1.98412698e-04f;
+  p = 1.38888889e-03f + r * p;
+  p = 8.33333333e-03f + r * p;
+  p = 4.16666667e-02f + r * p;
+  p = 1.66666667e-01f + r * p;
+  p = 0.5f + r * p;
+  p = 1.0f + r * p;
+  p = 1.0f + r * p;
+  const uint32_t eb = (uint32_t)((int)nf + 127) << 23;
+  float sc;
+  std::memcpy(&sc, &eb, 4);
+  return p * sc;
+}
+template <class R> inline R scale_exp(R x) { return std::exp(x); }
+template <> inline float scale_exp<float>(float x) { return own_expf(x); }
+
 inline uint16_t f32_to_bf16_rne(float f) {
   uint32_t b;
   std::memcpy(&b, &f, 4);
@@ -621,7 +645,7 @@ template <class R> struct Fast {
           uint64_t s = all_in_pos[q];
           R rel = (R)((double)contrib[s] / mean);
           R arg = (R)(-err) * rel * (R)c.dt / (R)c.h_tau;
-          R scale = std::exp(arg);
+          R scale = scale_exp<R>(arg);
           R ws = wget(s) * scale;
           wset(s, clampw<R>(ws, R(0), R(10)));
         }
@@ -943,6 +967,7 @@ void or_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out
   philox(ctr, key, out);
 }
 float or_logf(float x) { return own_logf(x); }
+float or_expf(float x) { return own_expf(x); }
 void or_sincos2pi(float u, float* s, float* c) { own_sincos2pi(u, s, c); }
 
 float or_drive_f32(const or_config* cfg, uint64_t n, const uint8_t* inhibitory, uint64_t i,

@@ -74,6 +74,7 @@ typedef struct or_net {
 /* ---- Philox4x32-10 and drive math (restated) ---- */
 void or_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 float or_logf(float x);
+float or_expf(float x);
 void or_sincos2pi(float u, float* s, float* c);
 /* drive value of neuron i at step k as the float engine computes it
  * (current added; for POISSON_KICK the kick) */

@@ -58,6 +58,7 @@ def load():
     sig = {
         "or_philox4x32_10": (None, [vp, vp, vp]),
         "or_logf": (C.c_float, [C.c_float]),
+        "or_expf": (C.c_float, [C.c_float]),
         "or_sincos2pi": (None, [C.c_float, vp, vp]),
         "or_drive_f32": (C.c_float, [C.POINTER(OrConfig), u64, vp, u64, u64, C.c_float]),
         "or_lif_step_f64": (C.c_int, [vp, vp, vp, C.c_double, C.c_double]),

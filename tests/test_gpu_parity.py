@@ -143,15 +143,31 @@ def test_hh_rush_larsen_network_tracks_fp64(lib):
 
 
 def test_bf16_weight_error_vs_fp64(lib):
-    # BF16 storage vs FP64 weights over 200 steps of STDP: the stated error
+    # The stated BF16 error. (1) Storage: every weight is its f32 value
+    # rounded to 8 significant bits, |w_bf16 - w| <= 2^-8 |w|. (2) One step
+    # of STDP from the same state: the BF16 weights stay within one BF16
+    # rounding of the FP64 update. (3) Over 300 steps the chaotic dynamics
+    # take another spike path, so the comparison is statistical: mean rate
+    # within 5%, weight mean within 1% and std within 2% of the FP64 run.
     net, cfg, drive = nets.izh_stdp(n=10_000, k=100, wf=A.WEIGHT_BF16)
-    eng = gpu_run(net, cfg, drive, 50)
+    eng = SimulationEngine(net, cfg, drive)
+    w0 = eng.download_state()["w"].astype(np.float64)
+    # 8 significant bits: unit roundoff 2^-8
+    assert np.all(np.abs(w0 - net.w) <= np.abs(net.w) * 2.0 ** -8)
+    eng.run(1)
     o = FastOracle(net, cfg, drive, precision=64)
-    o.step(50)
+    o.step(1)
+    w1, w64 = eng.download_state()["w"].astype(np.float64), o.weights()
+    # initial rounding plus the rounding of the stored result
+    assert np.all(np.abs(w1 - w64) <= 2.0 ** -8 * (np.abs(net.w) + np.abs(w64)) * 1.01 + 1e-7)
+    eng.run(299)
+    o.step(299)
     w_gpu, w64 = eng.download_state()["w"].astype(np.float64), o.weights()
-    err = np.abs(w_gpu - w64)
-    # bf16 keeps 8 significant bits: relative rounding 2^-9 per store
-    assert np.all(err <= np.abs(w64) * 2.0 ** -8 + 0.02)
+    spk_gpu = eng.counters()[1]
+    spk_64 = len(o.raster()[0])
+    assert abs(spk_gpu - spk_64) <= 0.05 * spk_64
+    assert abs(w_gpu.mean() - w64.mean()) <= 0.01 * abs(w64.mean())
+    assert abs(w_gpu.std() - w64.std()) <= 0.02 * w64.std()
 
 
 def single(model, params, v0, I0, dt, steps, u0=None, decay=1.0, hh_int=A.HH_EULER_REF, m0=None):

@@ -38,6 +38,13 @@ def test_drive_log_and_sincos_accuracy(oracle_lib):
         assert abs(s.value - np.sin(a)) < 3e-7 and abs(c.value - np.cos(a)) < 3e-7
 
 
+def test_homeostasis_exp_accuracy(oracle_lib):
+    xs = np.concatenate([np.linspace(-20, 20, 4001), np.random.default_rng(2).normal(0, 1e-3, 2000)])
+    for x in xs.astype(np.float32):
+        ref = np.exp(np.float64(x))
+        assert abs(oracle_lib.or_expf(float(x)) - ref) <= 4e-7 * ref
+
+
 def test_gauss_drive_statistics(oracle_lib):
     from oracle.oracle import make_config
     from neuralsim_b200 import Drive, SimConfig
