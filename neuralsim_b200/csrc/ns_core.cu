@@ -592,7 +592,7 @@ ns_status ns_upload_neurons(ns_handle* h, const ns_neuron_soa* s) {
 #define DA(ptr, cnt) if ((st = dalloc(h, B, &(ptr), (cnt)))) return st;
   DA(d.v, np) DA(d.u, np) DA(d.I, np) DA(d.gm, np) DA(d.gh, np) DA(d.gn, np)
   DA(d.refr, np) DA(d.refr_steps, np) DA(d.inh, np) DA(d.outp, np)
-  DA(d.pre, np) DA(d.post, np) DA(d.qdec, np) DA(d.last, np) DA(d.rate, np)
+  DA(d.pre, np) DA(d.post, np) DA(d.rec, np) DA(d.last, np) DA(d.rate, np)
   for (int q = 0; q < 7; ++q) d.par[q] = nullptr;
   for (int q = 0; q < npar; ++q) DA(d.par[q], np)
   for (int t = 0; t < 4; ++t) DA(d.G[t], np)

@@ -67,7 +67,8 @@ struct NsDev {
   float* par[7];
   int32_t* refr_steps;
   uint8_t *inh, *outp;
-  float *pre, *post, *qdec;
+  float *pre, *post;
+  float2* rec;                     // per step: {decayed pre, decayed post}, sign bit = spiked
   long long* last;
   double* rate;
   float* G[4];
@@ -422,15 +423,17 @@ __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
     }
     // ---- traces: per-step decay here; the spike-time bump (double decay of
     // StdpTrace, src/synapse/plasticity.rs:144-159) is done by the spiker's
-    // own row walk in k_propagate. qdec keeps the decayed, pre-bump post
-    // trace that LTP of a synapse whose target also spiked must see.
+    // own row walk in k_propagate. rec[i] carries this step's decayed,
+    // pre-bump traces with the sign bit set when i spiked: the one value a
+    // synapse's LTP (target side) or LTD (source side) needs.
     if (d.stdp) {
       const float pv0 = p2.x * d.ep, pv1 = p2.y * d.ep;
       const float qv0 = q2.x * d.em, qv1 = q2.y * d.em;
       *reinterpret_cast<float2*>(d.pre + i0) = make_float2(pv0, pv1);
       *reinterpret_cast<float2*>(d.post + i0) = make_float2(qv0, qv1);
-      if (spk[0]) d.qdec[i0] = qv0;
-      if (spk[1]) d.qdec[i0 + 1] = qv1;
+      const float4 rr = make_float4(spk[0] ? -pv0 : pv0, spk[0] ? -qv0 : qv0,
+                                    spk[1] ? -pv1 : pv1, spk[1] ? -qv1 : qv1);
+      *reinterpret_cast<float4*>(d.rec + i0) = rr;
     }
     // ---- write back state ----
     *reinterpret_cast<float2*>(d.v + i0) = make_float2(st[0].v, st[1].v);
@@ -530,27 +533,35 @@ __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
 }
 
 // ---------------------------------------------------------------------------
-// Kernel 2: propagation (+LTP) over spiking rows, then LTD over spiking
-// targets' plastic incoming synapses. Work items: [0, cnt) rows, [cnt, 2cnt)
-// incoming lists; one warp per item, grid-stride. Writes are disjoint: rows
-// of spiking sources (LTP, and LTP+LTD when the target spiked too) versus
-// incoming synapses whose source did not spike (LTD).
+// Kernel 2: one warp per spike j (grid-stride over the step's spikes). The
+// warp walks j's CSR row — coalesced 16-byte loads of column indices and
+// weights, int64 fixed-point atomicAdd into each target's delay slot, LTP
+// fused into the walk (engine.rs:414-473, :496-537) — and j's plastic
+// incoming list (LTD for synapses whose source did not spike). Both lists are
+// walked in 128-entry chunks whose loads are all issued before any use, so a
+// spike costs about four dependent memory round trips. Writes are disjoint:
+// row synapses of spiking sources (LTP, and LTP then LTD when the target
+// spiked too) versus incoming synapses of spiking targets whose source did
+// not spike (LTD). The spike's own bookkeeping (ordered log entry, last spike
+// step, trace bump) is done by the same warp.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void load_w4(const NsDev& d, bool bf16, uint64_t e0, float w[4]) {
   if (bf16) {
-    uint2 raw = *reinterpret_cast<const uint2*>(d.w16 + e0);
+    const uint2 raw = *reinterpret_cast<const uint2*>(d.w16 + e0);
     w[0] = bf16_bits_to_f32((uint16_t)(raw.x & 0xffffu));
     w[1] = bf16_bits_to_f32((uint16_t)(raw.x >> 16));
     w[2] = bf16_bits_to_f32((uint16_t)(raw.y & 0xffffu));
     w[3] = bf16_bits_to_f32((uint16_t)(raw.y >> 16));
   } else {
-    float4 f = *reinterpret_cast<const float4*>(d.w32 + e0);
+    const float4 f = *reinterpret_cast<const float4*>(d.w32 + e0);
     w[0] = f.x; w[1] = f.y; w[2] = f.z; w[3] = f.w;
   }
 }
 
+__device__ __forceinline__ bool neg(float x) { return (__float_as_uint(x) >> 31) != 0u; }
+
 template <bool COND, bool BF16>
-__global__ void __launch_bounds__(256) k_propagate(NsDev d, uint32_t jstep) {
+__global__ void __launch_bounds__(256, 5) k_propagate(NsDev d, uint32_t jstep) {
   __shared__ uint32_t s_toff[kSmemTiles + 1];
   __shared__ unsigned long long s_ev;
   __shared__ uint32_t s_out;
@@ -582,48 +593,60 @@ __global__ void __launch_bounds__(256) k_propagate(NsDev d, uint32_t jstep) {
     }
     const uint32_t j = __ldg(d.spk + (uint64_t)lo * kTile + (rank - toff[lo]));
     if (item < cnt) {
+      // ---------------- row walk of spiking source j ----------------
       const uint64_t beg = __ldg(d.row_ptr + j), end = __ldg(d.row_ptr + j + 1);
       const uint8_t rp = STDP ? __ldg(d.row_plastic + j) : 0;
       const uint8_t rt = COND ? __ldg(d.row_type + j) : 0;
-      // spike bookkeeping of neuron j: log, last spike step, trace bump
       float pj = 0.0f;
       if (lane == 0) {
+        const long long lst = d.last[j];
         if (log_ok) d.log_idx[log_base + item] = j;
         ev += end - beg;
         outs += d.outp[j] ? 1u : 0u;
-        const long long lst = d.last[j];
         d.last[j] = (long long)k;
         if (STDP) {
+          // spike-time trace bump: trace * exp(-(t - t_last)/tau) + 1
+          const float2 rj = d.rec[j];
           const long long dk = lst < 0 ? -1 : (long long)k - lst;
           const float fp = (dk >= 0 && (unsigned long long)dk < d.Kp) ? d.Ep[dk] : 0.0f;
           const float fm = (dk >= 0 && (unsigned long long)dk < d.Km) ? d.Em[dk] : 0.0f;
-          pj = d.pre[j] * fp + 1.0f;
+          pj = fabsf(rj.x) * fp + 1.0f;
           d.pre[j] = pj;
-          d.post[j] = d.qdec[j] * fm + 1.0f;
+          d.post[j] = fabsf(rj.y) * fm + 1.0f;
         }
       }
-      pj = __shfl_sync(0xffffffffu, pj, 0);
       const unsigned long long tbase = d.trace_pos ? d.trace_off[item] : 0ull;
-      for (uint64_t b = beg & ~3ull; b < end; b += 128) {
-        const uint64_t e0 = b + 4ull * lane;
-        if (e0 >= end || e0 + 4 <= beg) continue;
-        const uint4 c4 = __ldg(reinterpret_cast<const uint4*>(d.col + e0));
+      const uint64_t rb = beg & ~3ull;
+      const uint32_t nrow = end > beg ? (uint32_t)((end - rb + 127) >> 7) : 0u;
+      for (uint32_t c = 0; c < nrow; ++c) {
+        const uint64_t e0 = rb + 128ull * c + 4ull * lane;
+        const bool rv = e0 < end && e0 + 4 > beg;
+        uint4 c4 = make_uint4(0u, 0u, 0u, 0u);
+        float w[4] = {0.f, 0.f, 0.f, 0.f};
+        if (rv) {
+          c4 = __ldg(reinterpret_cast<const uint4*>(d.col + e0));
+          load_w4(d, BF16, e0, w);
+        }
         const uint32_t cc[4] = {c4.x, c4.y, c4.z, c4.w};
-        float w[4];
-        load_w4(d, BF16, e0, w);
-        float wn[4] = {w[0], w[1], w[2], w[3]};
-        bool inr[4], chg[4];
+        bool inr[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) inr[q] = rv && (e0 + q >= beg) && (e0 + q < end);
+        // target records for LTP, gathered before the atomics are issued
+        bool pl[4] = {false, false, false, false};
+        float2 tr[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-          const uint64_t e = e0 + q;
-          inr[q] = (e >= beg) && (e < end);
-          chg[q] = false;
+          pl[q] = STDP && rp && inr[q] && (rp == 1 || __ldg(d.plastic + e0 + q));
+          tr[q] = pl[q] ? d.rec[cc[q]] : make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
           if (!inr[q]) continue;
-          const uint32_t i = cc[q];
-          int t = 0;
-          if (COND) t = (rt == 255) ? (int)__ldg(d.type + e) : (int)rt;
-          const float val = (COND && (t == 1 || t == 2)) ? fabsf(w[q]) : w[q];
-          atomicAdd(d.acc + ((uint64_t)t * d.D + slot) * d.n_pad + i,
+          const uint64_t e = e0 + q;
+          int ty = 0;
+          if (COND) ty = (rt == 255) ? (int)__ldg(d.type + e) : (int)rt;
+          const float val = (COND && (ty == 1 || ty == 2)) ? fabsf(w[q]) : w[q];
+          atomicAdd(d.acc + ((uint64_t)ty * d.D + slot) * d.n_pad + cc[q],
                     (unsigned long long)to_fix(val));
           if (d.trace_pos) {
             const unsigned long long tp = tbase + (e - beg);
@@ -632,74 +655,76 @@ __global__ void __launch_bounds__(256) k_propagate(NsDev d, uint32_t jstep) {
           if (HOMEO) {
             float mag;
             if (COND) {
-              float g = w[q] * kSyn[t].gmax;
-              if (kSyn[t].mg) g = g * (1.0f / (1.0f + (1.0f / 3.57f) * expf(-0.062f * d.v[i])));
+              float g = w[q] * kSyn[ty].gmax;
+              if (kSyn[ty].mg) g = g * (1.0f / (1.0f + (1.0f / 3.57f) * expf(-0.062f * d.v[cc[q]])));
               mag = fabsf(g);
             } else {
               mag = fabsf(w[q]);
             }
             d.contrib[e] = d.contrib[e] * d.cd + mag * d.one_m_cd;
           }
-          if (STDP && rp && (rp == 1 || __ldg(d.plastic + e))) {
-            float w1;
-            if (!bit_of(d.bitmap, i)) {
-              w1 = clampw(w[q] + d.a_plus * d.post[i], d.w_min, d.w_max);
-            } else {
-              w1 = clampw(w[q] + d.a_plus * d.qdec[i], d.w_min, d.w_max);
-              w1 = clampw(w1 + d.neg_a_minus * pj, d.w_min, d.w_max);
-            }
-            wn[q] = w1;
-            chg[q] = true;
-          }
         }
         if (STDP && rp) {
-          if (BF16) {
-            if (chg[0] && chg[1] && chg[2] && chg[3]) {
-              uint2 raw;
-              raw.x = (uint32_t)f32_to_bf16_bits(wn[0]) | ((uint32_t)f32_to_bf16_bits(wn[1]) << 16);
-              raw.y = (uint32_t)f32_to_bf16_bits(wn[2]) | ((uint32_t)f32_to_bf16_bits(wn[3]) << 16);
-              *reinterpret_cast<uint2*>(d.w16 + e0) = raw;
-            } else {
+          pj = __shfl_sync(0xffffffffu, pj, 0);
+          // LTP, then LTD when the target spiked in this step too
+          float wn[4];
+          bool chg = false, all4 = true;
 #pragma unroll
-              for (int q = 0; q < 4; ++q)
-                if (chg[q]) d.w16[e0 + q] = f32_to_bf16_bits(wn[q]);
-            }
-          } else {
-            if (chg[0] && chg[1] && chg[2] && chg[3]) {
-              *reinterpret_cast<float4*>(d.w32 + e0) = make_float4(wn[0], wn[1], wn[2], wn[3]);
-            } else {
+          for (int q = 0; q < 4; ++q) {
+            wn[q] = w[q];
+            if (!pl[q]) { all4 = false; continue; }
+            float w1 = clampw(w[q] + d.a_plus * fabsf(tr[q].y), d.w_min, d.w_max);
+            if (neg(tr[q].y)) w1 = clampw(w1 + d.neg_a_minus * pj, d.w_min, d.w_max);
+            wn[q] = w1;
+            chg = true;
+          }
+          if (chg) {
+            if (BF16) {
+              if (all4) {
+                uint2 raw;
+                raw.x = (uint32_t)f32_to_bf16_bits(wn[0]) | ((uint32_t)f32_to_bf16_bits(wn[1]) << 16);
+                raw.y = (uint32_t)f32_to_bf16_bits(wn[2]) | ((uint32_t)f32_to_bf16_bits(wn[3]) << 16);
+                *reinterpret_cast<uint2*>(d.w16 + e0) = raw;
+              } else {
 #pragma unroll
-              for (int q = 0; q < 4; ++q)
-                if (chg[q]) d.w32[e0 + q] = wn[q];
+                for (int q = 0; q < 4; ++q)
+                  if (pl[q]) d.w16[e0 + q] = f32_to_bf16_bits(wn[q]);
+              }
+            } else {
+              if (all4) {
+                *reinterpret_cast<float4*>(d.w32 + e0) = make_float4(wn[0], wn[1], wn[2], wn[3]);
+              } else {
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                  if (pl[q]) d.w32[e0 + q] = wn[q];
+              }
             }
           }
         }
       }
     } else {
-      const uint32_t i = j;
-      const uint64_t b = __ldg(d.in_ptr + i), e = __ldg(d.in_ptr + i + 1);
-      for (uint64_t q0 = b; q0 < e; q0 += 128) {
-        // issue every load of up to four entries per lane before any use
+      // ------------- LTD over spiking target j's plastic inputs -------------
+      const uint64_t ib = __ldg(d.in_ptr + j), ie = __ldg(d.in_ptr + j + 1);
+      for (uint64_t q0 = ib; q0 < ie; q0 += 128) {
         uint2 sp[4];
         bool act[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
           const uint64_t q = q0 + lane + 32u * u;
-          act[u] = q < e;
+          act[u] = q < ie;
           sp[u] = act[u] ? __ldg(d.in_list + q) : make_uint2(0u, 0u);
         }
         float pre[4], wv[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-          // synapses whose source spiked are handled by the source's row walk
-          act[u] = act[u] && !bit_of(d.bitmap, sp[u].x);
-          pre[u] = act[u] ? d.pre[sp[u].x] : 0.0f;
+          pre[u] = act[u] ? d.rec[sp[u].x].x : 0.0f;
           if (BF16) wv[u] = act[u] ? bf16_bits_to_f32(d.w16[sp[u].y]) : 0.0f;
           else wv[u] = act[u] ? d.w32[sp[u].y] : 0.0f;
         }
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-          if (!act[u]) continue;
+          // synapses whose source spiked too are handled by the source's row walk
+          if (!act[u] || neg(pre[u])) continue;
           const float w1 = clampw(wv[u] + d.neg_a_minus * pre[u], d.w_min, d.w_max);
           if (BF16) d.w16[sp[u].y] = f32_to_bf16_bits(w1);
           else d.w32[sp[u].y] = w1;
