@@ -64,13 +64,14 @@ def peaks():
     return 6650.0, "fallback 6.65 TB/s (no MEASURED_PEAKS.json)"
 
 
-def profile_traffic():
-    """DRAM bytes per launch of the neuron kernel from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "k_neuron_izh_c2_ncu.md")
+def profile_traffic(kernel):
+    """DRAM bytes (read + write) per launch of `kernel` from the committed ncu
+    summary of the full-size workload, or None."""
+    path = os.path.join(ROOT, "profiles", "izh_c2_step_kernels_ncu.md")
     if not os.path.exists(path):
         return None
     for line in open(path):
-        if line.startswith("traffic_bytes_per_launch_full_size:"):
+        if line.startswith(f"traffic_bytes_per_launch_{kernel}:"):
             try:
                 return float(line.split(":", 1)[1].strip().split()[0])
             except ValueError:
@@ -141,10 +142,24 @@ def step_bytes(n, sim_steps, spikes, events, in_plastic):
     return 64.0 * n * sim_steps + 16.0 * spikes + 8.0 * events + 8.0 * in_plastic
 
 
-def neuron_kernel_bytes(n, spikes):
-    """Algorithmic bytes of one neuron-kernel launch: 64 N plus per spike the
-    spike index 4, last-spike step r/w 16, pre-bump trace 4, row_ptr pair 16."""
-    return 64.0 * n + 40.0 * spikes
+def kernel_bytes(n, spikes, events, in_plastic):
+    """Algorithmic HBM bytes per launch of each step kernel (one step):
+    neuron: 64 N (v,u r/w; a,b,c,d; int64 accumulator read + zero; pre/post
+            traces r/w) + 4 S (spike index);
+    rows:   16 S (row_ptr pair) + 24 S (last r/w, trace bump r/w)
+            + 8 E_out (column 4, bf16 weight read 2 and LTP write 2);
+    ltd:    16 S (incoming pointer pair) + 8 E_in,plastic (incoming entry
+            4 of the 8 B (source, position) pair counted as in the plan's
+            formula, bf16 weight read 2 + write 2).
+    Accumulator atomics and trace-record gathers hit L2-resident arrays and
+    count as 0 HBM bytes. `sector_bytes` counts the 32-byte DRAM sector that a
+    random 2-byte weight access moves (read + write) for the LTD."""
+    return {
+        "neuron": 64.0 * n + 4.0 * spikes,
+        "rows": 40.0 * spikes + 8.0 * events,
+        "ltd": 16.0 * spikes + 8.0 * in_plastic,
+        "ltd_sector": 16.0 * spikes + (8.0 + 64.0) * in_plastic,
+    }
 
 
 def run_ours(a):
@@ -192,16 +207,19 @@ def run_ours(a):
     ms = ev0.elapsed_time(ev1)
     c1 = eng.counters()
     launches = eng.launch_count() - l0
+    sched, sched_us = eng.schedule()
     events = c1[3] - c0[3]
     spikes = c1[1] - c0[1]
     sim_steps = c1[0] - c0[0]
     clocks = clk.summary()
 
-    # per-kernel device time (eager steps with events around each kernel)
+    # per-kernel device time (eager serial steps with events around each kernel)
     pc0 = eng.counters()
     prof = eng.profile_steps(200)
     pc1 = eng.counters()
-    prof_spikes = (pc1[1] - pc0[1]) / 200.0
+    prof_steps = 200.0
+    prof_spikes = (pc1[1] - pc0[1]) / prof_steps
+    prof_events = (pc1[3] - pc0[3]) / prof_steps
 
     # whole-step algorithmic bytes: plastic in-degree of the spikers is
     # estimated from the mean (80 of 100 incoming synapses are plastic)
@@ -228,12 +246,22 @@ def run_ours(a):
 
     if rank == 0:
         peak, peak_src = peaks()
-        nk_ms, nk_launches = prof["neuron"]
-        nk_avg_s = nk_ms / nk_launches / 1e3
-        nk_bytes = neuron_kernel_bytes(net.n, prof_spikes)
-        achieved = nk_bytes / nk_avg_s / 1e9
+        kb = kernel_bytes(net.n, prof_spikes, prof_events, prof_spikes * mean_in_plastic)
         total_prof_ms = sum(v[0] for v in prof.values())
-        traffic = profile_traffic()
+        kernels = {}
+        for name, (kms, kl) in prof.items():
+            avg_s = kms / kl / 1e3
+            kernels[name] = {"avg_launch_us": avg_s * 1e6, "share": kms / total_prof_ms,
+                             "bytes_per_launch": kb.get(name),
+                             "achieved_gbs": kb[name] / avg_s / 1e9 if name in kb else None}
+        if "ltd" in kernels:
+            kernels["ltd"]["sector_bytes_per_launch"] = kb["ltd_sector"]
+            kernels["ltd"]["sector_gbs"] = kb["ltd_sector"] / (kernels["ltd"]["avg_launch_us"] / 1e6) / 1e9
+        dom = max(kernels, key=lambda k: kernels[k]["share"])
+        nk_bytes = kb[dom]
+        nk_avg_s = kernels[dom]["avg_launch_us"] / 1e6
+        achieved = nk_bytes / nk_avg_s / 1e9
+        traffic = profile_traffic(dom)
         value = events_all / (ms_max / 1e3)
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -249,15 +277,17 @@ def run_ours(a):
                 "events_per_sim_step": events / max(sim_steps, 1),
                 "sim_time_per_wall_s": (sim_steps * cfg.dt_ms / 1e3) / (ms / 1e3),
                 "network_build_s": round(gen_s, 2),
+                "step_schedule": {1: "fused", 2: "split (LTD beside next neuron update)",
+                                  3: "fused, 4 blocks/SM",
+                                  4: "split, narrow LTD grid"}.get(sched, "undecided"),
+                "autotune_us_per_step": sched_us,
             },
             "roofline": {
                 "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic,
-                "kernel": "k_neuron<IZHIKEVICH,RESET_EACH_STEP>",
-                "bytes_per_launch": nk_bytes, "avg_launch_us": nk_avg_s * 1e6,
-                "peak_source": peak_src,
-                "kernel_share": {k: v[0] / total_prof_ms for k, v in prof.items()},
-                "kernel_avg_us": {k: v[0] / v[1] * 1e3 for k, v in prof.items()},
+                "kernel": dom, "bytes_per_launch": nk_bytes, "avg_launch_us": nk_avg_s * 1e6,
+                "peak_source": peak_src, "spikes_per_step_profiled": prof_spikes,
+                "kernels": kernels,
             },
             "step_roofline": {
                 "algorithmic_bytes_per_sim_step": bytes_total / max(sim_steps, 1),

@@ -136,6 +136,13 @@ typedef struct ns_config {
   uint64_t spike_log_capacity; /* indices held; 0 = no log */
   uint32_t spike_log_steps;    /* steps held */
   uint32_t graph_chunk;        /* steps per captured CUDA graph; 0 = 1000 */
+  /* kernel schedule of a step: 0 = autotune (time every candidate on live
+   * steps, keep the fastest), 1 = fused (row walks and LTD lists in one
+   * kernel, 6 resident blocks per SM), 2 = split (LTD of step k on a second
+   * stream beside the neuron update of step k+1), 3 = fused with 4 resident
+   * blocks per SM, 4 = split with a narrow (2 blocks/SM) LTD grid that leaves
+   * room for the neuron kernel. All give bit-identical results. */
+  uint32_t step_schedule;
 } ns_config;
 
 /* Fills cfg with the reference defaults: LIF, DIRECT_DECAY, dt 0.5 ms
@@ -233,6 +240,10 @@ ns_status ns_weight_stats(ns_handle* h, double* mean, double* stddev);
  *     CSR order). For parity tests of the CSR walk. */
 ns_status ns_step_traced(ns_handle* h, uint64_t* pos_out, uint64_t cap, uint64_t* n_events);
 
+/* Schedule in use (0 while the autotuner has not decided) and the measured
+ * microseconds per step of schedules 1..4 in us_per_step[4] (0 if untimed). */
+ns_status ns_get_schedule(ns_handle* h, uint32_t* schedule, double* us_per_step);
+
 /* Kernel launches issued by this handle since creation (own kernels only). */
 ns_status ns_launch_count(ns_handle* h, uint64_t* launches);
 
@@ -244,9 +255,9 @@ ns_status ns_counters(ns_handle* h, uint64_t out[4]);
  * so a caller can record its own CUDA events around ns_step. */
 ns_status ns_get_stream(ns_handle* h, void** stream);
 
-/* Runs n_steps eagerly with CUDA events around every kernel; adds the device
- * time (ms) and the launch count of the neuron, propagation and homeostasis
- * kernels to kernel_ms[3] / launches[3]. Same numerics as ns_step. */
+/* Runs n_steps eagerly and serially with CUDA events around every kernel;
+ * adds the device time (ms) and launch count of the neuron, row-walk, LTD and
+ * homeostasis kernels to kernel_ms[4] / launches[4]. Same numerics as ns_step. */
 ns_status ns_profile_steps(ns_handle* h, uint32_t n_steps, double* kernel_ms, uint64_t* launches);
 
 #ifdef __cplusplus

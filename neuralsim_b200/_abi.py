@@ -38,6 +38,7 @@ class NsConfig(C.Structure):
         ("homeostatic_target_rate", C.c_double), ("homeostatic_tau", C.c_double),
         ("contribution_tau", C.c_double), ("spike_log_capacity", C.c_uint64),
         ("spike_log_steps", C.c_uint32), ("graph_chunk", C.c_uint32),
+        ("step_schedule", C.c_uint32),
     ]
 
 
@@ -92,6 +93,7 @@ SIGNATURES = {
     "ns_weight_stats": (C.c_int32, [_P, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "ns_step_traced": (C.c_int32, [_P, _P, C.c_uint64, _U64P]),
     "ns_launch_count": (C.c_int32, [_P, _U64P]),
+    "ns_get_schedule": (C.c_int32, [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_double)]),
     "ns_get_stream": (C.c_int32, [_P, C.POINTER(_P)]),
     "ns_counters": (C.c_int32, [_P, _U64P]),
     "ns_profile_steps": (C.c_int32, [_P, C.c_uint32, C.POINTER(C.c_double), _U64P]),

@@ -23,6 +23,8 @@ struct ns_handle {
   int dev = 0;
   int sms = 148;
   cudaStream_t st = nullptr;
+  cudaStream_t st2 = nullptr;       // LTD of step k beside the neuron kernel of step k+1
+  cudaEvent_t ev_rows = nullptr, ev_ltd = nullptr;
   std::string err;
   bool have_neurons = false, have_csr = false;
   uint64_t n = 0, n_pad = 0, m = 0, m_pad = 0;
@@ -30,9 +32,16 @@ struct ns_handle {
   NsDev d{};
   ns::Ctl* ctl = nullptr;
   std::vector<void*> neuron_allocs, csr_allocs, log_allocs;
+  std::map<void*, size_t> alloc_bytes;   // size of every allocation made by dalloc
+  uint64_t next_tune_step = 0;          // autotuner runs at step 0 and once after 2000
   std::map<uint32_t, cudaGraphExec_t> graphs;
   uint64_t launches = 0;
   int prop_blocks = 0;
+  int fused_blocks[2] = {0, 0};
+  int ltd_blocks = 0;
+  int ltd_narrow_blocks = 0;
+  uint32_t sched = 0;               // 1 fused, 2 split, 3 fused (4 blocks/SM), 4 split (narrow LTD); 0 = undecided
+  double tune_us[5] = {0, 0, 0, 0, 0};
   int homeo_blocks = 0;
   int ntypes_acc = 1;
 };
@@ -65,6 +74,7 @@ template <class T> ns_status dalloc(ns_handle* h, std::vector<void*>& bag, T** p
   e = cudaMemsetAsync(q, 0, bytes, h->st);
   if (e != cudaSuccess) return fail(h, NS_ERR_CUDA, cudaGetErrorString(e));
   bag.push_back(q);
+  h->alloc_bytes[q] = bytes;
   *p = (T*)q;
   return NS_OK;
 }
@@ -72,6 +82,51 @@ template <class T> ns_status dalloc(ns_handle* h, std::vector<void*>& bag, T** p
 void free_bag(std::vector<void*>& bag) {
   for (void* p : bag) cudaFree(p);
   bag.clear();
+}
+
+// Device snapshot of every array a step writes (neuron state, spike buffers,
+// trace records, accumulators, contributions, weights, control block); the
+// spike log is rewritten identically from the restored control block.
+struct Snapshot {
+  std::vector<std::pair<void*, size_t>> regions;
+  std::vector<void*> copies;
+};
+
+void snapshot_free(Snapshot& sn) {
+  for (void* c : sn.copies) cudaFree(c);
+  sn.copies.clear();
+  sn.regions.clear();
+}
+
+cudaError_t snapshot_take(ns_handle* h, Snapshot& sn) {
+  auto add = [&](void* p) {
+    auto it = h->alloc_bytes.find(p);
+    if (p && it != h->alloc_bytes.end()) sn.regions.push_back({p, it->second});
+  };
+  for (void* p : h->neuron_allocs) add(p);
+  add(h->d.acc);
+  add(h->d.contrib);
+  add(h->d.w16);
+  add(h->d.w32);
+  sn.regions.push_back({h->ctl, sizeof(ns::Ctl)});
+  for (auto& r : sn.regions) {
+    void* c = nullptr;
+    cudaError_t e = cudaMalloc(&c, r.second);
+    if (e != cudaSuccess) { snapshot_free(sn); return e; }
+    sn.copies.push_back(c);
+    e = cudaMemcpyAsync(c, r.first, r.second, cudaMemcpyDeviceToDevice, h->st);
+    if (e != cudaSuccess) { snapshot_free(sn); return e; }
+  }
+  return cudaSuccess;
+}
+
+cudaError_t snapshot_restore(ns_handle* h, const Snapshot& sn) {
+  for (size_t q = 0; q < sn.regions.size(); ++q) {
+    cudaError_t e = cudaMemcpyAsync(sn.regions[q].first, sn.copies[q], sn.regions[q].second,
+                                    cudaMemcpyDeviceToDevice, h->st);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 void drop_graphs(ns_handle* h) {
@@ -197,8 +252,9 @@ __global__ void k_weight_sum(const float* w32, const uint16_t* w16, uint64_t m, 
 }
 
 // Builds an incoming index sorted by (target, CSR position): deterministic.
-ns_status build_incoming(ns_handle* h, const uint8_t* d_pl, int only_plastic, uint64_t** out_ptr,
-                         uint32_t** out_pos, uint2** out_list) {
+ns_status build_incoming(ns_handle* h, std::vector<void*>& bag, const uint64_t* rowp,
+                         const uint32_t* colp, const uint8_t* d_pl, int only_plastic,
+                         uint64_t** out_ptr, uint32_t** out_pos, uint2** out_list) {
   const uint64_t n = h->n, m = h->m;
   uint32_t *keys = nullptr, *vals = nullptr, *keys2 = nullptr, *vals2 = nullptr;
   unsigned long long* cnt_d = nullptr;
@@ -211,12 +267,12 @@ ns_status build_incoming(ns_handle* h, const uint8_t* d_pl, int only_plastic, ui
     return s;
   }
   const int grid = h->sms * 8;
-  k_in_keys<<<grid, 256, 0, h->st>>>(h->d.col, d_pl, m, keys, vals, cnt_d, only_plastic);
+  k_in_keys<<<grid, 256, 0, h->st>>>(colp, d_pl, m, keys, vals, cnt_d, only_plastic);
   unsigned long long cnt = 0;
   CK(cudaMemcpyAsync(&cnt, cnt_d, 8, cudaMemcpyDeviceToHost, h->st));
   CK(cudaStreamSynchronize(h->st));
   uint64_t* ptr = nullptr;
-  if ((s = dalloc(h, h->csr_allocs, &ptr, n + 1))) { free_bag(tmp); return s; }
+  if ((s = dalloc(h, bag, &ptr, n + 1))) { free_bag(tmp); return s; }
   if (cnt > 0) {
     // sort pairs by (target, position): first by position (already grouped
     // arbitrarily), then a stable sort by target keeps position order
@@ -249,13 +305,13 @@ ns_status build_incoming(ns_handle* h, const uint8_t* d_pl, int only_plastic, ui
     cub::DeviceScan::InclusiveSum(t3, tb3, deg, ptr, (int64_t)(n + 1), h->st);
     if (out_list) {
       uint2* lst = nullptr;
-      if ((s = dalloc(h, h->csr_allocs, &lst, cnt))) { free_bag(tmp); return s; }
-      k_in_list<<<grid, 256, 0, h->st>>>(vals, cnt, h->d.row_ptr, n, lst);
+      if ((s = dalloc(h, bag, &lst, cnt))) { free_bag(tmp); return s; }
+      k_in_list<<<grid, 256, 0, h->st>>>(vals, cnt, rowp, n, lst);
       *out_list = lst;
     }
     if (out_pos) {
       uint32_t* pos = nullptr;
-      if ((s = dalloc(h, h->csr_allocs, &pos, cnt))) { free_bag(tmp); return s; }
+      if ((s = dalloc(h, bag, &pos, cnt))) { free_bag(tmp); return s; }
       CK(cudaMemcpyAsync(pos, vals, cnt * 4, cudaMemcpyDeviceToDevice, h->st));
       *out_pos = pos;
     }
@@ -321,6 +377,7 @@ void fill_scalars(ns_handle* h) {
 
 typedef void (*neuron_fn)(NsDev, uint32_t);
 typedef void (*prop_fn)(NsDev, uint32_t);
+typedef void (*ltd_fn)(NsDev, uint32_t);
 
 neuron_fn pick_neuron(uint32_t model, uint32_t mode) {
 #define NSN(MO, MD) if (model == MO && mode == MD) return ns::k_neuron<MO, MD>;
@@ -334,40 +391,185 @@ neuron_fn pick_neuron(uint32_t model, uint32_t mode) {
 prop_fn pick_prop(uint32_t mode, uint32_t wf) {
   bool cond = mode == NS_INPUT_CONDUCTANCE_REF || mode == NS_INPUT_CONDUCTANCE_FRESH;
   bool bf = wf == NS_WEIGHT_BF16;
-  if (cond) return bf ? ns::k_propagate<true, true> : ns::k_propagate<true, false>;
-  return bf ? ns::k_propagate<false, true> : ns::k_propagate<false, false>;
+  if (cond) return bf ? ns::k_rows<true, true> : ns::k_rows<true, false>;
+  return bf ? ns::k_rows<false, true> : ns::k_rows<false, false>;
 }
 
-// Enqueues one step (graph-node index j) on the handle's stream.
-void enqueue_step(ns_handle* h, uint32_t j) {
-  neuron_fn nf = pick_neuron(h->cfg.model, h->cfg.input_mode);
-  prop_fn pf = pick_prop(h->cfg.input_mode, h->cfg.weight_format);
-  nf<<<h->ntiles, ns::kThreads, 0, h->st>>>(h->d, j);
-  pf<<<h->prop_blocks, 256, 0, h->st>>>(h->d, j);
-  if (h->cfg.homeostasis_enabled) {
-    if (h->cfg.weight_format == NS_WEIGHT_BF16)
-      ns::k_homeostasis<true><<<h->homeo_blocks, 256, 0, h->st>>>(h->d, j);
-    else
-      ns::k_homeostasis<false><<<h->homeo_blocks, 256, 0, h->st>>>(h->d, j);
+ltd_fn pick_ltd(uint32_t wf) { return wf == NS_WEIGHT_BF16 ? ns::k_ltd<true> : ns::k_ltd<false>; }
+
+// fused kernel at 6 (schedule 1) or 4 (schedule 3) resident blocks per SM
+prop_fn pick_fused(uint32_t mode, uint32_t wf, uint32_t sched) {
+  bool cond = mode == NS_INPUT_CONDUCTANCE_REF || mode == NS_INPUT_CONDUCTANCE_FRESH;
+  bool bf = wf == NS_WEIGHT_BF16;
+  if (sched == 3) {
+    if (cond) return bf ? ns::k_prop_fused<true, true, 4> : ns::k_prop_fused<true, false, 4>;
+    return bf ? ns::k_prop_fused<false, true, 4> : ns::k_prop_fused<false, false, 4>;
   }
+  if (cond) return bf ? ns::k_prop_fused<true, true, 6> : ns::k_prop_fused<true, false, 6>;
+  return bf ? ns::k_prop_fused<false, true, 6> : ns::k_prop_fused<false, false, 6>;
 }
 
-uint64_t launches_per_step(const ns_handle* h) { return 2u + (h->cfg.homeostasis_enabled ? 1u : 0u); }
+void launch_homeo(ns_handle* h, const NsDev& d, uint32_t j, cudaStream_t s) {
+  if (h->cfg.weight_format == NS_WEIGHT_BF16)
+    ns::k_homeostasis<true><<<h->homeo_blocks, 256, 0, s>>>(d, j);
+  else
+    ns::k_homeostasis<false><<<h->homeo_blocks, 256, 0, s>>>(d, j);
+}
 
-ns_status get_graph(ns_handle* h, uint32_t S, cudaGraphExec_t* out) {
-  auto it = h->graphs.find(S);
+// Split schedule: LTD of step k overlaps the neuron kernel of step k+1 when
+// nothing in between reads the weights (homeostasis rescales them, so it
+// serialises).
+bool overlap_ltd(const ns_handle* h) { return h->cfg.stdp_enabled && !h->cfg.homeostasis_enabled; }
+
+// schedule a step uses (fused at 6 blocks/SM until the autotuner decides)
+uint32_t sched_of(const ns_handle* h) { return h->sched == 0 ? 1u : h->sched; }
+
+// Enqueues one step (graph-node index j). With overlap, the LTD kernel of
+// step j runs on the side stream beside the neuron kernel of step j+1 and the
+// row walk of step j+1 waits for it; *ltd_pending tracks the open branch.
+cudaError_t enqueue_step(ns_handle* h, uint32_t j, bool* ltd_pending, uint32_t sched) {
+  neuron_fn nf = pick_neuron(h->cfg.model, h->cfg.input_mode);
+  nf<<<h->ntiles, ns::kThreads, 0, h->st>>>(h->d, j);
+  if (*ltd_pending) {
+    cudaError_t e = cudaStreamWaitEvent(h->st, h->ev_ltd, 0);
+    if (e != cudaSuccess) return e;
+    *ltd_pending = false;
+  }
+  if (sched == 1 || sched == 3) {
+    pick_fused(h->cfg.input_mode, h->cfg.weight_format, sched)
+        <<<h->fused_blocks[sched == 3 ? 1 : 0], 256, 0, h->st>>>(h->d, j);
+  } else {
+    pick_prop(h->cfg.input_mode, h->cfg.weight_format)<<<h->prop_blocks, 256, 0, h->st>>>(h->d, j);
+    if (h->cfg.stdp_enabled) {
+      ltd_fn lf = pick_ltd(h->cfg.weight_format);
+      if (overlap_ltd(h)) {
+        cudaError_t e = cudaEventRecord(h->ev_rows, h->st);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(h->st2, h->ev_rows, 0);
+        if (e != cudaSuccess) return e;
+        lf<<<sched == 4 ? h->ltd_narrow_blocks : h->ltd_blocks, 256, 0, h->st2>>>(h->d, j);
+        e = cudaEventRecord(h->ev_ltd, h->st2);
+        if (e != cudaSuccess) return e;
+        *ltd_pending = true;
+      } else {
+        lf<<<h->ltd_blocks, 256, 0, h->st>>>(h->d, j);
+      }
+    }
+  }
+  if (h->cfg.homeostasis_enabled) launch_homeo(h, h->d, j, h->st);
+  return cudaGetLastError();
+}
+
+cudaError_t join_ltd(ns_handle* h, bool* ltd_pending) {
+  if (!*ltd_pending) return cudaSuccess;
+  *ltd_pending = false;
+  return cudaStreamWaitEvent(h->st, h->ev_ltd, 0);
+}
+
+uint64_t launches_per_step(const ns_handle* h, uint32_t sched) {
+  const bool split = sched == 2 || sched == 4;
+  return 2u + ((split && h->cfg.stdp_enabled) ? 1u : 0u) + (h->cfg.homeostasis_enabled ? 1u : 0u);
+}
+
+ns_status get_graph(ns_handle* h, uint32_t S, uint32_t sched, cudaGraphExec_t* out) {
+  const uint32_t key = S * 4u + sched;
+  auto it = h->graphs.find(key);
   if (it != h->graphs.end()) { *out = it->second; return NS_OK; }
   cudaGraph_t g;
   CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
-  for (uint32_t j = 0; j < S; ++j) enqueue_step(h, j);
+  bool pending = false;
+  cudaError_t ce = cudaSuccess;
+  for (uint32_t j = 0; j < S && ce == cudaSuccess; ++j) ce = enqueue_step(h, j, &pending, sched);
+  if (ce == cudaSuccess) ce = join_ltd(h, &pending);
   ns::k_advance<<<1, 1, 0, h->st>>>(h->ctl, S);
-  CK(cudaStreamEndCapture(h->st, &g));
+  cudaError_t ee = cudaStreamEndCapture(h->st, &g);
+  if (ce != cudaSuccess || ee != cudaSuccess)
+    return fail(h, NS_ERR_CUDA, std::string("graph capture: ") +
+                                    cudaGetErrorString(ce != cudaSuccess ? ce : ee));
   cudaGraphExec_t ex;
   cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return fail(h, NS_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
-  h->graphs[S] = ex;
+  h->graphs[key] = ex;
   *out = ex;
+  return NS_OK;
+}
+
+// Runs n steps with the given schedule: whole graph chunks, then an eager
+// remainder. Enqueues only.
+ns_status run_steps(ns_handle* h, uint32_t n, uint32_t sched) {
+  const uint32_t S = h->cfg.graph_chunk;
+  uint32_t left = n;
+  if (left >= S) {
+    cudaGraphExec_t ex;
+    ns_status r = get_graph(h, S, sched, &ex);
+    if (r) return r;
+    while (left >= S) {
+      CK(cudaGraphLaunch(ex, h->st));
+      h->launches += (uint64_t)S * launches_per_step(h, sched) + 1;
+      left -= S;
+    }
+  }
+  if (left > 0) {
+    bool pending = false;
+    for (uint32_t j = 0; j < left; ++j) CK(enqueue_step(h, j, &pending, sched));
+    CK(join_ltd(h, &pending));
+    ns::k_advance<<<1, 1, 0, h->st>>>(h->ctl, left);
+    h->launches += (uint64_t)left * launches_per_step(h, sched) + 1;
+    CK(cudaGetLastError());
+  }
+  return NS_OK;
+}
+
+// Online autotuner: every candidate schedule runs the same window of steps
+// from one device snapshot (all give identical results, so the state after
+// the last candidate is the state after the window), timed with CUDA events
+// around one captured graph each; the fastest is kept. Runs at step 0 and
+// once more after the first 2000 steps, past the initial transient.
+uint32_t kTuneWindow = 100;
+ns_status autotune(ns_handle* h, uint32_t budget, uint32_t* used) {
+  *used = 0;
+  if (h->cfg.step_schedule != 0) return NS_OK;
+  if (!h->cfg.stdp_enabled) { h->sched = 1; return NS_OK; }
+  if (budget < kTuneWindow) return NS_OK;
+  unsigned long long step = 0;
+  CK(cudaMemcpyAsync(&step, &h->ctl->step_base, 8, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  if (step < h->next_tune_step) return NS_OK;
+  Snapshot sn;
+  CK(snapshot_take(h, sn));
+  cudaEvent_t e0, e1;
+  cudaError_t ce = cudaEventCreate(&e0);
+  if (ce == cudaSuccess) ce = cudaEventCreate(&e1);
+  if (ce != cudaSuccess) { snapshot_free(sn); return fail(h, NS_ERR_CUDA, cudaGetErrorString(ce)); }
+  const uint32_t cand[4] = {1, 2, 3, 4};
+  double us[5] = {0, 0, 0, 0, 0};
+  ns_status r = NS_OK;
+  for (int q = 0; q < 4 && r == NS_OK; ++q) {
+    if (q > 0 && (ce = snapshot_restore(h, sn)) != cudaSuccess) break;
+    cudaGraphExec_t ex;
+    if ((r = get_graph(h, kTuneWindow, cand[q], &ex))) break;
+    float ms = 0;
+    if ((ce = cudaEventRecord(e0, h->st)) != cudaSuccess) break;
+    if ((ce = cudaGraphLaunch(ex, h->st)) != cudaSuccess) break;
+    if ((ce = cudaEventRecord(e1, h->st)) != cudaSuccess) break;
+    if ((ce = cudaEventSynchronize(e1)) != cudaSuccess) break;
+    if ((ce = cudaEventElapsedTime(&ms, e0, e1)) != cudaSuccess) break;
+    us[cand[q]] = ms * 1e3 / kTuneWindow;
+    h->launches += (uint64_t)kTuneWindow * launches_per_step(h, cand[q]) + 1;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  snapshot_free(sn);
+  if (r) return r;
+  if (ce != cudaSuccess) return fail(h, NS_ERR_CUDA, std::string("autotune: ") + cudaGetErrorString(ce));
+  uint32_t best = 1;
+  for (uint32_t q = 1; q <= 4; ++q) {
+    h->tune_us[q] = us[q];
+    if (us[q] < us[best]) best = q;
+  }
+  h->sched = best;
+  h->next_tune_step = step < 2000 ? 2000 : ~0ull;
+  *used = kTuneWindow;
   return NS_OK;
 }
 
@@ -439,7 +641,8 @@ ns_status ns_create(const ns_config* cfg, ns_handle** out) {
   if (!cfg || !out) return fail(h, NS_ERR_INVALID_ARG, "null config or out pointer");
   *out = nullptr;
   const ns_config& c = *cfg;
-  if (c.model > 2 || c.input_mode > 4 || c.hh_integrator > 1 || c.weight_format > 1)
+  if (c.model > 2 || c.input_mode > 4 || c.hh_integrator > 1 || c.weight_format > 1 ||
+      c.step_schedule > 4)
     return fail(h, NS_ERR_INVALID_ARG, "unknown model / input mode / integrator / weight format");
   if (!(c.dt_ms > 0) || !is_fin(c.dt_ms)) return fail(h, NS_ERR_INVALID_ARG, "dt_ms must be > 0");
   if (c.delay_steps < 1 || c.delay_steps > 4096) return fail(h, NS_ERR_INVALID_ARG, "delay_steps in [1, 4096]");
@@ -458,8 +661,12 @@ ns_status ns_create(const ns_config* cfg, ns_handle** out) {
   h->cfg = c;
   if (h->cfg.graph_chunk == 0) h->cfg.graph_chunk = 1000;
   h->dev = c.device;
+  h->sched = c.step_schedule;
   cudaError_t e = cudaSetDevice(h->dev);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->st2, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_rows, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_ltd, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, h->dev);
   if (e != cudaSuccess) {
     g_err = std::string("device init: ") + cudaGetErrorString(e);
@@ -472,6 +679,16 @@ ns_status ns_create(const ns_config* cfg, ns_handle** out) {
     prop_fn pf = pick_prop(c.input_mode, c.weight_format);
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pf, 256, 0) != cudaSuccess || nb < 1) nb = 4;
     h->prop_blocks = h->sms * nb;
+    nb = 0;
+    for (int v = 0; v < 2; ++v) {
+      nb = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pick_fused(c.input_mode, c.weight_format, v ? 3u : 1u), 256, 0) != cudaSuccess || nb < 1) nb = 4;
+      h->fused_blocks[v] = h->sms * nb;
+    }
+    nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pick_ltd(c.weight_format), 256, 0) != cudaSuccess || nb < 1) nb = 4;
+    h->ltd_blocks = h->sms * nb;
+    h->ltd_narrow_blocks = h->sms * 2;
     nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ns::k_homeostasis<true>, 256, 0) != cudaSuccess || nb < 1) nb = 4;
     h->homeo_blocks = h->sms * nb;
@@ -500,6 +717,10 @@ ns_status ns_destroy(ns_handle* h) {
   free_bag(h->csr_allocs);
   free_bag(h->log_allocs);
   if (h->ctl) cudaFree(h->ctl);
+  if (h->st2) cudaStreamSynchronize(h->st2);
+  if (h->ev_rows) cudaEventDestroy(h->ev_rows);
+  if (h->ev_ltd) cudaEventDestroy(h->ev_ltd);
+  if (h->st2) cudaStreamDestroy(h->st2);
   if (h->st) cudaStreamDestroy(h->st);
   delete h;
   return NS_OK;
@@ -534,8 +755,14 @@ ns_status ns_upload_neurons(ns_handle* h, const ns_neuron_soa* s) {
   if (h->have_csr && s->n != h->n) return fail(h, NS_ERR_INVALID_ARG, "n differs from the CSR");
   CK(cudaSetDevice(h->dev));
   CK(cudaStreamSynchronize(h->st));
-  drop_graphs(h);
-  free_bag(h->neuron_allocs);
+  CK(cudaStreamSynchronize(h->st2));
+  // a network of the same size reuses the device buffers, so pointers and
+  // therefore the captured step graphs stay valid
+  const bool reuse = h->have_neurons && s->n == h->n && !h->neuron_allocs.empty();
+  if (!reuse) {
+    drop_graphs(h);
+    free_bag(h->neuron_allocs);
+  }
   const uint64_t n = s->n;
   h->n = n;
   h->ntiles = (uint32_t)((n + ns::kTile - 1) / ns::kTile);
@@ -589,15 +816,20 @@ ns_status ns_upload_neurons(ns_handle* h, const ns_neuron_soa* s) {
   NsDev& d = h->d;
   ns_status st;
   auto& B = h->neuron_allocs;
+  if (reuse) {
+    for (void* p : B) CK(cudaMemsetAsync(p, 0, h->alloc_bytes[p], h->st));
+  } else {
 #define DA(ptr, cnt) if ((st = dalloc(h, B, &(ptr), (cnt)))) return st;
-  DA(d.v, np) DA(d.u, np) DA(d.I, np) DA(d.gm, np) DA(d.gh, np) DA(d.gn, np)
-  DA(d.refr, np) DA(d.refr_steps, np) DA(d.inh, np) DA(d.outp, np)
-  DA(d.pre, np) DA(d.post, np) DA(d.rec, np) DA(d.last, np) DA(d.rate, np)
-  for (int q = 0; q < 7; ++q) d.par[q] = nullptr;
-  for (int q = 0; q < npar; ++q) DA(d.par[q], np)
-  for (int t = 0; t < 4; ++t) DA(d.G[t], np)
-  DA(d.bitmap, np / 32 + 2) DA(d.spk, np) DA(d.tile_cnt, h->ntiles + 1) DA(d.tile_off, h->ntiles + 1)
+    DA(d.v, np) DA(d.u, np) DA(d.I, np) DA(d.gm, np) DA(d.gh, np) DA(d.gn, np)
+    DA(d.refr, np) DA(d.refr_steps, np) DA(d.inh, np) DA(d.outp, np)
+    DA(d.pre, np) DA(d.post, np) DA(d.rec, 2 * np) DA(d.last, np) DA(d.rate, np)
+    for (int q = 0; q < 7; ++q) d.par[q] = nullptr;
+    for (int q = 0; q < npar; ++q) DA(d.par[q], np)
+    for (int t = 0; t < 4; ++t) DA(d.G[t], np)
+    DA(d.bitmap, np / 32 + 2) DA(d.spk, 2 * np)
+    DA(d.tile_cnt, 2 * ((uint64_t)h->ntiles + 1)) DA(d.tile_off, 2 * ((uint64_t)h->ntiles + 1))
 #undef DA
+  }
   auto up = [&](void* dst, const void* src, size_t bytes) {
     return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->st);
   };
@@ -631,11 +863,22 @@ ns_status ns_upload_neurons(ns_handle* h, const ns_neuron_soa* s) {
 
 // accumulators, contribution, tables, log: need both n and m
 static ns_status alloc_dynamic(ns_handle* h) {
-  free_bag(h->log_allocs);
   NsDev& d = h->d;
   const ns_config& c = h->cfg;
   const bool cond = c.input_mode == NS_INPUT_CONDUCTANCE_REF || c.input_mode == NS_INPUT_CONDUCTANCE_FRESH;
   h->ntypes_acc = cond ? 4 : 1;
+  const size_t acc_bytes = (size_t)h->ntypes_acc * c.delay_steps * h->n_pad * 8;
+  if (!h->log_allocs.empty() && d.acc && h->alloc_bytes[d.acc] == acc_bytes &&
+      (!c.homeostasis_enabled || (d.contrib && h->alloc_bytes[d.contrib] == std::max<uint64_t>(h->m, 1) * 4))) {
+    // same shape: clear in place, keep pointers (and graphs)
+    CK(cudaMemsetAsync(d.acc, 0, acc_bytes, h->st));
+    if (d.contrib) CK(cudaMemsetAsync(d.contrib, 0, h->alloc_bytes[d.contrib], h->st));
+    CK(cudaMemsetAsync(h->ctl, 0, sizeof(ns::Ctl), h->st));
+    CK(cudaStreamSynchronize(h->st));
+    return NS_OK;
+  }
+  drop_graphs(h);
+  free_bag(h->log_allocs);
   ns_status st;
   auto& B = h->log_allocs;
   if ((st = dalloc(h, B, &d.acc, (uint64_t)h->ntypes_acc * c.delay_steps * h->n_pad))) return st;
@@ -675,10 +918,14 @@ ns_status ns_upload_csr(ns_handle* h, uint64_t n, uint64_t m, const uint64_t* ro
   if (row_ptr[0] != 0 || row_ptr[n] != m) return fail(h, NS_ERR_CSR, "row_ptr[0] must be 0 and row_ptr[n] == m");
   CK(cudaSetDevice(h->dev));
   CK(cudaStreamSynchronize(h->st));
-  drop_graphs(h);
-  free_bag(h->csr_allocs);
-  h->have_csr = false;
-  NsDev& d = h->d;
+  CK(cudaStreamSynchronize(h->st2));
+  // everything is built into a new set of buffers (the handle keeps working
+  // on the old ones until the new CSR validates); a same-shaped result is then
+  // copied into the old buffers so pointers and captured graphs stay valid
+  std::vector<void*> B;
+  NsDev dn = h->d;
+  NsDev& d = dn;
+  const uint64_t old_m = h->m, old_m_pad = h->m_pad;
   h->m = m;
   h->m_pad = round_up(std::max<uint64_t>(m, 4), 4) + 4;
   if (!h->have_neurons) {
@@ -687,10 +934,10 @@ ns_status ns_upload_csr(ns_handle* h, uint64_t n, uint64_t m, const uint64_t* ro
     h->n_pad = (uint64_t)h->ntiles * ns::kTile;
   }
   ns_status st;
-  auto& B = h->csr_allocs;
+  auto undo = [&]() { free_bag(B); h->m = old_m; h->m_pad = old_m_pad; };
   uint64_t* rp = nullptr;
   uint32_t* cl = nullptr;
-  if ((st = dalloc(h, B, &rp, n + 1)) || (st = dalloc(h, B, &cl, h->m_pad))) return st;
+  if ((st = dalloc(h, B, &rp, n + 1)) || (st = dalloc(h, B, &cl, h->m_pad))) { undo(); return st; }
   CK(cudaMemcpyAsync(rp, row_ptr, (n + 1) * 8, cudaMemcpyHostToDevice, h->st));
   if (m) CK(cudaMemcpyAsync(cl, col, m * 4, cudaMemcpyHostToDevice, h->st));
   d.row_ptr = rp; d.col = cl;
@@ -699,14 +946,14 @@ ns_status ns_upload_csr(ns_handle* h, uint64_t n, uint64_t m, const uint64_t* ro
   float* wt = nullptr;
   uint8_t *ty = nullptr, *pl = nullptr;
   unsigned int* bad = nullptr;
-  if ((st = dalloc(h, tmp, &wt, h->m_pad)) || (st = dalloc(h, tmp, &bad, 2))) { free_bag(tmp); return st; }
+  if ((st = dalloc(h, tmp, &wt, h->m_pad)) || (st = dalloc(h, tmp, &bad, 2))) { free_bag(tmp); undo(); return st; }
   if (m) CK(cudaMemcpyAsync(wt, w, m * 4, cudaMemcpyHostToDevice, h->st));
   if (syn_type) {
-    if ((st = dalloc(h, tmp, &ty, h->m_pad))) { free_bag(tmp); return st; }
+    if ((st = dalloc(h, tmp, &ty, h->m_pad))) { free_bag(tmp); undo(); return st; }
     if (m) CK(cudaMemcpyAsync(ty, syn_type, m, cudaMemcpyHostToDevice, h->st));
   }
   if (plastic) {
-    if ((st = dalloc(h, tmp, &pl, h->m_pad))) { free_bag(tmp); return st; }
+    if ((st = dalloc(h, tmp, &pl, h->m_pad))) { free_bag(tmp); undo(); return st; }
     if (m) CK(cudaMemcpyAsync(pl, plastic, m, cudaMemcpyHostToDevice, h->st));
   }
   const int grid = h->sms * 8;
@@ -718,7 +965,7 @@ ns_status ns_upload_csr(ns_handle* h, uint64_t n, uint64_t m, const uint64_t* ro
   CK(cudaGetLastError());
   if (badh) {
     free_bag(tmp);
-    free_bag(h->csr_allocs);
+    undo();
     if (badh & 1u) return fail(h, NS_ERR_CSR, "row_ptr is not monotone or exceeds m");
     if (badh & 2u) return fail(h, NS_ERR_CSR, "column index >= n");
     if (badh & 4u) return fail(h, NS_ERR_NONFINITE, "weight is not finite or |w| >= 2^22");
@@ -763,18 +1010,43 @@ ns_status ns_upload_csr(ns_handle* h, uint64_t n, uint64_t m, const uint64_t* ro
   if (h->cfg.stdp_enabled) {
     uint64_t* ip = nullptr;
     uint2* il = nullptr;
-    if ((st = build_incoming(h, pl, 1, &ip, nullptr, &il))) { free_bag(tmp); return st; }
+    if ((st = build_incoming(h, B, rp, cl, pl, 1, &ip, nullptr, &il))) { free_bag(tmp); undo(); return st; }
     d.in_ptr = ip; d.in_list = il;
   }
   if (h->cfg.homeostasis_enabled) {
     uint64_t* ap = nullptr;
     uint32_t* apos = nullptr;
-    if ((st = build_incoming(h, pl, 0, &ap, &apos, nullptr))) { free_bag(tmp); return st; }
+    if ((st = build_incoming(h, B, rp, cl, pl, 0, &ap, &apos, nullptr))) { free_bag(tmp); undo(); return st; }
     d.all_in_ptr = ap; d.all_in_pos = apos;
   }
   CK(cudaStreamSynchronize(h->st));
   free_bag(tmp);
   CK(cudaGetLastError());
+  // commit: the CSR fields of the new build, field by field
+  void* oldp[13] = {(void*)h->d.row_ptr, (void*)h->d.col, h->d.w32, h->d.w16, (void*)h->d.type,
+                    (void*)h->d.plastic, (void*)h->d.row_plastic, (void*)h->d.row_type,
+                    (void*)h->d.in_ptr, (void*)h->d.in_list, (void*)h->d.all_in_ptr,
+                    (void*)h->d.all_in_pos, nullptr};
+  void* newp[13] = {(void*)dn.row_ptr, (void*)dn.col, dn.w32, dn.w16, (void*)dn.type,
+                    (void*)dn.plastic, (void*)dn.row_plastic, (void*)dn.row_type,
+                    (void*)dn.in_ptr, (void*)dn.in_list, (void*)dn.all_in_ptr,
+                    (void*)dn.all_in_pos, nullptr};
+  bool same = h->have_csr && !h->csr_allocs.empty();
+  for (int q = 0; q < 12 && same; ++q) {
+    if ((oldp[q] == nullptr) != (newp[q] == nullptr)) same = false;
+    else if (oldp[q] && h->alloc_bytes[oldp[q]] != h->alloc_bytes[newp[q]]) same = false;
+  }
+  if (same) {
+    for (int q = 0; q < 12; ++q)
+      if (newp[q]) CK(cudaMemcpyAsync(oldp[q], newp[q], h->alloc_bytes[newp[q]], cudaMemcpyDeviceToDevice, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    free_bag(B);
+  } else {
+    drop_graphs(h);
+    free_bag(h->csr_allocs);
+    h->csr_allocs = B;
+    h->d = dn;
+  }
   h->have_csr = true;
   if (h->have_neurons) return alloc_dynamic(h);
   return NS_OK;
@@ -788,23 +1060,9 @@ ns_status ns_step(ns_handle* h, uint32_t n_steps, ns_step_stats* out) {
   fill_scalars(h);
   ns::Ctl before{};
   CK(cudaMemcpyAsync(&before, h->ctl, sizeof(before), cudaMemcpyDeviceToHost, h->st));
-  const uint32_t S = h->cfg.graph_chunk;
-  uint32_t left = n_steps;
-  if (left >= S) {
-    cudaGraphExec_t ex;
-    if ((r = get_graph(h, S, &ex))) return r;
-    while (left >= S) {
-      CK(cudaGraphLaunch(ex, h->st));
-      h->launches += (uint64_t)S * launches_per_step(h) + 1;
-      left -= S;
-    }
-  }
-  if (left > 0) {
-    for (uint32_t j = 0; j < left; ++j) enqueue_step(h, j);
-    ns::k_advance<<<1, 1, 0, h->st>>>(h->ctl, left);
-    h->launches += (uint64_t)left * launches_per_step(h) + 1;
-    CK(cudaGetLastError());
-  }
+  uint32_t tuned = 0;
+  if ((r = autotune(h, n_steps, &tuned))) return r;
+  if ((r = run_steps(h, n_steps - tuned, sched_of(h)))) return r;
   ns::Ctl after{};
   CK(cudaMemcpyAsync(&after, h->ctl, sizeof(after), cudaMemcpyDeviceToHost, h->st));
   CK(cudaStreamSynchronize(h->st));
@@ -842,12 +1100,10 @@ ns_status ns_step_traced(ns_handle* h, uint64_t* pos_out, uint64_t cap, uint64_t
   ns::k_trace_offsets<<<1, 32, 0, h->st>>>(d, off);
   d.trace_pos = pos; d.trace_off = off; d.trace_cap = cap;
   pf<<<h->prop_blocks, 256, 0, h->st>>>(d, 0);
-  if (h->cfg.homeostasis_enabled) {
-    if (h->cfg.weight_format == NS_WEIGHT_BF16) ns::k_homeostasis<true><<<h->homeo_blocks, 256, 0, h->st>>>(d, 0);
-    else ns::k_homeostasis<false><<<h->homeo_blocks, 256, 0, h->st>>>(d, 0);
-  }
+  if (h->cfg.stdp_enabled) pick_ltd(h->cfg.weight_format)<<<h->ltd_blocks, 256, 0, h->st>>>(d, 0);
+  if (h->cfg.homeostasis_enabled) launch_homeo(h, d, 0, h->st);
   ns::k_advance<<<1, 1, 0, h->st>>>(h->ctl, 1);
-  h->launches += launches_per_step(h) + 2;
+  h->launches += launches_per_step(h, 2) + 2;
   CK(cudaGetLastError());
   ns::Ctl after{};
   CK(cudaMemcpyAsync(&after, h->ctl, sizeof(after), cudaMemcpyDeviceToHost, h->st));
@@ -1103,39 +1359,50 @@ ns_status ns_profile_steps(ns_handle* h, uint32_t n_steps, double* kernel_ms, ui
   fill_scalars(h);
   neuron_fn nf = pick_neuron(h->cfg.model, h->cfg.input_mode);
   prop_fn pf = pick_prop(h->cfg.input_mode, h->cfg.weight_format);
-  const int nk = h->cfg.homeostasis_enabled ? 3 : 2;
-  std::vector<cudaEvent_t> ev((size_t)n_steps * nk * 2);
+  ltd_fn lf = pick_ltd(h->cfg.weight_format);
+  // kernels in order neuron, rows, ltd, homeostasis; serial, one event pair each
+  const bool on[4] = {true, true, h->cfg.stdp_enabled != 0, h->cfg.homeostasis_enabled != 0};
+  std::vector<cudaEvent_t> ev((size_t)n_steps * 8);
   for (auto& e : ev) CK(cudaEventCreate(&e));
   for (uint32_t j = 0; j < n_steps; ++j) {
-    cudaEvent_t* e = &ev[(size_t)j * nk * 2];
+    cudaEvent_t* e = &ev[(size_t)j * 8];
     CK(cudaEventRecord(e[0], h->st));
     nf<<<h->ntiles, ns::kThreads, 0, h->st>>>(h->d, j);
     CK(cudaEventRecord(e[1], h->st));
     CK(cudaEventRecord(e[2], h->st));
     pf<<<h->prop_blocks, 256, 0, h->st>>>(h->d, j);
     CK(cudaEventRecord(e[3], h->st));
-    if (nk == 3) {
-      CK(cudaEventRecord(e[4], h->st));
-      if (h->cfg.weight_format == NS_WEIGHT_BF16)
-        ns::k_homeostasis<true><<<h->homeo_blocks, 256, 0, h->st>>>(h->d, j);
-      else
-        ns::k_homeostasis<false><<<h->homeo_blocks, 256, 0, h->st>>>(h->d, j);
-      CK(cudaEventRecord(e[5], h->st));
-    }
+    CK(cudaEventRecord(e[4], h->st));
+    if (on[2]) lf<<<h->ltd_blocks, 256, 0, h->st>>>(h->d, j);
+    CK(cudaEventRecord(e[5], h->st));
+    CK(cudaEventRecord(e[6], h->st));
+    if (on[3]) launch_homeo(h, h->d, j, h->st);
+    CK(cudaEventRecord(e[7], h->st));
   }
   ns::k_advance<<<1, 1, 0, h->st>>>(h->ctl, n_steps);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(h->st));
+  uint64_t nl = 0;
   for (uint32_t j = 0; j < n_steps; ++j)
-    for (int q = 0; q < nk; ++q) {
+    for (int q = 0; q < 4; ++q) {
+      if (!on[q]) continue;
       float ms = 0;
-      CK(cudaEventElapsedTime(&ms, ev[((size_t)j * nk + q) * 2], ev[((size_t)j * nk + q) * 2 + 1]));
+      CK(cudaEventElapsedTime(&ms, ev[(size_t)j * 8 + 2 * q], ev[(size_t)j * 8 + 2 * q + 1]));
       kernel_ms[q] += ms;
       launches[q] += 1;
+      ++nl;
     }
   for (auto& e : ev) cudaEventDestroy(e);
-  h->launches += (uint64_t)n_steps * nk + 1;
+  h->launches += nl + 1;
   return check_device_status(h);
+}
+
+ns_status ns_get_schedule(ns_handle* h, uint32_t* schedule, double* us_per_step) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  if (schedule) *schedule = h->sched;
+  if (us_per_step)
+    for (int q = 0; q < 4; ++q) us_per_step[q] = h->tune_us[q + 1];
+  return NS_OK;
 }
 
 ns_status ns_launch_count(ns_handle* h, uint64_t* launches) {

@@ -273,6 +273,12 @@ __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
   constexpr bool COND = (MODE == 3 || MODE == 4);
   constexpr int NT = COND ? 4 : 1;
   constexpr int NP = MODEL == 0 ? 5 : (MODEL == 1 ? 4 : 7);
+  // spike lists, tile counts and trace records are double-buffered by step
+  // parity so that the LTD kernel of step k can run beside this kernel
+  const uint32_t par_k = (uint32_t)(k & 1);
+  uint32_t* const spk_k = d.spk + par_k * d.n_pad;
+  uint32_t* const tcnt_k = d.tile_cnt + par_k * (d.ntiles + 1);
+  float2* const rec_k = d.rec + par_k * d.n_pad;
 
   if (tid == 0) s_nk = 0;
   __syncthreads();
@@ -433,7 +439,7 @@ __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
       *reinterpret_cast<float2*>(d.post + i0) = make_float2(qv0, qv1);
       const float4 rr = make_float4(spk[0] ? -pv0 : pv0, spk[0] ? -qv0 : qv0,
                                     spk[1] ? -pv1 : pv1, spk[1] ? -qv1 : qv1);
-      *reinterpret_cast<float4*>(d.rec + i0) = rr;
+      *reinterpret_cast<float4*>(rec_k + i0) = rr;
     }
     // ---- write back state ----
     *reinterpret_cast<float2*>(d.v + i0) = make_float2(st[0].v, st[1].v);
@@ -481,7 +487,7 @@ __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
     if (lane < kPairs * kWarps) s_off[lane] = incl - c;
     if (lane == kPairs * kWarps - 1) {
       s_total = incl;
-      d.tile_cnt[tile] = incl;
+      tcnt_k[tile] = incl;
     }
   }
   __syncthreads();
@@ -493,8 +499,8 @@ __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
     const uint32_t pre_cnt = __popc(me & lt) + __popc(mo & lt);
     const uint32_t i0 = (uint32_t)(base + (uint64_t)r * 512 + 2 * (uint64_t)tid);
     const uint32_t o = s_off[r * kWarps + warp] + pre_cnt;
-    if (s0) d.spk[base + o] = i0;
-    if (s1) d.spk[base + o + (s0 ? 1u : 0u)] = i0 + 1;
+    if (s0) spk_k[base + o] = i0;
+    if (s1) spk_k[base + o + (s0 ? 1u : 0u)] = i0 + 1;
   }
   // last tile of the step: counters, FP64 clock, spike-log bookkeeping
   if (tid == 0) {
@@ -506,7 +512,7 @@ __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
   __syncthreads();
   if (!s_last) return;
   __threadfence();
-  if (d.ntiles > kSmemTiles) block_scan_u32(d.tile_cnt, d.tile_off, d.ntiles);
+  if (d.ntiles > kSmemTiles) block_scan_u32(tcnt_k, d.tile_off + par_k * (d.ntiles + 1), d.ntiles);
   if (tid == 0) {
     Ctl* c = d.ctl;
     const unsigned long long total = atomicAdd(&c->spk_acc[k & 3], 0ull);
@@ -560,192 +566,281 @@ __device__ __forceinline__ void load_w4(const NsDev& d, bool bf16, uint64_t e0, 
 
 __device__ __forceinline__ bool neg(float x) { return (__float_as_uint(x) >> 31) != 0u; }
 
-template <bool COND, bool BF16>
-__global__ void __launch_bounds__(256, 5) k_propagate(NsDev d, uint32_t jstep) {
-  __shared__ uint32_t s_toff[kSmemTiles + 1];
-  __shared__ unsigned long long s_ev;
-  __shared__ uint32_t s_out;
-  const int lane = threadIdx.x & 31;
-  const uint64_t k = d.ctl->step_base + jstep;
-  const uint32_t slot = (uint32_t)(k % d.D);
-  const uint32_t cnt = (uint32_t)d.ctl->step_spikes[k & 3];
-  const bool STDP = d.stdp != 0;
-  const bool HOMEO = d.homeo != 0;
-  const bool small = d.ntiles <= kSmemTiles;
-  if (threadIdx.x == 0) { s_ev = 0ull; s_out = 0u; }
-  if (small && cnt) block_scan_u32(d.tile_cnt, s_toff, d.ntiles);
-  __syncthreads();
-  const uint32_t* toff = small ? s_toff : d.tile_off;
-  const bool log_ok = d.ctl->log_ok[k & 3] != 0u;
-  const unsigned long long log_base = log_ok ? d.ctl->log_size - cnt : 0ull;
-  const uint32_t items = STDP ? 2u * cnt : cnt;
-  const uint32_t wglob = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const uint32_t nw = gridDim.x * (blockDim.x >> 5);
-  unsigned long long ev = 0ull;
-  uint32_t outs = 0u;
-  for (uint32_t item = wglob; item < items; item += nw) {
-    const uint32_t rank = item < cnt ? item : item - cnt;
-    // tile holding the rank-th spike: largest t with toff[t] <= rank
-    uint32_t lo = 0, hi = d.ntiles;
+// Spike list of step k as seen by the consumers: per-tile offsets in shared
+// memory (exclusive scan of the tile counts) or, for networks of more than
+// kSmemTiles tiles, the scan the neuron kernel's last tile wrote.
+struct SpikeView {
+  const uint32_t* spk;
+  const uint32_t* toff;
+  uint32_t ntiles;
+  __device__ __forceinline__ uint32_t at(uint32_t rank) const {
+    uint32_t lo = 0, hi = ntiles;   // largest t with toff[t] <= rank
     while (hi - lo > 1) {
       const uint32_t mid = (lo + hi) >> 1;
       if (toff[mid] <= rank) lo = mid; else hi = mid;
     }
-    const uint32_t j = __ldg(d.spk + (uint64_t)lo * kTile + (rank - toff[lo]));
-    if (item < cnt) {
-      // ---------------- row walk of spiking source j ----------------
-      const uint64_t beg = __ldg(d.row_ptr + j), end = __ldg(d.row_ptr + j + 1);
-      const uint8_t rp = STDP ? __ldg(d.row_plastic + j) : 0;
-      const uint8_t rt = COND ? __ldg(d.row_type + j) : 0;
-      float pj = 0.0f;
-      if (lane == 0) {
-        const long long lst = d.last[j];
-        if (log_ok) d.log_idx[log_base + item] = j;
-        ev += end - beg;
-        outs += d.outp[j] ? 1u : 0u;
-        d.last[j] = (long long)k;
-        if (STDP) {
-          // spike-time trace bump: trace * exp(-(t - t_last)/tau) + 1
-          const float2 rj = d.rec[j];
-          const long long dk = lst < 0 ? -1 : (long long)k - lst;
-          const float fp = (dk >= 0 && (unsigned long long)dk < d.Kp) ? d.Ep[dk] : 0.0f;
-          const float fm = (dk >= 0 && (unsigned long long)dk < d.Km) ? d.Em[dk] : 0.0f;
-          pj = fabsf(rj.x) * fp + 1.0f;
-          d.pre[j] = pj;
-          d.post[j] = fabsf(rj.y) * fm + 1.0f;
-        }
+    return __ldg(spk + (uint64_t)lo * kTile + (rank - toff[lo]));
+  }
+};
+
+__device__ __forceinline__ SpikeView spike_view(const NsDev& d, uint64_t k, uint32_t cnt,
+                                                uint32_t* s_toff) {
+  const uint32_t par_k = (uint32_t)(k & 1);
+  const uint32_t* tcnt = d.tile_cnt + par_k * (d.ntiles + 1);
+  const bool small = d.ntiles <= kSmemTiles;
+  if (small && cnt) block_scan_u32(tcnt, s_toff, d.ntiles);
+  __syncthreads();
+  SpikeView v;
+  v.spk = d.spk + par_k * d.n_pad;
+  v.toff = small ? s_toff : d.tile_off + par_k * (d.ntiles + 1);
+  v.ntiles = d.ntiles;
+  return v;
+}
+
+
+// Per-step context shared by the consumers of the spike list.
+struct StepCtx {
+  uint64_t k;
+  uint32_t slot, cnt;
+  bool stdp, homeo, log_ok;
+  unsigned long long log_base;
+  const float2* rec_k;
+};
+
+__device__ __forceinline__ StepCtx step_ctx(const NsDev& d, uint32_t jstep) {
+  StepCtx c;
+  c.k = d.ctl->step_base + jstep;
+  c.slot = (uint32_t)(c.k % d.D);
+  c.cnt = (uint32_t)d.ctl->step_spikes[c.k & 3];
+  c.stdp = d.stdp != 0;
+  c.homeo = d.homeo != 0;
+  c.rec_k = d.rec + (c.k & 1) * d.n_pad;
+  c.log_ok = d.ctl->log_ok[c.k & 3] != 0u;
+  c.log_base = c.log_ok ? d.ctl->log_size - c.cnt : 0ull;
+  return c;
+}
+
+// Row walk of spiking source j (the item-th spike of the step): bookkeeping
+// (log entry, last spike step, trace bump), then the CSR row in 128-entry
+// chunks: accumulation into the delay slot and LTP (LTP then LTD when the
+// target spiked in this step too).
+template <bool COND, bool BF16>
+__device__ __forceinline__ void row_item(const NsDev& d, const StepCtx& c, uint32_t item, uint32_t j,
+                                         int lane, unsigned long long& ev, uint32_t& outs) {
+  const bool STDP = c.stdp, HOMEO = c.homeo;
+  const uint64_t k = c.k;
+  const uint64_t beg = __ldg(d.row_ptr + j), end = __ldg(d.row_ptr + j + 1);
+  const uint8_t rp = STDP ? __ldg(d.row_plastic + j) : 0;
+  const uint8_t rt = COND ? __ldg(d.row_type + j) : 0;
+  float pj = 0.0f;
+  if (lane == 0) {
+    const long long lst = d.last[j];
+    if (c.log_ok) d.log_idx[c.log_base + item] = j;
+    ev += end - beg;
+    outs += d.outp[j] ? 1u : 0u;
+    d.last[j] = (long long)k;
+    if (STDP) {
+      // spike-time trace bump: trace * exp(-(t - t_last)/tau) + 1
+      const float2 rj = c.rec_k[j];
+      const long long dk = lst < 0 ? -1 : (long long)k - lst;
+      const float fp = (dk >= 0 && (unsigned long long)dk < d.Kp) ? d.Ep[dk] : 0.0f;
+      const float fm = (dk >= 0 && (unsigned long long)dk < d.Km) ? d.Em[dk] : 0.0f;
+      pj = fabsf(rj.x) * fp + 1.0f;
+      d.pre[j] = pj;
+      d.post[j] = fabsf(rj.y) * fm + 1.0f;
+    }
+  }
+  const unsigned long long tbase = d.trace_pos ? d.trace_off[item] : 0ull;
+  const uint64_t rb = beg & ~3ull;
+  const uint32_t nrow = end > beg ? (uint32_t)((end - rb + 127) >> 7) : 0u;
+  for (uint32_t ch = 0; ch < nrow; ++ch) {
+    const uint64_t e0 = rb + 128ull * ch + 4ull * lane;
+    const bool rv = e0 < end && e0 + 4 > beg;
+    uint4 c4 = make_uint4(0u, 0u, 0u, 0u);
+    float w[4] = {0.f, 0.f, 0.f, 0.f};
+    if (rv) {
+      c4 = __ldg(reinterpret_cast<const uint4*>(d.col + e0));
+      load_w4(d, BF16, e0, w);
+    }
+    const uint32_t cc[4] = {c4.x, c4.y, c4.z, c4.w};
+    bool inr[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) inr[q] = rv && (e0 + q >= beg) && (e0 + q < end);
+    // target records for LTP, gathered before the atomics are issued
+    bool pl[4] = {false, false, false, false};
+    float tq[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      pl[q] = STDP && rp && inr[q] && (rp == 1 || __ldg(d.plastic + e0 + q));
+      tq[q] = pl[q] ? c.rec_k[cc[q]].y : 0.f;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      if (!inr[q]) continue;
+      const uint64_t e = e0 + q;
+      int ty = 0;
+      if (COND) ty = (rt == 255) ? (int)__ldg(d.type + e) : (int)rt;
+      const float val = (COND && (ty == 1 || ty == 2)) ? fabsf(w[q]) : w[q];
+      atomicAdd(d.acc + ((uint64_t)ty * d.D + c.slot) * d.n_pad + cc[q],
+                (unsigned long long)to_fix(val));
+      if (d.trace_pos) {
+        const unsigned long long tp = tbase + (e - beg);
+        if (tp < d.trace_cap) d.trace_pos[tp] = e;
       }
-      const unsigned long long tbase = d.trace_pos ? d.trace_off[item] : 0ull;
-      const uint64_t rb = beg & ~3ull;
-      const uint32_t nrow = end > beg ? (uint32_t)((end - rb + 127) >> 7) : 0u;
-      for (uint32_t c = 0; c < nrow; ++c) {
-        const uint64_t e0 = rb + 128ull * c + 4ull * lane;
-        const bool rv = e0 < end && e0 + 4 > beg;
-        uint4 c4 = make_uint4(0u, 0u, 0u, 0u);
-        float w[4] = {0.f, 0.f, 0.f, 0.f};
-        if (rv) {
-          c4 = __ldg(reinterpret_cast<const uint4*>(d.col + e0));
-          load_w4(d, BF16, e0, w);
+      if (HOMEO) {
+        float mag;
+        if (COND) {
+          float g = w[q] * kSyn[ty].gmax;
+          if (kSyn[ty].mg) g = g * (1.0f / (1.0f + (1.0f / 3.57f) * expf(-0.062f * d.v[cc[q]])));
+          mag = fabsf(g);
+        } else {
+          mag = fabsf(w[q]);
         }
-        const uint32_t cc[4] = {c4.x, c4.y, c4.z, c4.w};
-        bool inr[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) inr[q] = rv && (e0 + q >= beg) && (e0 + q < end);
-        // target records for LTP, gathered before the atomics are issued
-        bool pl[4] = {false, false, false, false};
-        float2 tr[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          pl[q] = STDP && rp && inr[q] && (rp == 1 || __ldg(d.plastic + e0 + q));
-          tr[q] = pl[q] ? d.rec[cc[q]] : make_float2(0.f, 0.f);
-        }
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          if (!inr[q]) continue;
-          const uint64_t e = e0 + q;
-          int ty = 0;
-          if (COND) ty = (rt == 255) ? (int)__ldg(d.type + e) : (int)rt;
-          const float val = (COND && (ty == 1 || ty == 2)) ? fabsf(w[q]) : w[q];
-          atomicAdd(d.acc + ((uint64_t)ty * d.D + slot) * d.n_pad + cc[q],
-                    (unsigned long long)to_fix(val));
-          if (d.trace_pos) {
-            const unsigned long long tp = tbase + (e - beg);
-            if (tp < d.trace_cap) d.trace_pos[tp] = e;
-          }
-          if (HOMEO) {
-            float mag;
-            if (COND) {
-              float g = w[q] * kSyn[ty].gmax;
-              if (kSyn[ty].mg) g = g * (1.0f / (1.0f + (1.0f / 3.57f) * expf(-0.062f * d.v[cc[q]])));
-              mag = fabsf(g);
-            } else {
-              mag = fabsf(w[q]);
-            }
-            d.contrib[e] = d.contrib[e] * d.cd + mag * d.one_m_cd;
-          }
-        }
-        if (STDP && rp) {
-          pj = __shfl_sync(0xffffffffu, pj, 0);
-          // LTP, then LTD when the target spiked in this step too
-          float wn[4];
-          bool chg = false, all4 = true;
-#pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            wn[q] = w[q];
-            if (!pl[q]) { all4 = false; continue; }
-            float w1 = clampw(w[q] + d.a_plus * fabsf(tr[q].y), d.w_min, d.w_max);
-            if (neg(tr[q].y)) w1 = clampw(w1 + d.neg_a_minus * pj, d.w_min, d.w_max);
-            wn[q] = w1;
-            chg = true;
-          }
-          if (chg) {
-            if (BF16) {
-              if (all4) {
-                uint2 raw;
-                raw.x = (uint32_t)f32_to_bf16_bits(wn[0]) | ((uint32_t)f32_to_bf16_bits(wn[1]) << 16);
-                raw.y = (uint32_t)f32_to_bf16_bits(wn[2]) | ((uint32_t)f32_to_bf16_bits(wn[3]) << 16);
-                *reinterpret_cast<uint2*>(d.w16 + e0) = raw;
-              } else {
-#pragma unroll
-                for (int q = 0; q < 4; ++q)
-                  if (pl[q]) d.w16[e0 + q] = f32_to_bf16_bits(wn[q]);
-              }
-            } else {
-              if (all4) {
-                *reinterpret_cast<float4*>(d.w32 + e0) = make_float4(wn[0], wn[1], wn[2], wn[3]);
-              } else {
-#pragma unroll
-                for (int q = 0; q < 4; ++q)
-                  if (pl[q]) d.w32[e0 + q] = wn[q];
-              }
-            }
-          }
-        }
+        d.contrib[e] = d.contrib[e] * d.cd + mag * d.one_m_cd;
       }
-    } else {
-      // ------------- LTD over spiking target j's plastic inputs -------------
-      const uint64_t ib = __ldg(d.in_ptr + j), ie = __ldg(d.in_ptr + j + 1);
-      for (uint64_t q0 = ib; q0 < ie; q0 += 128) {
-        uint2 sp[4];
-        bool act[4];
+    }
+    if (STDP && rp) {
+      pj = __shfl_sync(0xffffffffu, pj, 0);
+      float wn[4];
+      bool chg = false, all4 = true;
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const uint64_t q = q0 + lane + 32u * u;
-          act[u] = q < ie;
-          sp[u] = act[u] ? __ldg(d.in_list + q) : make_uint2(0u, 0u);
-        }
-        float pre[4], wv[4];
+      for (int q = 0; q < 4; ++q) {
+        wn[q] = w[q];
+        if (!pl[q]) { all4 = false; continue; }
+        float w1 = clampw(w[q] + d.a_plus * fabsf(tq[q]), d.w_min, d.w_max);
+        if (neg(tq[q])) w1 = clampw(w1 + d.neg_a_minus * pj, d.w_min, d.w_max);
+        wn[q] = w1;
+        chg = true;
+      }
+      if (chg) {
+        if (BF16) {
+          if (all4) {
+            uint2 raw;
+            raw.x = (uint32_t)f32_to_bf16_bits(wn[0]) | ((uint32_t)f32_to_bf16_bits(wn[1]) << 16);
+            raw.y = (uint32_t)f32_to_bf16_bits(wn[2]) | ((uint32_t)f32_to_bf16_bits(wn[3]) << 16);
+            *reinterpret_cast<uint2*>(d.w16 + e0) = raw;
+          } else {
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          pre[u] = act[u] ? d.rec[sp[u].x].x : 0.0f;
-          if (BF16) wv[u] = act[u] ? bf16_bits_to_f32(d.w16[sp[u].y]) : 0.0f;
-          else wv[u] = act[u] ? d.w32[sp[u].y] : 0.0f;
-        }
+            for (int q = 0; q < 4; ++q)
+              if (pl[q]) d.w16[e0 + q] = f32_to_bf16_bits(wn[q]);
+          }
+        } else {
+          if (all4) {
+            *reinterpret_cast<float4*>(d.w32 + e0) = make_float4(wn[0], wn[1], wn[2], wn[3]);
+          } else {
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          // synapses whose source spiked too are handled by the source's row walk
-          if (!act[u] || neg(pre[u])) continue;
-          const float w1 = clampw(wv[u] + d.neg_a_minus * pre[u], d.w_min, d.w_max);
-          if (BF16) d.w16[sp[u].y] = f32_to_bf16_bits(w1);
-          else d.w32[sp[u].y] = w1;
+            for (int q = 0; q < 4; ++q)
+              if (pl[q]) d.w32[e0 + q] = wn[q];
+          }
         }
       }
     }
   }
-  // block sums of synaptic events and output spikes
+}
+
+// LTD over the plastic incoming synapses of spiking target j whose source did
+// not spike (those whose source spiked are handled by the source's row walk).
+template <bool BF16>
+__device__ __forceinline__ void ltd_item(const NsDev& d, const StepCtx& c, uint32_t j, int lane) {
+  const uint64_t ib = __ldg(d.in_ptr + j), ie = __ldg(d.in_ptr + j + 1);
+  for (uint64_t q0 = ib; q0 < ie; q0 += 128) {
+    uint2 sp[4];
+    bool act[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const uint64_t q = q0 + lane + 32u * u;
+      act[u] = q < ie;
+      sp[u] = act[u] ? __ldg(d.in_list + q) : make_uint2(0u, 0u);
+    }
+    float pre[4], wv[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      pre[u] = act[u] ? c.rec_k[sp[u].x].x : 0.0f;
+      if (BF16) wv[u] = act[u] ? bf16_bits_to_f32(d.w16[sp[u].y]) : 0.0f;
+      else wv[u] = act[u] ? d.w32[sp[u].y] : 0.0f;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      if (!act[u] || neg(pre[u])) continue;
+      const float w1 = clampw(wv[u] + d.neg_a_minus * pre[u], d.w_min, d.w_max);
+      if (BF16) d.w16[sp[u].y] = f32_to_bf16_bits(w1);
+      else d.w32[sp[u].y] = w1;
+    }
+  }
+}
+
+__device__ __forceinline__ void flush_counters(const NsDev& d, unsigned long long ev, uint32_t outs,
+                                               unsigned long long* s_ev, uint32_t* s_out) {
+  const int lane = threadIdx.x & 31;
   for (int o = 16; o > 0; o >>= 1) {
     ev += __shfl_down_sync(0xffffffffu, ev, o);
     outs += __shfl_down_sync(0xffffffffu, outs, o);
   }
   if (lane == 0 && (ev | outs)) {
-    atomicAdd(&s_ev, ev);
-    atomicAdd(&s_out, outs);
+    atomicAdd(s_ev, ev);
+    atomicAdd(s_out, outs);
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    if (s_ev) atomicAdd(&d.ctl->events_total, s_ev);
-    if (s_out) atomicAdd(&d.ctl->out_total, (unsigned long long)s_out);
+    if (*s_ev) atomicAdd(&d.ctl->events_total, *s_ev);
+    if (*s_out) atomicAdd(&d.ctl->out_total, (unsigned long long)*s_out);
   }
+}
+
+// Kernel 2 (fused schedule): row walks [0, cnt) and LTD lists [cnt, 2 cnt)
+// as warp work items of one grid-stride kernel.
+template <bool COND, bool BF16, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_prop_fused(NsDev d, uint32_t jstep) {
+  __shared__ uint32_t s_toff[kSmemTiles + 1];
+  __shared__ unsigned long long s_ev;
+  __shared__ uint32_t s_out;
+  const int lane = threadIdx.x & 31;
+  const StepCtx c = step_ctx(d, jstep);
+  if (threadIdx.x == 0) { s_ev = 0ull; s_out = 0u; }
+  const SpikeView sv = spike_view(d, c.k, c.cnt, s_toff);
+  const uint32_t items = c.stdp ? 2u * c.cnt : c.cnt;
+  const uint32_t wglob = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const uint32_t nw = gridDim.x * (blockDim.x >> 5);
+  unsigned long long ev = 0ull;
+  uint32_t outs = 0u;
+  for (uint32_t item = wglob; item < items; item += nw) {
+    const uint32_t rank = item < c.cnt ? item : item - c.cnt;
+    const uint32_t j = sv.at(rank);
+    if (item < c.cnt) row_item<COND, BF16>(d, c, item, j, lane, ev, outs);
+    else ltd_item<BF16>(d, c, j, lane);
+  }
+  flush_counters(d, ev, outs, &s_ev, &s_out);
+}
+
+// Kernel 2a / 2b (split schedule): the row walks, then the LTD lists on a
+// second stream beside the next step's neuron kernel.
+template <bool COND, bool BF16>
+__global__ void __launch_bounds__(256, 4) k_rows(NsDev d, uint32_t jstep) {
+  __shared__ uint32_t s_toff[kSmemTiles + 1];
+  __shared__ unsigned long long s_ev;
+  __shared__ uint32_t s_out;
+  const int lane = threadIdx.x & 31;
+  const StepCtx c = step_ctx(d, jstep);
+  if (threadIdx.x == 0) { s_ev = 0ull; s_out = 0u; }
+  const SpikeView sv = spike_view(d, c.k, c.cnt, s_toff);
+  const uint32_t wglob = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const uint32_t nw = gridDim.x * (blockDim.x >> 5);
+  unsigned long long ev = 0ull;
+  uint32_t outs = 0u;
+  for (uint32_t item = wglob; item < c.cnt; item += nw)
+    row_item<COND, BF16>(d, c, item, sv.at(item), lane, ev, outs);
+  flush_counters(d, ev, outs, &s_ev, &s_out);
+}
+
+template <bool BF16>
+__global__ void __launch_bounds__(256, 5) k_ltd(NsDev d, uint32_t jstep) {
+  __shared__ uint32_t s_toff[kSmemTiles + 1];
+  const int lane = threadIdx.x & 31;
+  const StepCtx c = step_ctx(d, jstep);
+  const SpikeView sv = spike_view(d, c.k, c.cnt, s_toff);
+  const uint32_t wglob = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const uint32_t nw = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t item = wglob; item < c.cnt; item += nw) ltd_item<BF16>(d, c, sv.at(item), lane);
 }
 
 // ---------------------------------------------------------------------------
@@ -793,13 +888,14 @@ __global__ void k_advance(Ctl* ctl, uint32_t steps) { ctl->step_base += steps; }
 // (traced step only): walks the tile-local lists in tile order
 __global__ void k_trace_offsets(NsDev d, unsigned long long* off) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const uint32_t par_k = (uint32_t)(d.ctl->step_base & 1);
   unsigned long long run = 0;
   uint32_t q = 0;
   for (uint32_t t = 0; t < d.ntiles; ++t) {
-    const uint32_t c = d.tile_cnt[t];
+    const uint32_t c = d.tile_cnt[par_k * (d.ntiles + 1) + t];
     for (uint32_t l = 0; l < c; ++l) {
       off[q++] = run;
-      const uint32_t j = d.spk[(uint64_t)t * kTile + l];
+      const uint32_t j = d.spk[par_k * d.n_pad + (uint64_t)t * kTile + l];
       run += d.row_ptr[j + 1] - d.row_ptr[j];
     }
   }

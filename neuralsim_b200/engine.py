@@ -91,6 +91,7 @@ class SimConfig:
     spike_log_capacity: int = 0
     spike_log_steps: int = 0
     graph_chunk: int = 1000
+    step_schedule: int = 0      # 0 autotune, 1 fused, 2 split, 3 fused (4 blocks/SM)
 
     def to_c(self):
         c = A.NsConfig()
@@ -309,13 +310,20 @@ class SimulationEngine:
         return int(p.value or 0)
 
     def profile_steps(self, n_steps: int):
-        """Per-kernel device time over n_steps eager steps:
-        {"neuron": (ms_total, launches), "propagate": ..., "homeostasis": ...}"""
-        ms = (C.c_double * 3)()
-        ln = (C.c_uint64 * 3)()
+        """Per-kernel device time over n_steps eager serial steps:
+        {"neuron": (ms_total, launches), "rows": ..., "ltd": ..., "homeostasis": ...}"""
+        ms = (C.c_double * 4)()
+        ln = (C.c_uint64 * 4)()
         self._check(self.lib.ns_profile_steps(self._h, int(n_steps), ms, ln))
-        names = ("neuron", "propagate", "homeostasis")
-        return {names[q]: (ms[q], int(ln[q])) for q in range(3) if ln[q]}
+        names = ("neuron", "rows", "ltd", "homeostasis")
+        return {names[q]: (ms[q], int(ln[q])) for q in range(4) if ln[q]}
+
+    def schedule(self):
+        """(schedule in use, {schedule: measured us/step}) from the autotuner."""
+        sc = C.c_uint32()
+        us = (C.c_double * 4)()
+        self._check(self.lib.ns_get_schedule(self._h, C.byref(sc), us))
+        return int(sc.value), {q + 1: us[q] for q in range(4)}
 
     def launch_count(self):
         c = C.c_uint64()

@@ -67,6 +67,32 @@ def test_izh_stdp_raster_weights_bit_exact_1s(lib, wf):
     assert np.count_nonzero(st["w"] != net.w) > 1000
 
 
+@pytest.mark.parametrize("sched", [1, 2, 3, 4])
+def test_step_schedules_identical(lib, sched):
+    # fused, split (LTD beside the next neuron update) and fused-4 schedules
+    # compute the same step: rasters and BF16 weights bit-identical to the oracle
+    net, cfg, drive = nets.izh_stdp(n=30_000, k=100)
+    cfg.step_schedule = sched
+    cfg.graph_chunk = 100
+    eng = gpu_run(net, cfg, drive, 350)
+    o = FastOracle(net, cfg, drive, precision=32)
+    o.step(350)
+    assert eng.schedule()[0] == sched
+    assert nets.rasters_equal(eng.read_raster(0, 350), o.raster())
+    assert np.array_equal(eng.download_state()["w"].astype(np.float64), o.weights())
+
+
+def test_autotuner_picks_a_schedule(lib):
+    net, cfg, drive = nets.izh_stdp(n=30_000, k=100)
+    eng = gpu_run(net, cfg, drive, 700)
+    sched, us = eng.schedule()
+    assert sched in (1, 2, 3, 4) and all(v > 0 for v in us.values())
+    assert us[sched] == min(us.values())
+    o = FastOracle(net, cfg, drive, precision=32)
+    o.step(700)
+    assert nets.rasters_equal(eng.read_raster(0, 700), o.raster())
+
+
 def test_csr_traversal_order_bit_exact(lib):
     net, cfg, drive = nets.izh_stdp(n=8000, k=60)
     eng = SimulationEngine(net, cfg, drive)
@@ -256,6 +282,25 @@ def test_checkpoint_resume_bit_exact(lib):
     for key in ("v", "u", "pre_trace", "post_trace", "last_spike_step", "w"):
         assert np.array_equal(st[key], full_state[key]), key
     assert nets.rasters_equal(c.read_raster(200, 200), full_raster)
+
+
+def test_reupload_same_and_other_shape(lib):
+    # re-uploading a same-shaped network reuses buffers (and captured graphs);
+    # a different shape reallocates; both give the fresh engine's results
+    net, cfg, drive = nets.izh_stdp(n=20_000, k=50)
+    cfg.graph_chunk = 100
+    eng = gpu_run(net, cfg, drive, 300)
+    ref = (eng.read_raster(0, 300), eng.download_state()["w"])
+    eng._upload(net)
+    eng.run(300)
+    assert nets.rasters_equal(eng.read_raster(0, 300), ref[0])
+    assert np.array_equal(eng.download_state()["w"], ref[1])
+    net2, _, _ = nets.izh_stdp(n=20_000, k=40, seed=7)
+    eng._upload(net2)
+    eng.run(200)
+    o = FastOracle(net2, cfg, drive, precision=32)
+    o.step(200)
+    assert nets.rasters_equal(eng.read_raster(0, 200), o.raster())
 
 
 def test_empty_and_ragged_networks(lib):
