@@ -260,6 +260,33 @@ ns_status ns_get_stream(ns_handle* h, void** stream);
  * homeostasis kernels to kernel_ms[4] / launches[4]. Same numerics as ns_step. */
 ns_status ns_profile_steps(ns_handle* h, uint32_t n_steps, double* kernel_ms, uint64_t* launches);
 
+/* --- allocation-free step (no counterpart in the reference) -------------
+ * For callers that cannot allocate device memory where they step neurons:
+ * one recorded into their own CUDA stream capture (cudaMalloc cannot be
+ * captured), a latency-bound loop that cannot take the synchronisation an
+ * allocation may cause, or a plugin confined to another framework's memory
+ * pool. One Izhikevich step (izhikevich.rs:20-52, the same float arithmetic
+ * as ns_step) of n neurons held in the caller's device arrays v, u (updated
+ * in place), a, b, c, d and current (input current of this step, NULL = 0),
+ * followed by ordered spike compaction: spikes_out (device, capacity n)
+ * receives the ascending indices of the neurons that spiked and
+ * *n_spikes_out (device) their number. Work is enqueued on `stream`
+ * (a cudaStream_t; NULL = legacy default stream) and not waited for.
+ * The compaction's scratch is a fixed device array of NS_NOALLOC_MAX_NEURONS
+ * + 1024 words (4 MiB + 4 KiB) that every GPU which loads the library holds
+ * until exit; n above NS_NOALLOC_MAX_NEURONS is rejected with
+ * NS_ERR_INVALID_ARG. Nothing is allocated or freed. The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress with that
+ * device current): make that first call before any stream capture. All calls
+ * on a device share the one scratch array, so calls whose kernels overlap on
+ * the GPU (different streams without ordering between them) race; order
+ * them on one stream. */
+#define NS_NOALLOC_MAX_NEURONS 1048576u
+ns_status ns_izhikevich_step_noalloc(uint64_t n, float* v, float* u, const float* a,
+                                     const float* b, const float* c, const float* d,
+                                     const float* current, float dt_ms, uint32_t* spikes_out,
+                                     uint32_t* n_spikes_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

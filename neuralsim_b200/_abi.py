@@ -97,6 +97,8 @@ SIGNATURES = {
     "ns_get_stream": (C.c_int32, [_P, C.POINTER(_P)]),
     "ns_counters": (C.c_int32, [_P, _U64P]),
     "ns_profile_steps": (C.c_int32, [_P, C.c_uint32, C.POINTER(C.c_double), _U64P]),
+    "ns_izhikevich_step_noalloc": (C.c_int32, [C.c_uint64, _P, _P, _P, _P, _P, _P, _P,
+                                               C.c_float, _P, _P, _P]),
     "ns_gen_topology": (C.c_int32, [C.c_uint64, C.c_uint32, C.c_uint64, _P, _P, _P, C.c_int32]),
     "ns_gen_weights": (C.c_int32, [C.c_uint32, C.c_uint64, C.c_uint64, _P, C.c_uint64,
                                    C.c_uint64, C.c_double, C.c_double, C.c_double, C.c_double,
