@@ -53,6 +53,7 @@ def args_():
     p.add_argument("--cpu-seconds", type=float, default=20.0)
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-extra", action="store_true", help="skip the LIF and HH configuration lines")
     return p.parse_args()
 
 
@@ -240,6 +241,10 @@ def run_ours(a):
     if not a.no_e2e:
         e2e = run_e2e(a, net, cfg, drive, local, dist)
 
+    extra = None
+    if rank == 0 and not a.no_extra:
+        extra = run_extra_configs(local)
+
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
         cpu = run_cpu_baseline(net, cfg, drive, a.cpu_seconds)
@@ -299,12 +304,55 @@ def run_ours(a):
             "gpu_launches": launches,
             "e2e": e2e,
             "cpu_baseline": cpu,
+            "other_configs": extra,
         }
         print(json.dumps(out), flush=True)
     eng.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def timed_run(eng, steps, stream):
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    c0 = eng.counters()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    eng.run(steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    c1 = eng.counters()
+    return e0.elapsed_time(e1), c1[1] - c0[1], c1[3] - c0[3]
+
+
+def run_extra_configs(local):
+    """The other configurations on this GPU: the plain LIF network (10k / 1M,
+    dt 0.1 ms, 1 ms delay, 1 s) and the plain Hodgkin-Huxley network (100k /
+    10M, Rush-Larsen, dt 0.01 ms, 1 ms delay), each timed with windowed
+    stepping (W = delay) and with one pass per step."""
+    import torch
+    from neuralsim_b200 import SimulationEngine, configs
+    out = {}
+    for name, builder, steps, warm in (("lif_c1", configs.lif_c1, 10_000, 2_000),
+                                       ("hh_c4", configs.hh_c4, 20_000, 2_000)):
+        net, cfg, drive, full_steps = builder()
+        cfg.device = local
+        res = {"neurons": net.n, "synapses": net.m, "dt_ms": cfg.dt_ms,
+               "delay_steps": cfg.delay_steps, "timed_steps": steps}
+        for label, wsteps in (("windowed", 0), ("per_step", 1)):
+            cfg.window_steps = wsteps
+            eng = SimulationEngine(net, cfg, drive)
+            stream = torch.cuda.ExternalStream(eng.stream(), device=local)
+            eng.run(warm)
+            ms, spikes, events = timed_run(eng, steps, stream)
+            eng.close()
+            res[label] = {"ns_per_step": ms * 1e6 / steps,
+                          "x_realtime": (steps * cfg.dt_ms) / ms,
+                          "events_per_s": events / (ms / 1e3),
+                          "spikes_per_step": spikes / steps}
+        out[name] = res
+    return out
 
 
 def run_e2e(a, net, cfg, drive, local, dist):

@@ -143,6 +143,11 @@ typedef struct ns_config {
    * blocks per SM, 4 = split with a narrow (2 blocks/SM) LTD grid that leaves
    * room for the neuron kernel. All give bit-identical results. */
   uint32_t step_schedule;
+  /* windowed stepping for delay_steps >= 2 without STDP or homeostasis: W
+   * steps per neuron kernel (W <= delay_steps), one row-walk pass per window.
+   * 0 = on with W = delay_steps (capped at 1024), 1 = off (one pass per
+   * step), W > 1 = on with that W. Results are identical either way. */
+  uint32_t window_steps;
 } ns_config;
 
 /* Fills cfg with the reference defaults: LIF, DIRECT_DECAY, dt 0.5 ms

@@ -38,7 +38,7 @@ class NsConfig(C.Structure):
         ("homeostatic_target_rate", C.c_double), ("homeostatic_tau", C.c_double),
         ("contribution_tau", C.c_double), ("spike_log_capacity", C.c_uint64),
         ("spike_log_steps", C.c_uint32), ("graph_chunk", C.c_uint32),
-        ("step_schedule", C.c_uint32),
+        ("step_schedule", C.c_uint32), ("window_steps", C.c_uint32),
     ]
 
 

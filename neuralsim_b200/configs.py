@@ -100,8 +100,11 @@ def izh_c2(n=1_000_000, k=100, seed=44, threads=0, weight_format=A.WEIGHT_BF16):
 # HH_AREA_CM2 converts nS to mS/cm^2 (g[mS/cm^2] = g[nS] * 1e-6 / area), and
 # the 20 Hz drive is K_EXT independent inputs, each event adding the mean
 # synaptic conductance (one Bernoulli per neuron-step, p = K_EXT*20 Hz*dt).
+# 5e-6 cm^2 (a 500 um^2 soma) gives an active asynchronous network of about
+# 40 Hz; at 1e-5 cm^2 the same network is silent (measured on the oracle,
+# 2000 neurons, 100 ms: 0 Hz at 1e-5, 13 Hz decaying at 6e-6, 40 Hz at 5e-6).
 # ---------------------------------------------------------------------------
-HH_AREA_CM2 = 1.0e-5
+HH_AREA_CM2 = 5.0e-6
 HH_K_EXT = 100
 HH_DELAY_MS = 1.0
 

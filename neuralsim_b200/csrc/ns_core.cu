@@ -14,6 +14,7 @@
 
 #include "../../include/neuralsim.h"
 #include "ns_kernels.cuh"
+#include "ns_window.cuh"
 
 using ns::NsDev;
 
@@ -34,6 +35,8 @@ struct ns_handle {
   std::vector<void*> neuron_allocs, csr_allocs, log_allocs;
   std::map<void*, size_t> alloc_bytes;   // size of every allocation made by dalloc
   uint64_t next_tune_step = 0;          // autotuner runs at step 0 and once after 2000
+  uint32_t win = 0;                     // window length W (0 = step-synchronous)
+  int win_rows_blocks = 0;
   std::map<uint32_t, cudaGraphExec_t> graphs;
   uint64_t launches = 0;
   int prop_blocks = 0;
@@ -470,6 +473,45 @@ uint64_t launches_per_step(const ns_handle* h, uint32_t sched) {
   return 2u + ((split && h->cfg.stdp_enabled) ? 1u : 0u) + (h->cfg.homeostasis_enabled ? 1u : 0u);
 }
 
+typedef void (*window_fn)(NsDev, uint32_t, uint32_t);
+
+window_fn pick_window(uint32_t model, uint32_t mode) {
+#define NSW(MO, MD) if (model == MO && mode == MD) return ns::k_window<MO, MD>;
+  NSW(0, 0) NSW(0, 1) NSW(0, 2) NSW(0, 4)
+  NSW(1, 0) NSW(1, 1) NSW(1, 2) NSW(1, 4)
+  NSW(2, 0) NSW(2, 1) NSW(2, 2) NSW(2, 4)
+#undef NSW
+  return nullptr;
+}
+
+window_fn pick_window_rows(uint32_t mode, uint32_t wf) {
+  bool cond = mode == NS_INPUT_CONDUCTANCE_REF || mode == NS_INPUT_CONDUCTANCE_FRESH;
+  bool bf = wf == NS_WEIGHT_BF16;
+  if (cond) return bf ? ns::k_window_rows<true, true> : ns::k_window_rows<true, false>;
+  return bf ? ns::k_window_rows<false, true> : ns::k_window_rows<false, false>;
+}
+
+// Window length the handle's configuration allows (0 = step-synchronous).
+uint32_t window_len(const ns_config& c) {
+  if (c.stdp_enabled || c.homeostasis_enabled || c.delay_steps < 2 || c.window_steps == 1) return 0;
+  if (c.input_mode == NS_INPUT_CONDUCTANCE_REF) return 0;
+  uint32_t w = c.window_steps > 1 ? std::min(c.window_steps, c.delay_steps) : c.delay_steps;
+  return std::min<uint32_t>(w, 1024u);
+}
+
+// Enqueues a window of Wc steps starting at graph-node offset j0.
+cudaError_t enqueue_window(ns_handle* h, uint32_t j0, uint32_t Wc) {
+  const uint32_t nseg = h->d.nseg;
+  pick_window(h->cfg.model, h->cfg.input_mode)<<<nseg, ns::kWinThreads, 0, h->st>>>(h->d, j0, Wc);
+  pick_window_rows(h->cfg.input_mode, h->cfg.weight_format)
+      <<<h->win_rows_blocks, 256, 0, h->st>>>(h->d, j0, Wc);
+  ns::k_window_scan<<<Wc, 256, 0, h->st>>>(h->d, Wc);
+  if (h->d.log_idx) ns::k_window_log<<<Wc, 256, 0, h->st>>>(h->d, Wc);
+  ns::k_window_commit<<<1, 32, 0, h->st>>>(h->d, j0, Wc);
+  h->launches += h->d.log_idx ? 5 : 4;
+  return cudaGetLastError();
+}
+
 ns_status get_graph(ns_handle* h, uint32_t S, uint32_t sched, cudaGraphExec_t* out) {
   const uint32_t key = S * 4u + sched;
   auto it = h->graphs.find(key);
@@ -478,8 +520,13 @@ ns_status get_graph(ns_handle* h, uint32_t S, uint32_t sched, cudaGraphExec_t* o
   CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
   bool pending = false;
   cudaError_t ce = cudaSuccess;
-  for (uint32_t j = 0; j < S && ce == cudaSuccess; ++j) ce = enqueue_step(h, j, &pending, sched);
-  if (ce == cudaSuccess) ce = join_ltd(h, &pending);
+  if (h->win) {
+    for (uint32_t j = 0; j < S && ce == cudaSuccess; j += h->win)
+      ce = enqueue_window(h, j, std::min(h->win, S - j));
+  } else {
+    for (uint32_t j = 0; j < S && ce == cudaSuccess; ++j) ce = enqueue_step(h, j, &pending, sched);
+    if (ce == cudaSuccess) ce = join_ltd(h, &pending);
+  }
   ns::k_advance<<<1, 1, 0, h->st>>>(h->ctl, S);
   cudaError_t ee = cudaStreamEndCapture(h->st, &g);
   if (ce != cudaSuccess || ee != cudaSuccess)
@@ -505,9 +552,17 @@ ns_status run_steps(ns_handle* h, uint32_t n, uint32_t sched) {
     if (r) return r;
     while (left >= S) {
       CK(cudaGraphLaunch(ex, h->st));
-      h->launches += (uint64_t)S * launches_per_step(h, sched) + 1;
+      if (h->win) h->launches += ((S + h->win - 1) / h->win) * (h->d.log_idx ? 5 : 4) + 1;
+      else h->launches += (uint64_t)S * launches_per_step(h, sched) + 1;
       left -= S;
     }
+  }
+  if (left > 0 && h->win) {
+    for (uint32_t j = 0; j < left; j += h->win) CK(enqueue_window(h, j, std::min(h->win, left - j)));
+    ns::k_advance<<<1, 1, 0, h->st>>>(h->ctl, left);
+    h->launches += 1;
+    CK(cudaGetLastError());
+    left = 0;
   }
   if (left > 0) {
     bool pending = false;
@@ -529,7 +584,7 @@ uint32_t kTuneWindow = 100;
 ns_status autotune(ns_handle* h, uint32_t budget, uint32_t* used) {
   *used = 0;
   if (h->cfg.step_schedule != 0) return NS_OK;
-  if (!h->cfg.stdp_enabled) { h->sched = 1; return NS_OK; }
+  if (!h->cfg.stdp_enabled || h->win) { h->sched = 1; return NS_OK; }
   if (budget < kTuneWindow) return NS_OK;
   unsigned long long step = 0;
   CK(cudaMemcpyAsync(&step, &h->ctl->step_base, 8, cudaMemcpyDeviceToHost, h->st));
@@ -642,7 +697,7 @@ ns_status ns_create(const ns_config* cfg, ns_handle** out) {
   *out = nullptr;
   const ns_config& c = *cfg;
   if (c.model > 2 || c.input_mode > 4 || c.hh_integrator > 1 || c.weight_format > 1 ||
-      c.step_schedule > 4)
+      c.step_schedule > 4 || c.window_steps > 4096)
     return fail(h, NS_ERR_INVALID_ARG, "unknown model / input mode / integrator / weight format");
   if (!(c.dt_ms > 0) || !is_fin(c.dt_ms)) return fail(h, NS_ERR_INVALID_ARG, "dt_ms must be > 0");
   if (c.delay_steps < 1 || c.delay_steps > 4096) return fail(h, NS_ERR_INVALID_ARG, "delay_steps in [1, 4096]");
@@ -872,6 +927,7 @@ static ns_status alloc_dynamic(ns_handle* h) {
       (!c.homeostasis_enabled || (d.contrib && h->alloc_bytes[d.contrib] == std::max<uint64_t>(h->m, 1) * 4))) {
     // same shape: clear in place, keep pointers (and graphs)
     CK(cudaMemsetAsync(d.acc, 0, acc_bytes, h->st));
+    if (d.inbits) CK(cudaMemsetAsync(d.inbits, 0, h->alloc_bytes[d.inbits], h->st));
     if (d.contrib) CK(cudaMemsetAsync(d.contrib, 0, h->alloc_bytes[d.contrib], h->st));
     CK(cudaMemsetAsync(h->ctl, 0, sizeof(ns::Ctl), h->st));
     CK(cudaStreamSynchronize(h->st));
@@ -901,6 +957,23 @@ static ns_status alloc_dynamic(ns_handle* h) {
     if ((st = dalloc(h, B, &d.log_off, (uint64_t)c.spike_log_steps + 1))) return st;
   }
   d.trace_pos = nullptr; d.trace_off = nullptr; d.trace_cap = 0;
+  // windowed stepping buffers
+  h->win = window_len(c);
+  d.inbits = nullptr; d.seg_cnt = nullptr; d.seg_lst = nullptr; d.seg_off = nullptr;
+  d.step_total = nullptr; d.nseg = 0; d.wmax = 0;
+  if (h->win) {
+    d.nseg = (uint32_t)(h->n_pad / ns::kWinThreads);
+    d.wmax = h->win;
+    if ((st = dalloc(h, B, &d.inbits, (uint64_t)c.delay_steps * (h->n_pad >> 5)))) return st;
+    if ((st = dalloc(h, B, &d.seg_cnt, (uint64_t)h->win * d.nseg))) return st;
+    if ((st = dalloc(h, B, &d.seg_lst, (uint64_t)h->win * h->n_pad))) return st;
+    if ((st = dalloc(h, B, &d.seg_off, (uint64_t)h->win * (d.nseg + 1)))) return st;
+    if ((st = dalloc(h, B, &d.step_total, h->win))) return st;
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pick_window_rows(c.input_mode, c.weight_format), 256, 0) != cudaSuccess || nb < 1) nb = 4;
+    h->win_rows_blocks = h->sms * nb;
+    cudaGetLastError();
+  }
   // reset the control block: counters, log, tickets
   CK(cudaMemsetAsync(h->ctl, 0, sizeof(ns::Ctl), h->st));
   CK(cudaStreamSynchronize(h->st));
@@ -1284,6 +1357,12 @@ ns_status ns_upload_state(ns_handle* h, const ns_neuron_soa* in, const float* w_
     }
     cudaFree(tmpw);
     CK(e);
+  }
+  if (d.inbits) {
+    fill_scalars(h);  // sizes the kernel reads (a fresh handle may not have stepped yet)
+    ns::k_rebuild_inbits<<<h->sms * 8, 256, 0, h->st>>>(d, (uint32_t)h->ntypes_acc);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->st));
   }
   ns::Ctl c{};
   c.step_base = step;

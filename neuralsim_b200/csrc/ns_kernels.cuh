@@ -100,6 +100,14 @@ struct NsDev {
   unsigned long long* trace_pos;   // traced step only
   const unsigned long long* trace_off;
   unsigned long long trace_cap;
+  // windowed stepping (delay >= 2, no plasticity): "slot has input" bits
+  // [D][n_pad/32], and per-window spike segments of 256 neurons
+  uint32_t* inbits;
+  uint32_t* seg_cnt;               // [W][nseg]
+  uint32_t* seg_lst;               // [W][n_pad]
+  uint32_t* seg_off;               // [W][nseg + 1]
+  uint32_t* step_total;            // [W]
+  uint32_t nseg, wmax;
 };
 
 __device__ __forceinline__ bool bit_of(const uint32_t* bm, uint32_t i) {
@@ -249,6 +257,73 @@ __device__ __forceinline__ bool model_step(const NsDev& d, NState& s, const floa
   }
 }
 
+// Drive of neuron i at step k from its Philox draw y (kinds 1, 2, 4) or its
+// Gaussian sample z (kind 3): added current, voltage kick, added conductance.
+__device__ __forceinline__ void drive_of(const NsDev& d, const U4& y, float z, uint8_t inh,
+                                         float& addI, float& kick, float& addg) {
+  addI = 0.f; kick = 0.f; addg = 0.f;
+  if (d.drive_kind == 1) {
+    if (unif(y.x) < d.drive_p) addI = unif(y.y) * d.drive_amp;
+  } else if (d.drive_kind == 2) {
+    if (y.x < d.p_thr) kick = d.drive_amp;
+  } else if (d.drive_kind == 4) {
+    if (y.x < d.p_thr) addg = d.drive_amp;
+  } else if (d.drive_kind == 3) {
+    addI = (inh ? d.sig_i : d.sig_e) * z;
+  }
+}
+
+// Gaussian pair of the draw x: cos for the even neuron, sin for the odd one
+// (Box-Muller on the drive's own log / sincos).
+__device__ __forceinline__ void gauss_pair(const U4& x, float& z0, float& z1) {
+  const float u1 = unif_open(x.x), u2 = unif(x.y);
+  const float l = ln_f(u1);
+  const float rr = sqrtf(-2.0f * l);
+  float sn, cs;
+  sincos_2pi(u2, &sn, &cs);
+  z0 = rr * cs;
+  z1 = rr * sn;
+}
+
+// Input assembly and model update of one neuron at step k (the arithmetic
+// the float oracle mirrors). S: delivered synaptic input per accumulator
+// type; G: the neuron's conductances (conductance modes).
+template <int MODEL, int MODE>
+__device__ __forceinline__ bool update_one(const NsDev& d, uint64_t k, uint64_t i, NState& st,
+                                           const float* par, int rs, const float* S, float* G,
+                                           float addI, float kick, float addg, const Kick* kicks,
+                                           int nk) {
+  float Iv = 0.f, kk = 0.f;
+  const float vi = st.v;
+  if (MODE == 0) {
+    Iv = st.I;
+    if (k > 0) Iv = (Iv + S[0]) * d.decay_I;
+  } else if (MODE == 1) {
+    kk = S[0];
+  } else if (MODE == 2) {
+    Iv = S[0];
+  } else {
+    float isyn = 0.f;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      float inc = S[t] * kSyn[t].gmax;
+      if (kSyn[t].mg) inc = inc * (1.0f / (1.0f + (1.0f / 3.57f) * expf(-0.062f * vi)));
+      float g = G[t] * d.Gdec[t] + inc;
+      if (t == 0) g = g + addg;
+      G[t] = g;
+      isyn = isyn + g * (kSyn[t].erev - vi);
+    }
+    Iv = (MODE == 3) ? st.I + isyn : isyn;
+  }
+  Iv = Iv + addI;
+  for (int q = 0; q < nk; ++q)
+    if (kicks[q].target == (uint32_t)i) Iv = Iv + kicks[q].amt;
+  kk = kk + kick;
+  const bool sp = model_step<MODEL>(d, st, par, rs, Iv, kk, MODE == 1);
+  st.I = Iv;
+  return sp;
+}
+
 // ---------------------------------------------------------------------------
 // Kernel 1: fused drive + neuron update + trace decay + ordered compaction.
 // Thread t of tile T owns the neuron pairs (T*2048 + r*512 + 2t, +1), r < 4,
@@ -359,6 +434,10 @@ __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
     uchar2 ih = make_uchar2(0, 0);
     if (d.drive_kind == 3) ih = *reinterpret_cast<const uchar2*>(d.inh + i0);
     // ---- delivered synaptic input for this step (the slot is cleared) ----
+    if (d.inbits && lane == 0) {
+      uint32_t* ib = d.inbits + (uint64_t)slot * (d.n_pad >> 5) + ((i0 - 2 * (uint64_t)lane) >> 5);
+      *reinterpret_cast<uint2*>(ib) = make_uint2(0u, 0u);
+    }
     float S[NT][2];
 #pragma unroll
     for (int t = 0; t < NT; ++t) {
@@ -370,61 +449,25 @@ __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
     // ---- drive draws: one Philox per pair ----
     const U4 x = make_drive_draw(d, i0, k);
     float z[2] = {0.f, 0.f};
-    if (d.drive_kind == 3) {
-      const float u1 = unif_open(x.x), u2 = unif(x.y);
-      const float l = ln_f(u1);
-      const float rr = sqrtf(-2.0f * l);
-      float sn, cs;
-      sincos_2pi(u2, &sn, &cs);
-      z[0] = rr * cs;
-      z[1] = rr * sn;
-    }
+    if (d.drive_kind == 3) gauss_pair(x, z[0], z[1]);
     const uint8_t inhv[2] = {ih.x, ih.y};
     bool spk[2];
 #pragma unroll
     for (int e = 0; e < 2; ++e) {
       const uint64_t i = i0 + e;
-      float addI = 0.f, kick = 0.f, addg = 0.f;
-      if (d.drive_kind == 1 || d.drive_kind == 2 || d.drive_kind == 4) {
-        const U4 y = (e == 0) ? x : draw(d.seed, (uint32_t)i, k, kStreamDrive);
-        if (d.drive_kind == 1) {
-          if (unif(y.x) < d.drive_p) addI = unif(y.y) * d.drive_amp;
-        } else if (d.drive_kind == 2) {
-          if (y.x < d.p_thr) kick = d.drive_amp;
-        } else {
-          if (y.x < d.p_thr) addg = d.drive_amp;
-        }
-      } else if (d.drive_kind == 3) {
-        addI = (inhv[e] ? d.sig_i : d.sig_e) * z[e];
-      }
-      float Iv = 0.f, kk = 0.f;
-      const float vi = st[e].v;
-      if (MODE == 0) {
-        Iv = st[e].I;
-        if (k > 0) Iv = (Iv + S[0][e]) * d.decay_I;
-      } else if (MODE == 1) {
-        kk = S[0][e];
-      } else if (MODE == 2) {
-        Iv = S[0][e];
-      } else {
-        float isyn = 0.f;
+      float addI, kick, addg;
+      const U4 y = (e == 1 && (d.drive_kind == 1 || d.drive_kind == 2 || d.drive_kind == 4))
+                       ? draw(d.seed, (uint32_t)i, k, kStreamDrive) : x;
+      drive_of(d, y, z[e], inhv[e], addI, kick, addg);
+      float Se[NT], Ge[4];
 #pragma unroll
-        for (int t = 0; t < 4; ++t) {
-          float inc = S[t][e] * kSyn[t].gmax;
-          if (kSyn[t].mg) inc = inc * (1.0f / (1.0f + (1.0f / 3.57f) * expf(-0.062f * vi)));
-          float g = G[t][e] * d.Gdec[t] + inc;
-          if (t == 0) g = g + addg;
-          G[t][e] = g;
-          isyn = isyn + g * (kSyn[t].erev - vi);
-        }
-        Iv = (MODE == 3) ? st[e].I + isyn : isyn;
-      }
-      Iv = Iv + addI;
-      for (int q = 0; q < nk; ++q)
-        if (s_kick[q].target == (uint32_t)i) Iv = Iv + s_kick[q].amt;
-      kk = kk + kick;
-      bool sp = model_step<MODEL>(d, st[e], par[e], rs[e], Iv, kk, MODE == 1);
-      st[e].I = Iv;
+      for (int t = 0; t < NT; ++t) Se[t] = S[t][e];
+#pragma unroll
+      for (int t = 0; t < 4; ++t) Ge[t] = COND ? G[t][e] : 0.f;
+      const bool sp = update_one<MODEL, MODE>(d, k, i, st[e], par[e], rs[e], Se, Ge, addI, kick,
+                                              addg, s_kick, nk);
+#pragma unroll
+      for (int t = 0; t < 4; ++t) if (COND) G[t][e] = Ge[t];
       spk[e] = sp && (i < d.n);
     }
     // ---- traces: per-step decay here; the spike-time bump (double decay of
@@ -683,6 +726,8 @@ __device__ __forceinline__ void row_item(const NsDev& d, const StepCtx& c, uint3
       const float val = (COND && (ty == 1 || ty == 2)) ? fabsf(w[q]) : w[q];
       atomicAdd(d.acc + ((uint64_t)ty * d.D + c.slot) * d.n_pad + cc[q],
                 (unsigned long long)to_fix(val));
+      if (d.inbits)
+        atomicOr(d.inbits + (uint64_t)c.slot * (d.n_pad >> 5) + (cc[q] >> 5), 1u << (cc[q] & 31));
       if (d.trace_pos) {
         const unsigned long long tp = tbase + (e - beg);
         if (tp < d.trace_cap) d.trace_pos[tp] = e;

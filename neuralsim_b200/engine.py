@@ -92,6 +92,7 @@ class SimConfig:
     spike_log_steps: int = 0
     graph_chunk: int = 1000
     step_schedule: int = 0      # 0 autotune, 1 fused, 2 split, 3 fused (4 blocks/SM)
+    window_steps: int = 0       # 0 auto (= delay), 1 off, W > 1 explicit
 
     def to_c(self):
         c = A.NsConfig()
