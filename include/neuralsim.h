@@ -145,8 +145,9 @@ typedef struct ns_config {
   uint32_t step_schedule;
   /* windowed stepping for delay_steps >= 2 without STDP or homeostasis: W
    * steps per neuron kernel (W <= delay_steps), one row-walk pass per window.
-   * 0 = on with W = delay_steps (capped at 1024), 1 = off (one pass per
-   * step), W > 1 = on with that W. Results are identical either way. */
+   * 0 = on, W tuned at the first ns_step among delay_steps (capped at 1024)
+   * and its successive halves down to 2 (ns_get_window), 1 = off (one pass
+   * per step), W > 1 = on with that W. Results are identical either way. */
   uint32_t window_steps;
 } ns_config;
 
@@ -213,6 +214,36 @@ ns_status ns_upload_csr(ns_handle* h, uint64_t n, uint64_t m, const uint64_t* ro
 /* Drive: the noise loop of engine.rs:273-287 (host RNG in the reference). */
 ns_status ns_set_drive(ns_handle* h, const ns_drive* d);
 
+/* --- batches: many independent networks in one launch ------------------
+ * Replaces the per-genome engines of Population::evolve_generation
+ * (src/evolution/population.rs:117-124) and one-engine-per-point parameter
+ * sweeps. One network of a batch: its neuron SoA (the same fields and
+ * defaults as ns_upload_neurons), its CSR in local indices (the same rules as
+ * ns_upload_csr) and the seed of its own drive stream. */
+typedef struct ns_net_desc {
+  const ns_neuron_soa* neurons;
+  uint64_t m;
+  const uint64_t* row_ptr;   /* n + 1 entries, row_ptr[0] == 0, row_ptr[n] == m */
+  const uint32_t* col;       /* m local target indices < n */
+  const float* w;            /* m */
+  const uint8_t* syn_type;   /* m or NULL; all networks give it or none */
+  const uint8_t* plastic;    /* m or NULL; all networks give it or none */
+  uint64_t seed;             /* drive stream: the stream a lone handle with
+                                ns_config.seed == seed would draw */
+} ns_net_desc;
+/* Concatenates the networks block-diagonally (network q owns neurons
+ * first_neuron_out[q] .. first_neuron_out[q+1]-1 of the handle) and uploads
+ * them. Every step kernel then runs over all networks at once; network q
+ * draws its drive from its own seed and its local neuron indices, so its
+ * raster equals the one it produces alone on a handle with the same config
+ * and seed. Spike logs, state and weights use the concatenated indices.
+ * first_neuron_out: n_nets + 1 entries or NULL. The reference-uniform drive
+ * (global kicks per network) is not available for batches
+ * (NS_ERR_UNSUPPORTED at ns_step). A later ns_upload_neurons ends batch
+ * mode. A batch of the same networks' sizes reuses the device buffers. */
+ns_status ns_upload_batch(ns_handle* h, uint32_t n_nets, const ns_net_desc* nets,
+                          uint64_t* first_neuron_out);
+
 /* --- stepping: SimulationEngine::step / simulate_ms, engine.rs:254-680,
  *     :792-797; GpuBackend::step_neurons + step_spmv, gpu_backend.rs:852-981.
  *     Runs n_steps on the device (CUDA-graph chunks) and blocks until done. */
@@ -248,6 +279,12 @@ ns_status ns_step_traced(ns_handle* h, uint64_t* pos_out, uint64_t cap, uint64_t
 /* Schedule in use (0 while the autotuner has not decided) and the measured
  * microseconds per step of schedules 1..4 in us_per_step[4] (0 if untimed). */
 ns_status ns_get_schedule(ns_handle* h, uint32_t* schedule, double* us_per_step);
+
+/* Windowed stepping: the window length in use (0 = step-synchronous), and
+ * the candidates the window tuner timed with their microseconds per step
+ * (0 where untimed). The tuner runs at the first ns_step when
+ * ns_config.window_steps is 0. */
+ns_status ns_get_window(ns_handle* h, uint32_t* window, uint32_t* candidates, double* us_per_step);
 
 /* Kernel launches issued by this handle since creation (own kernels only). */
 ns_status ns_launch_count(ns_handle* h, uint64_t* launches);

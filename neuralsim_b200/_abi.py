@@ -62,6 +62,14 @@ class NsNeuronSoa(C.Structure):
     ]
 
 
+class NsNetDesc(C.Structure):
+    _fields_ = [
+        ("neurons", C.POINTER(NsNeuronSoa)), ("m", C.c_uint64), ("row_ptr", C.c_void_p),
+        ("col", C.c_void_p), ("w", C.c_void_p), ("syn_type", C.c_void_p),
+        ("plastic", C.c_void_p), ("seed", C.c_uint64),
+    ]
+
+
 class NsStepStats(C.Structure):
     _fields_ = [
         ("steps_done", C.c_uint64), ("spikes", C.c_uint64), ("output_spikes", C.c_uint64),
@@ -82,6 +90,8 @@ SIGNATURES = {
     "ns_upload_neurons": (C.c_int32, [_P, C.POINTER(NsNeuronSoa)]),
     "ns_upload_csr": (C.c_int32, [_P, C.c_uint64, C.c_uint64, _P, _P, _P, _P, _P]),
     "ns_set_drive": (C.c_int32, [_P, C.POINTER(NsDrive)]),
+    "ns_upload_batch": (C.c_int32, [_P, C.c_uint32, C.POINTER(NsNetDesc), _P]),
+    "ns_get_window": (C.c_int32, [_P, _P, _P, _P]),
     "ns_step": (C.c_int32, [_P, C.c_uint32, C.POINTER(NsStepStats)]),
     "ns_read_spikes": (C.c_int32, [_P, C.c_uint64, C.c_uint32, _P, _P, C.c_uint64, _U64P]),
     "ns_clear_spike_log": (C.c_int32, [_P]),

@@ -130,3 +130,38 @@ def hh_c4(n=100_000, k=100, seed=46, threads=0, integrator=A.HH_RUSH_LARSEN, dt_
     g_mean = float(np.exp(-3.0 + 0.5 * 0.5 * 0.5) * scale)
     drive = Drive(A.DRIVE_POISSON_CONDUCTANCE, p=HH_K_EXT * 20.0 * dt_ms / 1000.0, amplitude=g_mean)
     return net, cfg, drive, int(round(1000.0 / dt_ms))
+
+
+# ---------------------------------------------------------------------------
+# C3: batched sweep, 256 independent LIF networks, sizes log-uniform in
+# [2,000, 50,000], in-degree uniform in {50..200}, per network tau_m ~
+# U[10,30] ms and inhibitory/excitatory weight ratio g ~ U[3,6]
+# (w_exc = +0.5 mV, w_inh = -g * 0.5 mV, each x U[0.8,1.2] as in C1), 80/20,
+# the C1 drive (Poisson 8 Hz, 0.8 mV kicks), 1 ms delay, V_rest -65 mV,
+# dt 0.1 ms, 1000 steps. Network q is generated and driven from its own seed.
+# ---------------------------------------------------------------------------
+def lif_batch_c3(n_nets=256, seed=45, size_range=(2_000, 50_000), k_range=(50, 200), threads=0,
+                 drive=None):
+    rng = np.random.default_rng(seed)
+    lo, hi = np.log(size_range[0]), np.log(size_range[1])
+    sizes = np.exp(rng.uniform(lo, hi, n_nets)).astype(np.int64)
+    ks = rng.integers(k_range[0], k_range[1] + 1, n_nets)
+    taus = rng.uniform(10.0, 30.0, n_nets)
+    gs = rng.uniform(3.0, 6.0, n_nets)
+    nets, seeds = [], []
+    for q in range(n_nets):
+        n, k = int(sizes[q]), int(min(ks[q], sizes[q] - 1))
+        sq = seed * 1_000_003 + q
+        n_exc = int(round(0.8 * n))
+        rp, col = topology(n, k, sq, threads)
+        w, ty, _ = weights(A.GEN_W_SCALED, n, n_exc, rp, sq, 0.5, -float(gs[q]) * 0.5, 0.8, 1.2,
+                           threads=threads)
+        params = np.tile(np.array([-65.0, -50.0, -65.0, float(taus[q]), 2.0, 1.0], np.float32),
+                         (n, 1))
+        inh = (np.arange(n) >= n_exc).astype(np.uint8)
+        nets.append(Network(A.MODEL_LIF, params, rp, col, w, syn_type=ty, inhibitory=inh))
+        seeds.append(sq)
+    cfg = SimConfig(model=A.MODEL_LIF, input_mode=A.INPUT_DELTA_V, dt_ms=0.1, delay_steps=10,
+                    seed=seed, stdp_enabled=False, homeostasis_enabled=False)
+    drive = drive or Drive(A.DRIVE_POISSON_KICK, p=8.0 * 0.1 / 1000.0, amplitude=0.8)
+    return nets, seeds, cfg, drive, 1000

@@ -35,9 +35,12 @@ struct ns_handle {
   std::vector<void*> neuron_allocs, csr_allocs, log_allocs;
   std::map<void*, size_t> alloc_bytes;   // size of every allocation made by dalloc
   uint64_t next_tune_step = 0;          // autotuner runs at step 0 and once after 2000
-  uint32_t win = 0;                     // window length W (0 = step-synchronous)
+  uint32_t win = 0;                     // longest window W allowed (0 = step-synchronous)
+  uint32_t wcur = 0;                    // window length in use (<= win; chosen by the autotuner)
+  uint32_t tune_w[4] = {0, 0, 0, 0};    // window candidates timed, and their us per step
+  double tune_w_us[4] = {0, 0, 0, 0};
   int win_rows_blocks = 0;
-  std::map<uint32_t, cudaGraphExec_t> graphs;
+  std::map<uint64_t, cudaGraphExec_t> graphs;   // (window, steps, schedule)
   uint64_t launches = 0;
   int prop_blocks = 0;
   int fused_blocks[2] = {0, 0};
@@ -47,6 +50,10 @@ struct ns_handle {
   double tune_us[5] = {0, 0, 0, 0, 0};
   int homeo_blocks = 0;
   int ntypes_acc = 1;
+  // batch of networks: per-neuron network ids, per-network seeds and bases
+  std::vector<void*> batch_allocs;
+  uint32_t n_nets = 0;              // 0 = single network
+  bool batch_uploading = false;     // ns_upload_batch is calling the uploads
 };
 
 namespace {
@@ -109,8 +116,11 @@ cudaError_t snapshot_take(ns_handle* h, Snapshot& sn) {
   for (void* p : h->neuron_allocs) add(p);
   add(h->d.acc);
   add(h->d.contrib);
-  add(h->d.w16);
-  add(h->d.w32);
+  add(h->d.inbits);
+  if (h->cfg.stdp_enabled || h->cfg.homeostasis_enabled) {
+    add(h->d.w16);
+    add(h->d.w32);
+  }
   sn.regions.push_back({h->ctl, sizeof(ns::Ctl)});
   for (auto& r : sn.regions) {
     void* c = nullptr;
@@ -513,7 +523,7 @@ cudaError_t enqueue_window(ns_handle* h, uint32_t j0, uint32_t Wc) {
 }
 
 ns_status get_graph(ns_handle* h, uint32_t S, uint32_t sched, cudaGraphExec_t* out) {
-  const uint32_t key = S * 4u + sched;
+  const uint64_t key = ((uint64_t)(h->win ? h->wcur : 0u) << 40) | ((uint64_t)S * 4u + sched);
   auto it = h->graphs.find(key);
   if (it != h->graphs.end()) { *out = it->second; return NS_OK; }
   cudaGraph_t g;
@@ -521,8 +531,8 @@ ns_status get_graph(ns_handle* h, uint32_t S, uint32_t sched, cudaGraphExec_t* o
   bool pending = false;
   cudaError_t ce = cudaSuccess;
   if (h->win) {
-    for (uint32_t j = 0; j < S && ce == cudaSuccess; j += h->win)
-      ce = enqueue_window(h, j, std::min(h->win, S - j));
+    for (uint32_t j = 0; j < S && ce == cudaSuccess; j += h->wcur)
+      ce = enqueue_window(h, j, std::min(h->wcur, S - j));
   } else {
     for (uint32_t j = 0; j < S && ce == cudaSuccess; ++j) ce = enqueue_step(h, j, &pending, sched);
     if (ce == cudaSuccess) ce = join_ltd(h, &pending);
@@ -552,13 +562,13 @@ ns_status run_steps(ns_handle* h, uint32_t n, uint32_t sched) {
     if (r) return r;
     while (left >= S) {
       CK(cudaGraphLaunch(ex, h->st));
-      if (h->win) h->launches += ((S + h->win - 1) / h->win) * (h->d.log_idx ? 5 : 4) + 1;
+      if (h->win) h->launches += ((S + h->wcur - 1) / h->wcur) * (h->d.log_idx ? 5 : 4) + 1;
       else h->launches += (uint64_t)S * launches_per_step(h, sched) + 1;
       left -= S;
     }
   }
   if (left > 0 && h->win) {
-    for (uint32_t j = 0; j < left; j += h->win) CK(enqueue_window(h, j, std::min(h->win, left - j)));
+    for (uint32_t j = 0; j < left; j += h->wcur) CK(enqueue_window(h, j, std::min(h->wcur, left - j)));
     ns::k_advance<<<1, 1, 0, h->st>>>(h->ctl, left);
     h->launches += 1;
     CK(cudaGetLastError());
@@ -581,10 +591,16 @@ ns_status run_steps(ns_handle* h, uint32_t n, uint32_t sched) {
 // around one captured graph each; the fastest is kept. Runs at step 0 and
 // once more after the first 2000 steps, past the initial transient.
 uint32_t kTuneWindow = 100;
+ns_status autotune_window(ns_handle* h, uint32_t budget, uint32_t* used);
 ns_status autotune(ns_handle* h, uint32_t budget, uint32_t* used) {
   *used = 0;
+  if (h->win) {
+    h->sched = 1;
+    if (h->cfg.window_steps != 0) return NS_OK;
+    return autotune_window(h, budget, used);
+  }
   if (h->cfg.step_schedule != 0) return NS_OK;
-  if (!h->cfg.stdp_enabled || h->win) { h->sched = 1; return NS_OK; }
+  if (!h->cfg.stdp_enabled) { h->sched = 1; return NS_OK; }
   if (budget < kTuneWindow) return NS_OK;
   unsigned long long step = 0;
   CK(cudaMemcpyAsync(&step, &h->ctl->step_base, 8, cudaMemcpyDeviceToHost, h->st));
@@ -628,9 +644,67 @@ ns_status autotune(ns_handle* h, uint32_t budget, uint32_t* used) {
   return NS_OK;
 }
 
+// Window-length tuner for windowed networks (window_steps = 0): the
+// longest window the delay allows and its halves down to 2 replay the same
+// steps from one snapshot, the fastest is kept. Longer windows mean fewer
+// launches and state held in registers longer; shorter ones keep more
+// neurons' segments busy per row-walk launch. Runs once, at step 0.
+ns_status autotune_window(ns_handle* h, uint32_t budget, uint32_t* used) {
+  *used = 0;
+  if (h->next_tune_step != 0) return NS_OK;
+  uint32_t cand[4] = {0, 0, 0, 0};
+  int nc = 0;
+  for (uint32_t w = h->win; w >= 2 && nc < 4; w = (w + 1) / 2) {
+    if (nc == 0 || cand[nc - 1] != w) cand[nc++] = w;
+    if (w == 2) break;
+  }
+  // every candidate replays a whole number of windows of the longest one
+  const uint32_t T = std::max<uint32_t>(kTuneWindow / h->win, 1u) * h->win;
+  if (nc < 2 || budget < T) return NS_OK;
+  Snapshot sn;
+  CK(snapshot_take(h, sn));
+  cudaEvent_t e0, e1;
+  cudaError_t ce = cudaEventCreate(&e0);
+  if (ce == cudaSuccess) ce = cudaEventCreate(&e1);
+  if (ce != cudaSuccess) { snapshot_free(sn); return fail(h, NS_ERR_CUDA, cudaGetErrorString(ce)); }
+  double us[4] = {0, 0, 0, 0};
+  ns_status r = NS_OK;
+  for (int q = 0; q < nc && r == NS_OK; ++q) {
+    if (q > 0 && (ce = snapshot_restore(h, sn)) != cudaSuccess) break;
+    h->wcur = cand[q];
+    cudaGraphExec_t ex;
+    if ((r = get_graph(h, T, 1, &ex))) break;
+    float ms = 0;
+    if ((ce = cudaEventRecord(e0, h->st)) != cudaSuccess) break;
+    if ((ce = cudaGraphLaunch(ex, h->st)) != cudaSuccess) break;
+    if ((ce = cudaEventRecord(e1, h->st)) != cudaSuccess) break;
+    if ((ce = cudaEventSynchronize(e1)) != cudaSuccess) break;
+    if ((ce = cudaEventElapsedTime(&ms, e0, e1)) != cudaSuccess) break;
+    us[q] = ms * 1e3 / T;
+    h->launches += ((T + cand[q] - 1) / cand[q]) * (h->d.log_idx ? 5 : 4) + 1;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  snapshot_free(sn);
+  if (r) { h->wcur = h->win; return r; }
+  if (ce != cudaSuccess) { h->wcur = h->win; return fail(h, NS_ERR_CUDA, std::string("autotune: ") + cudaGetErrorString(ce)); }
+  int best = 0;
+  for (int q = 0; q < nc; ++q) {
+    h->tune_w[q] = cand[q];
+    h->tune_w_us[q] = us[q];
+    if (us[q] < us[best]) best = q;
+  }
+  h->wcur = cand[best];
+  h->next_tune_step = ~0ull;
+  *used = T;
+  return NS_OK;
+}
+
 ns_status ready(ns_handle* h) {
   if (!h->have_neurons || !h->have_csr) return fail(h, NS_ERR_STATE, "upload neurons and CSR first");
   if (h->n == 0) return fail(h, NS_ERR_STATE, "empty network");
+  if (h->n_nets && h->drive.kind == NS_DRIVE_REF_UNIFORM)
+    return fail(h, NS_ERR_UNSUPPORTED, "the reference-uniform drive's kicks are global to one network; batches take per-neuron drives");
   return NS_OK;
 }
 
@@ -771,6 +845,7 @@ ns_status ns_destroy(ns_handle* h) {
   free_bag(h->neuron_allocs);
   free_bag(h->csr_allocs);
   free_bag(h->log_allocs);
+  free_bag(h->batch_allocs);
   if (h->ctl) cudaFree(h->ctl);
   if (h->st2) cudaStreamSynchronize(h->st2);
   if (h->ev_rows) cudaEventDestroy(h->ev_rows);
@@ -807,9 +882,18 @@ ns_status ns_upload_neurons(ns_handle* h, const ns_neuron_soa* s) {
   if ((int)s->params_per_neuron != ppn)
     return fail(h, NS_ERR_INVALID_ARG, "params_per_neuron does not match the model");
   if (s->n == 0 || s->n > 0xFFFFFFF0ull) return fail(h, NS_ERR_INVALID_ARG, "n out of range");
-  if (h->have_csr && s->n != h->n) return fail(h, NS_ERR_INVALID_ARG, "n differs from the CSR");
+  if (h->have_csr && s->n != h->n && !h->batch_uploading)
+    return fail(h, NS_ERR_INVALID_ARG, "n differs from the CSR");
   CK(cudaSetDevice(h->dev));
   CK(cudaStreamSynchronize(h->st));
+  if (h->n_nets && !h->batch_uploading) {
+    // a plain upload ends batch mode
+    drop_graphs(h);
+    free_bag(h->batch_allocs);
+    h->n_nets = 0;
+    h->d.net_of = nullptr; h->d.net_seed = nullptr; h->d.net_base = nullptr;
+  }
+  if (h->batch_uploading && s->n != h->n) h->have_csr = false;
   CK(cudaStreamSynchronize(h->st2));
   // a network of the same size reuses the device buffers, so pointers and
   // therefore the captured step graphs stay valid
@@ -959,6 +1043,8 @@ static ns_status alloc_dynamic(ns_handle* h) {
   d.trace_pos = nullptr; d.trace_off = nullptr; d.trace_cap = 0;
   // windowed stepping buffers
   h->win = window_len(c);
+  h->wcur = h->win;
+  h->next_tune_step = 0;
   d.inbits = nullptr; d.seg_cnt = nullptr; d.seg_lst = nullptr; d.seg_off = nullptr;
   d.step_total = nullptr; d.nseg = 0; d.wmax = 0;
   if (h->win) {
@@ -1122,6 +1208,131 @@ ns_status ns_upload_csr(ns_handle* h, uint64_t n, uint64_t m, const uint64_t* ro
   }
   h->have_csr = true;
   if (h->have_neurons) return alloc_dynamic(h);
+  return NS_OK;
+}
+
+ns_status ns_upload_batch(ns_handle* h, uint32_t n_nets, const ns_net_desc* nets,
+                          uint64_t* first_neuron_out) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  if (n_nets == 0 || !nets) return fail(h, NS_ERR_INVALID_ARG, "empty batch");
+  const int ppn = params_for(h->cfg.model);
+  const uint32_t model = h->cfg.model;
+  std::vector<uint64_t> base(n_nets + 1, 0), ebase(n_nets + 1, 0);
+  uint32_t with_ty = 0, with_pl = 0;
+  for (uint32_t q = 0; q < n_nets; ++q) {
+    const ns_net_desc& x = nets[q];
+    const std::string tag = "network " + std::to_string(q) + ": ";
+    if (!x.neurons || !x.neurons->params || x.neurons->n == 0)
+      return fail(h, NS_ERR_INVALID_ARG, tag + "no neurons or params");
+    if ((int)x.neurons->params_per_neuron != ppn)
+      return fail(h, NS_ERR_INVALID_ARG, tag + "params_per_neuron does not match the model");
+    const uint64_t n = x.neurons->n;
+    if (!x.row_ptr || (x.m && (!x.col || !x.w))) return fail(h, NS_ERR_INVALID_ARG, tag + "null CSR array");
+    if (x.row_ptr[0] != 0 || x.row_ptr[n] != x.m) return fail(h, NS_ERR_CSR, tag + "row_ptr must run from 0 to m");
+    for (uint64_t i = 0; i < n; ++i)
+      if (x.row_ptr[i + 1] < x.row_ptr[i]) return fail(h, NS_ERR_CSR, tag + "row_ptr not monotone");
+    for (uint64_t e = 0; e < x.m; ++e)
+      if (x.col[e] >= n) return fail(h, NS_ERR_CSR, tag + "col >= n");
+    with_ty += x.syn_type ? 1u : 0u;
+    with_pl += x.plastic ? 1u : 0u;
+    base[q + 1] = base[q] + n;
+    ebase[q + 1] = ebase[q] + x.m;
+    if (base[q + 1] > 0xFFFFFFF0ull) return fail(h, NS_ERR_INVALID_ARG, "batch too large (neurons)");
+  }
+  if ((with_ty && with_ty != n_nets) || (with_pl && with_pl != n_nets))
+    return fail(h, NS_ERR_INVALID_ARG, "syn_type / plastic must be given by every network or by none");
+  const uint64_t N = base[n_nets], M = ebase[n_nets];
+
+  // concatenated neuron SoA (missing fields take ns_upload_neurons' defaults)
+  std::vector<float> P(N * ppn), V(N), U(N, 0.f), I(N, 0.f), GM(N, 0.05f), GH(N, 0.6f), GN(N, 0.32f);
+  std::vector<float> PRE(N, 0.f), POST(N, 0.f);
+  std::vector<int32_t> REFR(N, 0);
+  std::vector<uint8_t> INH(N, 0), OUTP(N, 0);
+  std::vector<int64_t> LAST(N, -1);
+  for (uint32_t q = 0; q < n_nets; ++q) {
+    const ns_neuron_soa& a = *nets[q].neurons;
+    const uint64_t o = base[q], n = a.n;
+    std::memcpy(P.data() + o * ppn, a.params, n * ppn * sizeof(float));
+    for (uint64_t i = 0; i < n; ++i) {
+      const float* p = a.params + i * ppn;
+      const float rest = model == NS_MODEL_LIF ? p[0] : (model == NS_MODEL_IZHIKEVICH ? p[2] : p[5]);
+      V[o + i] = a.v ? a.v[i] : rest;
+    }
+    if (a.u) std::memcpy(U.data() + o, a.u, n * 4);
+    if (a.current) std::memcpy(I.data() + o, a.current, n * 4);
+    if (a.hh_m) std::memcpy(GM.data() + o, a.hh_m, n * 4);
+    if (a.hh_h) std::memcpy(GH.data() + o, a.hh_h, n * 4);
+    if (a.hh_n) std::memcpy(GN.data() + o, a.hh_n, n * 4);
+    if (a.pre_trace) std::memcpy(PRE.data() + o, a.pre_trace, n * 4);
+    if (a.post_trace) std::memcpy(POST.data() + o, a.post_trace, n * 4);
+    if (a.refractory) std::memcpy(REFR.data() + o, a.refractory, n * 4);
+    if (a.inhibitory) std::memcpy(INH.data() + o, a.inhibitory, n);
+    if (a.is_output) std::memcpy(OUTP.data() + o, a.is_output, n);
+    if (a.last_spike_step) std::memcpy(LAST.data() + o, a.last_spike_step, n * 8);
+  }
+  ns_neuron_soa c{};
+  c.n = N; c.params = P.data(); c.params_per_neuron = (uint32_t)ppn;
+  c.v = V.data(); c.u = U.data(); c.current = I.data();
+  c.hh_m = GM.data(); c.hh_h = GH.data(); c.hh_n = GN.data();
+  c.pre_trace = PRE.data(); c.post_trace = POST.data(); c.refractory = REFR.data();
+  c.inhibitory = INH.data(); c.is_output = OUTP.data(); c.last_spike_step = LAST.data();
+
+  // concatenated CSR (block diagonal)
+  std::vector<uint64_t> RP(N + 1);
+  std::vector<uint32_t> COL(M);
+  std::vector<float> W(M);
+  std::vector<uint8_t> TY(with_ty ? M : 0), PL(with_pl ? M : 0);
+  for (uint32_t q = 0; q < n_nets; ++q) {
+    const ns_net_desc& x = nets[q];
+    const uint64_t o = base[q], eo = ebase[q], n = x.neurons->n;
+    for (uint64_t i = 0; i < n; ++i) RP[o + i] = eo + x.row_ptr[i];
+    for (uint64_t e = 0; e < x.m; ++e) COL[eo + e] = (uint32_t)(o + x.col[e]);
+    if (x.m) std::memcpy(W.data() + eo, x.w, x.m * 4);
+    if (with_ty && x.m) std::memcpy(TY.data() + eo, x.syn_type, x.m);
+    if (with_pl && x.m) std::memcpy(PL.data() + eo, x.plastic, x.m);
+  }
+  RP[N] = M;
+
+  h->batch_uploading = true;
+  ns_status r = ns_upload_neurons(h, &c);
+  if (r == NS_OK)
+    r = ns_upload_csr(h, N, M, RP.data(), COL.data(), W.data(), with_ty ? TY.data() : nullptr,
+                      with_pl ? PL.data() : nullptr);
+  h->batch_uploading = false;
+  if (r != NS_OK) return r;
+
+  // per-neuron network ids (padding neurons belong to the last network),
+  // per-network seeds and first neurons
+  std::vector<uint32_t> net_of(h->n_pad, n_nets - 1);
+  std::vector<unsigned long long> seeds(n_nets), bases(n_nets + 1);
+  for (uint32_t q = 0; q < n_nets; ++q) {
+    std::fill(net_of.begin() + base[q], net_of.begin() + base[q + 1], q);
+    seeds[q] = nets[q].seed;
+  }
+  for (uint32_t q = 0; q <= n_nets; ++q) bases[q] = base[q];
+  NsDev& d = h->d;
+  const bool reuse = h->n_nets == n_nets && h->batch_allocs.size() == 3 &&
+                     h->alloc_bytes[(void*)d.net_of] >= h->n_pad * 4;
+  if (!reuse) {
+    drop_graphs(h);
+    free_bag(h->batch_allocs);
+    uint32_t* a = nullptr;
+    unsigned long long *b = nullptr, *e = nullptr;
+    ns_status st;
+    if ((st = dalloc(h, h->batch_allocs, &a, h->n_pad)) || (st = dalloc(h, h->batch_allocs, &b, n_nets)) ||
+        (st = dalloc(h, h->batch_allocs, &e, n_nets + 1))) {
+      free_bag(h->batch_allocs);
+      h->n_nets = 0;
+      d.net_of = nullptr; d.net_seed = nullptr; d.net_base = nullptr;
+      return st;
+    }
+    d.net_of = a; d.net_seed = b; d.net_base = e;
+  }
+  h->n_nets = n_nets;
+  CK(copy_sync(h, (void*)d.net_of, net_of.data(), h->n_pad * 4, cudaMemcpyHostToDevice));
+  CK(copy_sync(h, (void*)d.net_seed, seeds.data(), n_nets * 8ull, cudaMemcpyHostToDevice));
+  CK(copy_sync(h, (void*)d.net_base, bases.data(), (n_nets + 1) * 8ull, cudaMemcpyHostToDevice));
+  if (first_neuron_out) std::memcpy(first_neuron_out, base.data(), (n_nets + 1) * 8ull);
   return NS_OK;
 }
 
@@ -1481,6 +1692,16 @@ ns_status ns_get_schedule(ns_handle* h, uint32_t* schedule, double* us_per_step)
   if (schedule) *schedule = h->sched;
   if (us_per_step)
     for (int q = 0; q < 4; ++q) us_per_step[q] = h->tune_us[q + 1];
+  return NS_OK;
+}
+
+ns_status ns_get_window(ns_handle* h, uint32_t* window, uint32_t* candidates, double* us_per_step) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  if (window) *window = h->win ? h->wcur : 0u;
+  for (int q = 0; q < 4; ++q) {
+    if (candidates) candidates[q] = h->tune_w[q];
+    if (us_per_step) us_per_step[q] = h->tune_w_us[q];
+  }
   return NS_OK;
 }
 

@@ -100,6 +100,11 @@ struct NsDev {
   unsigned long long* trace_pos;   // traced step only
   const unsigned long long* trace_off;
   unsigned long long trace_cap;
+  // batched networks: network of each neuron, and per network its drive
+  // seed and first neuron (null for a single network)
+  const uint32_t* net_of;
+  const unsigned long long* net_seed;
+  const unsigned long long* net_base;
   // windowed stepping (delay >= 2, no plasticity): "slot has input" bits
   // [D][n_pad/32], and per-window spike segments of 256 neurons
   uint32_t* inbits;
@@ -177,6 +182,19 @@ __device__ __forceinline__ void hh_rates(float v, float& am, float& bm, float& a
   float y = (v + 55.0f) / 10.0f;
   an = (y == 0.0f) ? 0.1f : (0.1f * y) / (-expm1f(-y));
   bn = 0.125f * expf(-(v + 65.0f) / 80.0f);
+}
+
+// Drive stream key of neuron i: the handle's seed and i, or, in a batch of
+// networks, the network's own seed and i's index inside its network, so that
+// a network draws the same drive in a batch as when it runs alone.
+__device__ __forceinline__ void drive_key(const NsDev& d, uint64_t i, uint64_t& seed, uint32_t& li) {
+  seed = d.seed;
+  li = (uint32_t)i;
+  if (d.net_of != nullptr) {
+    const uint32_t q = d.net_of[i];
+    seed = d.net_seed[q];
+    li = (uint32_t)(i - d.net_base[q]);
+  }
 }
 
 __device__ __forceinline__ U4 make_drive_draw(const NsDev& d, uint64_t i0, uint64_t k) {
@@ -447,18 +465,39 @@ __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
           make_longlong2(0, 0);
     }
     // ---- drive draws: one Philox per pair ----
-    const U4 x = make_drive_draw(d, i0, k);
+    U4 y2[2];
     float z[2] = {0.f, 0.f};
-    if (d.drive_kind == 3) gauss_pair(x, z[0], z[1]);
+    if (d.net_of == nullptr) {
+      const U4 x = make_drive_draw(d, i0, k);
+      if (d.drive_kind == 3) gauss_pair(x, z[0], z[1]);
+      y2[0] = x;
+      y2[1] = (d.drive_kind == 1 || d.drive_kind == 2 || d.drive_kind == 4)
+                  ? draw(d.seed, (uint32_t)(i0 + 1), k, kStreamDrive) : x;
+    } else {
+      // batch: the pair may straddle two networks, so each neuron draws
+      // from its own network's stream (Gaussian pairs by local index)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        uint64_t sd;
+        uint32_t li;
+        drive_key(d, i0 + e, sd, li);
+        y2[e] = U4{0u, 0u, 0u, 0u};
+        if (d.drive_kind == 3) {
+          float g0, g1;
+          gauss_pair(draw(sd, li >> 1, k, kStreamDrive), g0, g1);
+          z[e] = (li & 1u) ? g1 : g0;
+        } else if (d.drive_kind != 0) {
+          y2[e] = draw(sd, li, k, kStreamDrive);
+        }
+      }
+    }
     const uint8_t inhv[2] = {ih.x, ih.y};
     bool spk[2];
 #pragma unroll
     for (int e = 0; e < 2; ++e) {
       const uint64_t i = i0 + e;
       float addI, kick, addg;
-      const U4 y = (e == 1 && (d.drive_kind == 1 || d.drive_kind == 2 || d.drive_kind == 4))
-                       ? draw(d.seed, (uint32_t)i, k, kStreamDrive) : x;
-      drive_of(d, y, z[e], inhv[e], addI, kick, addg);
+      drive_of(d, y2[e], z[e], inhv[e], addI, kick, addg);
       float Se[NT], Ge[4];
 #pragma unroll
       for (int t = 0; t < NT; ++t) Se[t] = S[t][e];

@@ -51,6 +51,9 @@ __global__ void __launch_bounds__(kWinThreads) k_window(NsDev d, uint32_t j0, ui
     for (int t = 0; t < 4; ++t) G[t] = d.G[t][i];
   }
   const uint8_t inh = d.drive_kind == 3 ? d.inh[i] : 0;
+  uint64_t dseed;
+  uint32_t dli;
+  drive_key(d, i, dseed, dli);
   const uint64_t words = d.n_pad >> 5;
   unsigned long long my_spk = 0;
   for (uint32_t s = 0; s < W; ++s) {
@@ -99,10 +102,10 @@ __global__ void __launch_bounds__(kWinThreads) k_window(NsDev d, uint32_t j0, ui
     U4 y{0u, 0u, 0u, 0u};
     if (d.drive_kind == 3) {
       float z0, z1;
-      gauss_pair(draw(d.seed, (uint32_t)(i >> 1), k, kStreamDrive), z0, z1);
-      z = (i & 1) ? z1 : z0;
+      gauss_pair(draw(dseed, dli >> 1, k, kStreamDrive), z0, z1);
+      z = (dli & 1u) ? z1 : z0;
     } else if (d.drive_kind != 0) {
-      y = draw(d.seed, (uint32_t)i, k, kStreamDrive);
+      y = draw(dseed, dli, k, kStreamDrive);
     }
     float addI, kick, addg;
     drive_of(d, y, z, inh, addI, kick, addg);

@@ -326,6 +326,15 @@ class SimulationEngine:
         self._check(self.lib.ns_get_schedule(self._h, C.byref(sc), us))
         return int(sc.value), {q + 1: us[q] for q in range(4)}
 
+    def window(self):
+        """(window length in use, {candidate W: us per step} timed by the
+        window tuner)."""
+        w = C.c_uint32()
+        cand = np.zeros(4, np.uint32)
+        us = np.zeros(4, np.float64)
+        self._check(self.lib.ns_get_window(self._h, C.byref(w), _ptr(cand), _ptr(us)))
+        return int(w.value), {int(c): float(t) for c, t in zip(cand, us) if c}
+
     def launch_count(self):
         c = C.c_uint64()
         self._check(self.lib.ns_launch_count(self._h, C.byref(c)))

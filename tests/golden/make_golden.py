@@ -1,0 +1,73 @@
+"""Writes the golden fixtures under tests/golden/.
+
+Each fixture is a small seeded network of one configuration family, run on
+the oracle (FP32-mirroring engine for LIF and Izhikevich, FP64 engine for
+Hodgkin-Huxley), saved with a digest of the network it ran on so that a
+change of the generator shows up as a fixture mismatch instead of a silent
+re-pin. The reference crate cannot be built in this image (no Rust
+toolchain), so these vectors are generated by the restatement and pinned by
+the known-answer tests in test_oracle_known_answers.py.
+
+Usage: python tests/golden/make_golden.py
+"""
+import hashlib
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.dirname(HERE))
+
+from neuralsim_b200 import _abi as A  # noqa: E402
+import nets  # noqa: E402
+
+
+def net_digest(net):
+    h = hashlib.sha256()
+    for a in (net.row_ptr, net.col, net.w, net.params, net.syn_type, net.plastic):
+        if a is not None:
+            h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()
+
+
+# name -> (builder, steps, oracle precision)
+CASES = {
+    "lif_delta_n600": (lambda: nets.lif_delta(n=600, k=40, seed=143), 1500, 32),
+    "izh_stdp_bf16_n800": (lambda: nets.izh_stdp(n=800, k=40, seed=144), 300, 32),
+    "izh_stdp_f32_n800": (lambda: nets.izh_stdp(n=800, k=40, seed=145, wf=A.WEIGHT_F32), 300, 32),
+    "lif_reference_default_n200": (lambda: nets.lif_reference_default(n=200, seed=142), 300, 32),
+    "hh_rush_larsen_n400": (lambda: nets.hh_cond(n=400, k=40, seed=146), 2000, 64),
+}
+
+
+def run_case(name):
+    from oracle.oracle import FastOracle
+    build, steps, prec = CASES[name]
+    net, cfg, drive = build()
+    o = FastOracle(net, cfg, drive, precision=prec)
+    o.step(steps)
+    idx, off = o.raster()
+    st = o.state()
+    out = {"idx": np.asarray(idx, np.uint32), "off": np.asarray(off, np.uint64),
+           "v": np.asarray(st["v"], np.float64), "weights": np.asarray(o.weights(), np.float64 if prec == 64 else np.float32),
+           "steps": np.int64(steps), "precision": np.int64(prec),
+           "net_sha256": np.array(net_digest(net))}
+    for k in ("u", "m", "h", "n", "pre", "post", "refr"):
+        if k in st and st[k] is not None:
+            out[k] = np.asarray(st[k])
+    o.close()
+    return out
+
+
+def main():
+    for name in CASES:
+        out = run_case(name)
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+        print(name, "spikes", len(out["idx"]))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,99 @@
+"""Multi-rank host logic on CPU (gloo, world size 2): sharding of network
+batches across ranks and the final gather; raster splitting of a batch.
+The device work per rank is stood in for by the oracle (test side only)."""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+from neuralsim_b200 import shard
+from neuralsim_b200.batch import split_raster_by_network
+
+
+def test_assign_covers_and_balances():
+    rng = np.random.default_rng(0)
+    costs = np.exp(rng.uniform(np.log(2e3), np.log(5e4), 256)) * rng.integers(50, 201, 256)
+    for world in (1, 2, 3, 8):
+        r = shard.assign(costs, world)
+        assert r.min() >= 0 and r.max() < world
+        load = np.bincount(r, weights=costs, minlength=world)
+        assert np.isclose(load.sum(), costs.sum())
+        # LPT bound: no rank exceeds the mean by more than the largest item
+        assert load.max() <= costs.sum() / world + costs.max() + 1e-6
+        assert np.array_equal(r, shard.assign(costs, world))  # deterministic
+
+
+def test_split_raster_by_network():
+    first = np.array([0, 3, 7, 10])
+    # two steps: step 0 spikes 1, 4, 9; step 1 spikes 0, 6
+    idx = np.array([1, 4, 9, 0, 6], np.uint32)
+    off = np.array([0, 3, 5], np.uint64)
+    parts = split_raster_by_network(idx, off, first)
+    assert [list(p[0]) for p in parts] == [[1, 0], [1, 3], [2]]
+    assert [list(p[1]) for p in parts] == [[0, 1, 2], [0, 1, 2], [0, 1, 1]]
+
+
+def _small_nets():
+    from neuralsim_b200 import configs
+    nets, seeds, cfg, drive, _ = configs.lif_batch_c3(n_nets=5, size_range=(200, 500),
+                                                      k_range=(10, 30))
+    from neuralsim_b200 import _abi as A
+    from neuralsim_b200.engine import Drive
+    drive = Drive(A.DRIVE_POISSON_KICK, p=0.02, amplitude=4.0)
+    cfg.spike_log_capacity, cfg.spike_log_steps = 1_000_000, 1000
+    return nets, seeds, cfg, drive
+
+
+def _oracle_eval(nets, seeds, cfg, drive, steps=200):
+    import copy
+    from oracle.oracle import FastOracle
+    out = []
+    for net, sd in zip(nets, seeds):
+        c = copy.copy(cfg)
+        c.seed = sd
+        o = FastOracle(net, c, drive, precision=32)
+        o.step(steps)
+        out.append(int(len(o.raster()[0])))
+        o.close()
+    return out
+
+
+def _worker(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import datetime
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        nets, seeds, cfg, drive = _small_nets()
+        res = shard.run_sharded(nets, seeds, lambda n, s: _oracle_eval(n, s, cfg, drive),
+                                rank, world)
+        q.put((rank, res))
+    finally:
+        dist.destroy_process_group()
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def test_run_sharded_gloo_world2(lib, oracle_lib):
+    nets, seeds, cfg, drive = _small_nets()
+    want = _oracle_eval(nets, seeds, cfg, drive)
+    assert sum(want) > 0
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = dict(q.get(timeout=240) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert got[0] == want and got[1] == want
