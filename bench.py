@@ -67,14 +67,18 @@ def peaks():
     return 6650.0, "fallback 6.65 TB/s (no MEASURED_PEAKS.json)"
 
 
-def profile_traffic(kernel):
-    """DRAM bytes (read + write) per launch of `kernel` from the committed ncu
-    summary of the full-size workload, or None."""
+PROFILE_UNIT_STEPS = 20
+
+
+def profile_traffic_ratio(kernel):
+    """DRAM bytes (read + write) per algorithmic byte of `kernel`, measured by
+    the committed ncu capture of the full-size workload (the launches of the
+    steps whose units bench.py records), or None."""
     path = os.path.join(ROOT, "profiles", "izh_c2_step_kernels_ncu.md")
     if not os.path.exists(path):
         return None
     for line in open(path):
-        if line.startswith(f"traffic_bytes_per_launch_{kernel}:"):
+        if line.startswith(f"traffic_ratio_{kernel}:"):
             try:
                 return float(line.split(":", 1)[1].strip().split()[0])
             except ValueError:
@@ -218,8 +222,21 @@ def run_ours(a):
     clocks = clk.summary()
 
     # per-kernel device time (eager serial steps with events around each kernel)
+    # The first PROFILE_UNIT_STEPS are profiled one step at a time with each
+    # step's spikes and events recorded: the ncu traffic capture of the same
+    # command reads these launches, so its DRAM bytes can be set against the
+    # algorithmic bytes of exactly those steps.
     pc0 = eng.counters()
-    prof = eng.profile_steps(200)
+    prof, units = {}, []
+    for q in range(PROFILE_UNIT_STEPS + 1):
+        ca = eng.counters()
+        part = eng.profile_steps(1 if q < PROFILE_UNIT_STEPS else 200 - PROFILE_UNIT_STEPS)
+        cb = eng.counters()
+        if q < PROFILE_UNIT_STEPS:
+            units.append([int(cb[1] - ca[1]), int(cb[3] - ca[3])])
+        for name, (kms, kl) in part.items():
+            t = prof.get(name, (0.0, 0))
+            prof[name] = (t[0] + kms, t[1] + kl)
     pc1 = eng.counters()
     prof_steps = 200.0
     prof_spikes = (pc1[1] - pc0[1]) / prof_steps
@@ -272,7 +289,8 @@ def run_ours(a):
         nk_bytes = kb[dom]
         nk_avg_s = kernels[dom]["avg_launch_us"] / 1e6
         achieved = nk_bytes / nk_avg_s / 1e9
-        traffic = profile_traffic(dom)
+        ratio = profile_traffic_ratio(dom)
+        traffic = ratio * nk_bytes if ratio is not None else None
         value = events_all / (ms_max / 1e3)
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -298,6 +316,10 @@ def run_ours(a):
                 "frac": achieved / peak, "traffic": traffic,
                 "kernel": dom, "bytes_per_launch": nk_bytes, "avg_launch_us": nk_avg_s * 1e6,
                 "peak_source": peak_src, "spikes_per_step_profiled": prof_spikes,
+                "traffic_ratio": ratio,
+                "traffic_gbs": traffic / nk_avg_s / 1e9 if traffic is not None else None,
+                "traffic_source": "profiles/izh_c2_step_kernels_ncu.md (DRAM / algorithmic bytes, full-size capture)",
+                "profile_first_steps_spikes_events": units,
                 "kernels": kernels,
             },
             "step_roofline": {

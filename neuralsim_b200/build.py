@@ -10,7 +10,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libneuralsim.so")
 
-SOURCES = ["ns_core.cu", "ns_gen.cu", "ns_noalloc.cu"]
+SOURCES = ["ns_core.cu", "ns_gen.cu", "ns_noalloc.cu", "ns_surrogate.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",

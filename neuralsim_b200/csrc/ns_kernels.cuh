@@ -16,6 +16,7 @@
 #pragma once
 #include <cstdint>
 #include "ns_device.cuh"
+#include "ns_hh.cuh"
 
 namespace ns {
 
@@ -172,18 +173,6 @@ struct NState {
   int refr;
 };
 
-__device__ __forceinline__ void hh_rates(float v, float& am, float& bm, float& ah, float& bh,
-                                         float& an, float& bn) {
-  float x = (v + 40.0f) / 10.0f;
-  am = (x == 0.0f) ? 1.0f : x / (-expm1f(-x));
-  bm = 4.0f * expf(-(v + 65.0f) / 18.0f);
-  ah = 0.07f * expf(-(v + 65.0f) / 20.0f);
-  bh = 1.0f / (1.0f + expf(-(v + 35.0f) / 10.0f));
-  float y = (v + 55.0f) / 10.0f;
-  an = (y == 0.0f) ? 0.1f : (0.1f * y) / (-expm1f(-y));
-  bn = 0.125f * expf(-(v + 65.0f) / 80.0f);
-}
-
 // Drive stream key of neuron i: the handle's seed and i, or, in a batch of
 // networks, the network's own seed and i's index inside its network, so that
 // a network draws the same drive in a batch as when it runs alone.
@@ -242,10 +231,10 @@ __device__ __forceinline__ bool model_step(const NsDev& d, NState& s, const floa
   } else {
     float gna = p[0], gk = p[1], gl = p[2], ena = p[3], ek = p[4], el = p[5], cm = p[6];
     float v = s.v, m = s.m, h = s.h, n = s.n;
-    float am, bm, ah, bh, an, bn;
-    hh_rates(v, am, bm, ah, bh, an, bn);
     bool spk;
     if (d.hh_int == 0) {
+      float am, bm, ah, bh, an, bn;
+      hh_rates(v, am, bm, ah, bh, an, bn);
       m = m + (am * (1.0f - m) - bm * m) * dt;
       h = h + (ah * (1.0f - h) - bh * h) * dt;
       n = n + (an * (1.0f - n) - bn * n) * dt;
@@ -258,16 +247,7 @@ __device__ __forceinline__ bool model_step(const NsDev& d, NState& s, const floa
       spk = v >= -55.0f;
       if (spk) v = -70.0f;
     } else {
-      float sm = am + bm, sh = ah + bh, sn = an + bn;
-      float minf = am / sm, hinf = ah / sh, ninf = an / sn;
-      m = minf + (m - minf) * expf(-dt * sm);
-      h = hinf + (h - hinf) * expf(-dt * sh);
-      n = ninf + (n - ninf) * expf(-dt * sn);
-      float n2 = n * n;
-      float iion = gna * (m * m * m) * h * (v - ena) + gk * (n2 * n2) * (v - ek) + gl * (v - el);
-      float vn = v + dt * (Iin - iion) / cm;
-      spk = (v < 0.0f) && (vn >= 0.0f);
-      v = vn;
+      spk = hh_rl_step(v, m, h, n, Iin, p, dt);
     }
     if (delta) v = v + kick;
     s.v = v; s.m = m; s.h = h; s.n = n;
