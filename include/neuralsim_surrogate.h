@@ -101,6 +101,12 @@ ns_status ns_tc_gemm_bf16(const uint16_t* A, const uint16_t* B, float* C, uint16
 ns_status ns_set_surrogate(ns_handle* h, const ns_sur* s, float v_lo, float v_hi,
                            float residual_mv);
 
+/* What advances in-envelope neurons over a macro-step: 0 = the MLP (after
+ * ns_set_surrogate), 1 = one Rush-Larsen step of the macro-step's length
+ * (0.1 ms) with the same held current, envelope, residual check and fallback
+ * — the plain method in the surrogate's cost class, for comparison. */
+ns_status ns_set_macro_step_mode(ns_handle* h, int32_t mode);
+
 /* Neuron macro-steps taken by the surrogate and by the Rush-Larsen fallback
  * since the surrogate was attached. */
 ns_status ns_surrogate_counts(ns_handle* h, uint64_t* by_mlp, uint64_t* by_fallback);

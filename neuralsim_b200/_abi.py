@@ -92,6 +92,22 @@ SIGNATURES = {
     "ns_set_drive": (C.c_int32, [_P, C.POINTER(NsDrive)]),
     "ns_upload_batch": (C.c_int32, [_P, C.c_uint32, C.POINTER(NsNetDesc), _P]),
     "ns_get_window": (C.c_int32, [_P, _P, _P, _P]),
+    # neuralsim_surrogate.h
+    "ns_sur_create": (C.c_int32, [C.c_int32, _P, C.c_float, C.c_uint32, C.c_uint64, C.POINTER(_P)]),
+    "ns_sur_destroy": (C.c_int32, [_P]),
+    "ns_sur_last_error": (C.c_char_p, [_P]),
+    "ns_sur_set_data": (C.c_int32, [_P, _P, C.c_uint64, _P]),
+    "ns_sur_set_norm": (C.c_int32, [_P, _P, _P, _P, _P]),
+    "ns_sur_train": (C.c_int32, [_P, C.c_uint32, C.c_float, C.c_float, _P]),
+    "ns_sur_gradient": (C.c_int32, [_P, _P, _P, _P, _P]),
+    "ns_sur_get_params": (C.c_int32, [_P, _P]),
+    "ns_sur_set_params": (C.c_int32, [_P, _P]),
+    "ns_sur_predict": (C.c_int32, [_P, _P, C.c_uint64, _P]),
+    "ns_tc_gemm_bf16": (C.c_int32, [_P, _P, _P, _P, _P, C.c_uint32, C.c_uint32, C.c_uint32,
+                                    C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int32, _P]),
+    "ns_set_surrogate": (C.c_int32, [_P, _P, C.c_float, C.c_float, C.c_float]),
+    "ns_set_macro_step_mode": (C.c_int32, [_P, C.c_int32]),
+    "ns_surrogate_counts": (C.c_int32, [_P, _U64P, _U64P]),
     "ns_step": (C.c_int32, [_P, C.c_uint32, C.POINTER(NsStepStats)]),
     "ns_read_spikes": (C.c_int32, [_P, C.c_uint64, C.c_uint32, _P, _P, C.c_uint64, _U64P]),
     "ns_clear_spike_log": (C.c_int32, [_P]),

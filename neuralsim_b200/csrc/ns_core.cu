@@ -15,6 +15,8 @@
 #include "../../include/neuralsim.h"
 #include "ns_kernels.cuh"
 #include "ns_window.cuh"
+#include "ns_window_sur.cuh"
+#include "ns_sur_internal.h"
 
 using ns::NsDev;
 
@@ -54,6 +56,10 @@ struct ns_handle {
   std::vector<void*> batch_allocs;
   uint32_t n_nets = 0;              // 0 = single network
   bool batch_uploading = false;     // ns_upload_batch is calling the uploads
+  // learned HH macro-step (ns_set_surrogate)
+  bool sur_on = false;
+  ns::SurDev sd{};
+  std::vector<void*> sur_allocs;
 };
 
 namespace {
@@ -512,7 +518,10 @@ uint32_t window_len(const ns_config& c) {
 // Enqueues a window of Wc steps starting at graph-node offset j0.
 cudaError_t enqueue_window(ns_handle* h, uint32_t j0, uint32_t Wc) {
   const uint32_t nseg = h->d.nseg;
-  pick_window(h->cfg.model, h->cfg.input_mode)<<<nseg, ns::kWinThreads, 0, h->st>>>(h->d, j0, Wc);
+  if (h->sur_on)
+    ns::k_window_sur<<<nseg, ns::kWinThreads, ns::kSurSmem, h->st>>>(h->d, h->sd, j0, Wc);
+  else
+    pick_window(h->cfg.model, h->cfg.input_mode)<<<nseg, ns::kWinThreads, 0, h->st>>>(h->d, j0, Wc);
   pick_window_rows(h->cfg.input_mode, h->cfg.weight_format)
       <<<h->win_rows_blocks, 256, 0, h->st>>>(h->d, j0, Wc);
   ns::k_window_scan<<<Wc, 256, 0, h->st>>>(h->d, Wc);
@@ -649,8 +658,18 @@ ns_status autotune(ns_handle* h, uint32_t budget, uint32_t* used) {
 // steps from one snapshot, the fastest is kept. Longer windows mean fewer
 // launches and state held in registers longer; shorter ones keep more
 // neurons' segments busy per row-walk launch. Runs once, at step 0.
+// window length with the surrogate attached: whole macro-steps
+uint32_t sur_window(const ns_handle* h) {
+  return h->win >= (uint32_t)ns::kSub ? h->win / ns::kSub * ns::kSub : h->win;
+}
+
 ns_status autotune_window(ns_handle* h, uint32_t budget, uint32_t* used) {
   *used = 0;
+  if (h->sur_on) {
+    h->wcur = sur_window(h);
+    h->next_tune_step = ~0ull;
+    return NS_OK;
+  }
   if (h->next_tune_step != 0) return NS_OK;
   uint32_t cand[4] = {0, 0, 0, 0};
   int nc = 0;
@@ -703,6 +722,8 @@ ns_status autotune_window(ns_handle* h, uint32_t budget, uint32_t* used) {
 ns_status ready(ns_handle* h) {
   if (!h->have_neurons || !h->have_csr) return fail(h, NS_ERR_STATE, "upload neurons and CSR first");
   if (h->n == 0) return fail(h, NS_ERR_STATE, "empty network");
+  if (h->sur_on && h->drive.kind != NS_DRIVE_NONE && h->drive.kind != NS_DRIVE_POISSON_CONDUCTANCE)
+    return fail(h, NS_ERR_UNSUPPORTED, "the surrogate macro-step takes no drive or the Poisson conductance drive");
   if (h->n_nets && h->drive.kind == NS_DRIVE_REF_UNIFORM)
     return fail(h, NS_ERR_UNSUPPORTED, "the reference-uniform drive's kicks are global to one network; batches take per-neuron drives");
   return NS_OK;
@@ -846,6 +867,7 @@ ns_status ns_destroy(ns_handle* h) {
   free_bag(h->csr_allocs);
   free_bag(h->log_allocs);
   free_bag(h->batch_allocs);
+  free_bag(h->sur_allocs);
   if (h->ctl) cudaFree(h->ctl);
   if (h->st2) cudaStreamSynchronize(h->st2);
   if (h->ev_rows) cudaEventDestroy(h->ev_rows);
@@ -1692,6 +1714,107 @@ ns_status ns_get_schedule(ns_handle* h, uint32_t* schedule, double* us_per_step)
   if (schedule) *schedule = h->sched;
   if (us_per_step)
     for (int q = 0; q < 4; ++q) us_per_step[q] = h->tune_us[q + 1];
+  return NS_OK;
+}
+
+ns_status ns_set_surrogate(ns_handle* h, const ns_sur* s, float v_lo, float v_hi, float residual_mv) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  CK(cudaSetDevice(h->dev));
+  CK(cudaStreamSynchronize(h->st));
+  if (!s) {
+    if (h->sur_on) drop_graphs(h);
+    h->sur_on = false;
+    h->wcur = h->win;
+    return NS_OK;
+  }
+  const ns_config& c = h->cfg;
+  if (c.model != NS_MODEL_HH || c.hh_integrator != NS_HH_RUSH_LARSEN ||
+      c.input_mode != NS_INPUT_CONDUCTANCE_FRESH)
+    return fail(h, NS_ERR_UNSUPPORTED, "the surrogate needs Hodgkin-Huxley, Rush-Larsen, CONDUCTANCE_FRESH");
+  if (!h->have_neurons || !h->have_csr) return fail(h, NS_ERR_STATE, "upload neurons and CSR first");
+  if (h->win < (uint32_t)ns::kSub)
+    return fail(h, NS_ERR_UNSUPPORTED, "the surrogate needs windowed stepping with a window of at least 10 steps");
+  ns_sur_view v{};
+  ns_status r = ns_sur_view_of(s, &v);
+  if (r) return fail(h, r, "bad surrogate handle");
+  if (v.dev != h->dev) return fail(h, NS_ERR_INVALID_ARG, "surrogate and network live on different devices");
+  if (std::fabs((double)v.dt - c.dt_ms) > 1e-6 * c.dt_ms)
+    return fail(h, NS_ERR_INVALID_ARG, "the surrogate's fine step differs from dt");
+  if (!is_fin(v_lo) || !is_fin(v_hi) || !(v_lo < v_hi) || !(residual_mv > 0.0f) || !is_fin(residual_mv))
+    return fail(h, NS_ERR_INVALID_ARG, "need v_lo < v_hi and residual_mv > 0");
+  ns::SurDev& sd = h->sd;
+  if (h->sur_allocs.empty()) {
+    uint16_t *w1 = nullptr, *w2 = nullptr, *w3 = nullptr;
+    float* P = nullptr;
+    unsigned long long* cnt = nullptr;
+    uint32_t* err = nullptr;
+    ns_status st;
+    if ((st = dalloc(h, h->sur_allocs, &w1, 128 * 16)) || (st = dalloc(h, h->sur_allocs, &w2, 128 * 128)) ||
+        (st = dalloc(h, h->sur_allocs, &w3, 16 * 128)) || (st = dalloc(h, h->sur_allocs, &P, NS_SUR_PARAMS)) ||
+        (st = dalloc(h, h->sur_allocs, &cnt, 2)) || (st = dalloc(h, h->sur_allocs, &err, 1))) {
+      free_bag(h->sur_allocs);
+      return st;
+    }
+    sd.W1p = w1; sd.W2b = w2; sd.W3p = w3; sd.P = P; sd.counts = cnt; sd.err = err;
+  }
+  // the handle keeps its own copy of the weights: the surrogate may go away
+  CK(cudaMemcpyAsync((void*)sd.W1p, v.W1p, 128 * 16 * 2, cudaMemcpyDeviceToDevice, h->st));
+  CK(cudaMemcpyAsync((void*)sd.W2b, v.W2b, 128 * 128 * 2, cudaMemcpyDeviceToDevice, h->st));
+  CK(cudaMemcpyAsync((void*)sd.W3p, v.W3p, 16 * 128 * 2, cudaMemcpyDeviceToDevice, h->st));
+  CK(cudaMemcpyAsync((void*)sd.P, v.P, NS_SUR_PARAMS * 4, cudaMemcpyDeviceToDevice, h->st));
+  CK(cudaMemsetAsync(sd.counts, 0, 16, h->st));
+  CK(cudaMemsetAsync(sd.err, 0, 4, h->st));
+  std::memcpy(sd.in_mean, v.in_mean, 20);
+  std::memcpy(sd.in_scale, v.in_scale, 20);
+  std::memcpy(sd.out_mean, v.out_mean, 16);
+  std::memcpy(sd.out_scale, v.out_scale, 16);
+  sd.v_lo = v_lo;
+  sd.v_hi = v_hi;
+  sd.tol = residual_mv;
+  sd.dt_macro = (float)(c.dt_ms * ns::kSub);
+  sd.coarse = 0;
+  // the per-type conductance decay of one fine step, as the step kernels use it
+  const double taus[4] = {2.0, 10.0, 150.0, 100.0};
+  for (int t = 0; t < 4; ++t) {
+    const double dd = (double)(float)std::exp(-c.dt_ms / taus[t]);
+    double sum = 0.0, pw = 1.0;
+    for (int q = 0; q < ns::kSub; ++q) { sum += pw; pw *= dd; }
+    sd.gbar[t] = (float)(sum / ns::kSub);
+    sd.gdec9[t] = (float)std::pow(dd, ns::kSub - 1);
+  }
+  CK(cudaFuncSetAttribute(ns::k_window_sur, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ns::kSurSmem));
+  CK(cudaStreamSynchronize(h->st));
+  drop_graphs(h);
+  h->sur_on = true;
+  h->wcur = sur_window(h);
+  h->next_tune_step = ~0ull;
+  return NS_OK;
+}
+
+ns_status ns_set_macro_step_mode(ns_handle* h, int32_t mode) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  if (!h->sur_on) return fail(h, NS_ERR_STATE, "attach a surrogate first");
+  if (mode != 0 && mode != 1) return fail(h, NS_ERR_INVALID_ARG, "mode 0 (MLP) or 1 (coarse Rush-Larsen)");
+  CK(cudaSetDevice(h->dev));
+  CK(cudaStreamSynchronize(h->st));
+  h->sd.coarse = mode;
+  drop_graphs(h);
+  return NS_OK;
+}
+
+ns_status ns_surrogate_counts(ns_handle* h, uint64_t* by_mlp, uint64_t* by_fallback) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  unsigned long long c[2] = {0, 0};
+  uint32_t err = 0;
+  if (h->sur_on) {
+    CK(cudaSetDevice(h->dev));
+    CK(cudaMemcpyAsync(c, h->sd.counts, 16, cudaMemcpyDeviceToHost, h->st));
+    CK(cudaMemcpyAsync(&err, h->sd.err, 4, cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+  }
+  if (by_mlp) *by_mlp = c[0];
+  if (by_fallback) *by_fallback = c[1];
+  if (err) return fail(h, NS_ERR_DEVICE_TIMEOUT, "a tensor-core wait of the surrogate macro-step gave up");
   return NS_OK;
 }
 

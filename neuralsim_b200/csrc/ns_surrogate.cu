@@ -29,6 +29,7 @@
 #include "../../include/neuralsim_surrogate.h"
 #include "ns_gemm.cuh"
 #include "ns_hh.cuh"
+#include "ns_sur_internal.h"
 
 namespace {
 
@@ -660,3 +661,19 @@ ns_status ns_tc_gemm_bf16(const uint16_t* A, const uint16_t* B, float* C, uint16
 }
 
 }  // extern "C"
+
+ns_status ns_sur_view_of(const ns_sur* s, ns_sur_view* out) {
+  if (!s || !out) return NS_ERR_NULL_HANDLE;
+  out->dev = s->dev;
+  out->dt = s->dt;
+  std::memcpy(out->hh, s->hh.p, sizeof(out->hh));
+  out->W1p = s->W1p;
+  out->W2b = s->W2b;
+  out->W3p = s->W3p;
+  out->P = s->P;
+  std::memcpy(out->in_mean, s->norm.in_mean, 20);
+  std::memcpy(out->in_scale, s->norm.in_scale, 20);
+  std::memcpy(out->out_mean, s->norm.out_mean, 16);
+  std::memcpy(out->out_scale, s->norm.out_scale, 16);
+  return NS_OK;
+}

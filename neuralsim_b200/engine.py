@@ -335,6 +335,23 @@ class SimulationEngine:
         self._check(self.lib.ns_get_window(self._h, C.byref(w), _ptr(cand), _ptr(us)))
         return int(w.value), {int(c): float(t) for c, t in zip(cand, us) if c}
 
+    # -- learned HH macro-step (include/neuralsim_surrogate.h) --
+    def attach_surrogate(self, sur, v_lo=-85.0, v_hi=-52.0, residual_mv=0.5):
+        """Advance in-envelope neurons with the trained surrogate `sur`
+        (None detaches); the handle keeps its own copy of the weights."""
+        self._check(self.lib.ns_set_surrogate(self._h, sur.handle if sur is not None else None,
+                                              float(v_lo), float(v_hi), float(residual_mv)))
+
+    def macro_step_mode(self, mode):
+        """0: the MLP; 1: one Rush-Larsen step of 0.1 ms (comparison)."""
+        self._check(self.lib.ns_set_macro_step_mode(self._h, int(mode)))
+
+    def surrogate_counts(self):
+        """(neuron macro-steps by the MLP, by the Rush-Larsen fallback)."""
+        a, b = C.c_uint64(), C.c_uint64()
+        self._check(self.lib.ns_surrogate_counts(self._h, C.byref(a), C.byref(b)))
+        return int(a.value), int(b.value)
+
     def launch_count(self):
         c = C.c_uint64()
         self._check(self.lib.ns_launch_count(self._h, C.byref(c)))

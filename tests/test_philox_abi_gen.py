@@ -58,8 +58,9 @@ def test_gauss_drive_statistics(oracle_lib):
 
 def declared_symbols():
     names = []
-    for h in ("neuralsim.h", "neuralsim_gen.h"):
-        txt = open(os.path.join(ROOT, "include", h)).read()
+    import glob
+    for h in sorted(glob.glob(os.path.join(ROOT, "include", "*.h"))):
+        txt = open(h).read()
         txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
         names += re.findall(r"\b(ns_[a-z0-9_]+)\s*\(", txt)
     return sorted(set(names))
