@@ -54,6 +54,7 @@ def args_():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-extra", action="store_true", help="skip the LIF and HH configuration lines")
+    p.add_argument("--no-surrogate", action="store_true", help="skip the learned HH macro-step line")
     p.add_argument("--schedule", type=int, default=0, choices=[0, 1, 2, 3, 4],
                    help="step schedule: 0 autotune, 1 fused, 2 split, 3 fused 4 blocks/SM, 4 split narrow LTD")
     return p.parse_args()
@@ -267,6 +268,8 @@ def run_ours(a):
         if rank == 0:
             extra = run_extra_configs(local)
             extra["lif_batch_c3"] = batch
+            if not a.no_surrogate:
+                extra["hh_surrogate_c5"] = run_surrogate_config(local)
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
@@ -333,6 +336,12 @@ def run_ours(a):
             "e2e": e2e,
             "cpu_baseline": cpu,
             "other_configs": extra,
+            "surrogate": (None if not extra or "hh_surrogate_c5" not in extra else {
+                "speedup_vs_plain": extra["hh_surrogate_c5"]["speedup_vs_plain_windowed"],
+                "spike_time_err_ms": extra["hh_surrogate_c5"]["surrogate"]["spike_time_err_ms"],
+                "coarse_rl_spike_time_err_ms":
+                    extra["hh_surrogate_c5"]["coarse_rl_0.1ms"]["spike_time_err_ms"],
+                "fallback_fraction": extra["hh_surrogate_c5"]["surrogate"]["fallback_fraction"]}),
         }
         print(json.dumps(out), flush=True)
     eng.close()
@@ -435,6 +444,60 @@ def run_batch_config(local, rank, world, dist):
                       "step_path_bytes_per_s": bytes_step * steps / (ms / 1e3),
                       "window_steps": wlen,
                       "window_tuner_us_per_step": wtune}
+    return res
+
+
+def run_surrogate_config(local):
+    """The learned HH macro-step on the plain Hodgkin-Huxley network (100k
+    neurons, 10M synapses, dt 0.01 ms, Rush-Larsen): 10M transitions sampled
+    from the plain run (100 snapshots of all neurons, 0.5 ms apart, after a
+    20 ms warm-up; those with V in the envelope +- 3 mV kept), targets on the
+    device, training on the device; then the plain and the surrogate paths
+    timed over 100 ms each from the same state, spike times of the
+    surrogate run (and of the same macro-step scheme with one Rush-Larsen
+    step of 0.1 ms in the MLP's place) matched to the plain run's."""
+    import torch
+    from neuralsim_b200 import SimulationEngine, configs, surrogate as S
+    net, cfg, drive, _ = configs.hh_c4()
+    cfg.device = local
+    cfg.window_steps = 100
+    cfg.spike_log_capacity, cfg.spike_log_steps = 50_000_000, 20_000
+    t0 = time.time()
+    sur, x, y, losses = S.train_for_network(net, cfg, drive, warm_steps=2000, snapshots=100,
+                                            every_steps=50, batch=8192, steps=4000)
+    train_s = time.time() - t0
+    steps = 10_000
+    res = {"neurons": net.n, "synapses": net.m, "dt_ms": cfg.dt_ms, "macro_step_ms": 0.1,
+           "mlp": "5-128-128-4 SiLU, bf16 weights, fp32 accumulation (tcgen05)",
+           "train_samples": int(len(x)), "train_steps": 4000, "train_batch": 8192,
+           "train_wall_s": round(train_s, 2), "final_loss": float(np.mean(losses[-100:])),
+           "envelope_mv": [S.V_LO, S.V_HI], "residual_mv": S.RESIDUAL_MV}
+    rasters = {}
+    for mode in ("plain", "surrogate", "coarse_rl_0.1ms"):
+        eng = SimulationEngine(net, cfg, drive)
+        if mode != "plain":
+            eng.attach_surrogate(sur)
+            if mode != "surrogate":
+                eng.macro_step_mode(1)
+        stream = torch.cuda.ExternalStream(eng.stream(), device=local)
+        ms, spikes, events = timed_run(eng, steps, stream)
+        rasters[mode] = eng.read_raster(0, steps)
+        r = {"ns_per_step": ms * 1e6 / steps, "ns_per_sim_ms": ms * 1e6 / (steps * cfg.dt_ms),
+             "spikes": int(spikes)}
+        if mode != "plain":
+            mlp, fb = eng.surrogate_counts()
+            r["macro_steps_mlp"], r["macro_steps_fallback"] = mlp, fb
+            r["fallback_fraction"] = fb / max(mlp + fb, 1)
+        eng.close()
+        res[mode] = r
+    from neuralsim_b200.raster import match_spikes
+    w = int(round(2.0 / cfg.dt_ms))
+    for mode in ("surrogate", "coarse_rl_0.1ms"):
+        d, ua, ub = match_spikes(rasters["plain"], rasters[mode], w)
+        res[mode]["spike_time_err_ms"] = float(d.mean() * cfg.dt_ms) if len(d) else None
+        res[mode]["matched"], res[mode]["unmatched_plain"], res[mode]["unmatched_other"] = len(d), ua, ub
+    res["speedup_vs_plain_windowed"] = res["plain"]["ns_per_sim_ms"] / res["surrogate"]["ns_per_sim_ms"]
+    sur.close()
     return res
 
 
