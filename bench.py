@@ -55,6 +55,11 @@ def args_():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-extra", action="store_true", help="skip the LIF and HH configuration lines")
     p.add_argument("--no-surrogate", action="store_true", help="skip the learned HH macro-step line")
+    p.add_argument("--only", choices=["c1c4", "c3", "c5"], default=None,
+                   help="run one secondary configuration alone and print its result (profiling)")
+    p.add_argument("--sur-train-steps", type=int, default=12000)
+    p.add_argument("--sur-only-1m", action="store_true",
+                   help="surrogate line: evaluate only the 1M-neuron network (profiling)")
     p.add_argument("--schedule", type=int, default=0, choices=[0, 1, 2, 3, 4],
                    help="step schedule: 0 autotune, 1 fused, 2 split, 3 fused 4 blocks/SM, 4 split narrow LTD")
     return p.parse_args()
@@ -265,11 +270,15 @@ def run_ours(a):
     extra = None
     if not a.no_extra:
         batch = run_batch_config(local, rank, world, dist)
-        if rank == 0:
+        if rank == 0 and world > 1:
+            # single-GPU configurations are reported by the one-GPU run; the
+            # other ranks would only wait for them
+            extra = {"lif_batch_c3": batch}
+        elif rank == 0:
             extra = run_extra_configs(local)
             extra["lif_batch_c3"] = batch
             if not a.no_surrogate:
-                extra["hh_surrogate_c5"] = run_surrogate_config(local)
+                extra["hh_surrogate_c5"] = run_surrogate_config(local, a.sur_train_steps)
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
@@ -341,7 +350,11 @@ def run_ours(a):
                 "spike_time_err_ms": extra["hh_surrogate_c5"]["surrogate"]["spike_time_err_ms"],
                 "coarse_rl_spike_time_err_ms":
                     extra["hh_surrogate_c5"]["coarse_rl_0.1ms"]["spike_time_err_ms"],
-                "fallback_fraction": extra["hh_surrogate_c5"]["surrogate"]["fallback_fraction"]}),
+                "fallback_fraction": extra["hh_surrogate_c5"]["surrogate"]["fallback_fraction"],
+                "speedup_vs_plain_1m_neurons":
+                    extra["hh_surrogate_c5"]["same_network_1m_neurons"]["speedup_vs_plain_windowed"],
+                "spike_time_err_ms_1m_neurons":
+                    extra["hh_surrogate_c5"]["same_network_1m_neurons"]["surrogate"]["spike_time_err_ms"]}),
         }
         print(json.dumps(out), flush=True)
     eng.close()
@@ -447,38 +460,19 @@ def run_batch_config(local, rank, world, dist):
     return res
 
 
-def run_surrogate_config(local):
-    """The learned HH macro-step on the plain Hodgkin-Huxley network (100k
-    neurons, 10M synapses, dt 0.01 ms, Rush-Larsen): 10M transitions sampled
-    from the plain run (100 snapshots of all neurons, 0.5 ms apart, after a
-    20 ms warm-up; those with V in the envelope +- 3 mV kept), targets on the
-    device, training on the device; then the plain and the surrogate paths
-    timed over 100 ms each from the same state, spike times of the
-    surrogate run (and of the same macro-step scheme with one Rush-Larsen
-    step of 0.1 ms in the MLP's place) matched to the plain run's."""
+def _surrogate_eval(net, cfg, drive, sur, local, steps):
+    """Plain, surrogate and the two comparison modes from the same start,
+    timed; spike times matched to the plain run's (nearest within 2 ms)."""
     import torch
-    from neuralsim_b200 import SimulationEngine, configs, surrogate as S
-    net, cfg, drive, _ = configs.hh_c4()
-    cfg.device = local
-    cfg.window_steps = 100
-    cfg.spike_log_capacity, cfg.spike_log_steps = 50_000_000, 20_000
-    t0 = time.time()
-    sur, x, y, losses = S.train_for_network(net, cfg, drive, warm_steps=2000, snapshots=100,
-                                            every_steps=50, batch=8192, steps=4000)
-    train_s = time.time() - t0
-    steps = 10_000
-    res = {"neurons": net.n, "synapses": net.m, "dt_ms": cfg.dt_ms, "macro_step_ms": 0.1,
-           "mlp": "5-128-128-4 SiLU, bf16 weights, fp32 accumulation (tcgen05)",
-           "train_samples": int(len(x)), "train_steps": 4000, "train_batch": 8192,
-           "train_wall_s": round(train_s, 2), "final_loss": float(np.mean(losses[-100:])),
-           "envelope_mv": [S.V_LO, S.V_HI], "residual_mv": S.RESIDUAL_MV}
-    rasters = {}
-    for mode in ("plain", "surrogate", "coarse_rl_0.1ms"):
+    from neuralsim_b200 import SimulationEngine
+    from neuralsim_b200.raster import match_spikes
+    rasters, res = {}, {}
+    for mode in ("plain", "surrogate", "coarse_rl_0.1ms", "held_current_rl"):
         eng = SimulationEngine(net, cfg, drive)
         if mode != "plain":
             eng.attach_surrogate(sur)
             if mode != "surrogate":
-                eng.macro_step_mode(1)
+                eng.macro_step_mode(1 if mode == "coarse_rl_0.1ms" else 2)
         stream = torch.cuda.ExternalStream(eng.stream(), device=local)
         ms, spikes, events = timed_run(eng, steps, stream)
         rasters[mode] = eng.read_raster(0, steps)
@@ -490,13 +484,53 @@ def run_surrogate_config(local):
             r["fallback_fraction"] = fb / max(mlp + fb, 1)
         eng.close()
         res[mode] = r
-    from neuralsim_b200.raster import match_spikes
     w = int(round(2.0 / cfg.dt_ms))
-    for mode in ("surrogate", "coarse_rl_0.1ms"):
+    for mode in ("surrogate", "coarse_rl_0.1ms", "held_current_rl"):
         d, ua, ub = match_spikes(rasters["plain"], rasters[mode], w)
         res[mode]["spike_time_err_ms"] = float(d.mean() * cfg.dt_ms) if len(d) else None
         res[mode]["matched"], res[mode]["unmatched_plain"], res[mode]["unmatched_other"] = len(d), ua, ub
     res["speedup_vs_plain_windowed"] = res["plain"]["ns_per_sim_ms"] / res["surrogate"]["ns_per_sim_ms"]
+    return res
+
+
+def run_surrogate_config(local, train_steps=12000, only_1m=False):
+    """The learned HH macro-step on the plain Hodgkin-Huxley network (100k
+    neurons, 10M synapses, dt 0.01 ms, Rush-Larsen): about 10M transitions
+    sampled from the plain run (100 snapshots of all neurons, 0.5 ms apart,
+    after a 20 ms warm-up; those with V in the envelope +- 3 mV kept, the
+    approach to threshold weighted x4), targets and training on the device.
+    Then, from the same state, the plain and the surrogate paths each timed
+    over 100 ms and the surrogate's spike times matched to the plain run's;
+    beside them the same macro-step scheme with one Rush-Larsen step of
+    0.1 ms in the MLP's place (the plain method in the surrogate's cost
+    class) and with ten Rush-Larsen steps with the held current (the function
+    the MLP is trained on: the error of the scheme alone). The same trained
+    surrogate is also run on the same network shape at 1M neurons (100M
+    synapses), where the plain path is no longer bound by one Rush-Larsen
+    chain per neuron."""
+    from neuralsim_b200 import configs, surrogate as S
+    net, cfg, drive, _ = configs.hh_c4()
+    cfg.device = local
+    cfg.window_steps = 100
+    cfg.spike_log_capacity, cfg.spike_log_steps = 50_000_000, 20_000
+    t0 = time.time()
+    sur, x, y, losses = S.train_for_network(net, cfg, drive, warm_steps=2000, snapshots=100,
+                                            every_steps=50, batch=8192, steps=train_steps)
+    train_s = time.time() - t0
+    res = {"neurons": net.n, "synapses": net.m, "dt_ms": cfg.dt_ms, "macro_step_ms": 0.1,
+           "mlp": "5-128-128-4 SiLU, bf16 weights, fp32 accumulation (tcgen05)",
+           "train_samples": int(len(x)), "train_steps": train_steps, "train_batch": 8192,
+           "train_wall_s": round(train_s, 2), "final_loss": float(np.mean(losses[-100:])),
+           "envelope_mv": [S.V_LO, S.V_HI], "residual_mv": S.RESIDUAL_MV}
+    if not only_1m:
+        res.update(_surrogate_eval(net, cfg, drive, sur, local, 10_000))
+    big, bcfg, bdrive, _ = configs.hh_c4(n=1_000_000)
+    bcfg.device = local
+    bcfg.window_steps = 100
+    bcfg.spike_log_capacity, bcfg.spike_log_steps = 200_000_000, 5_000
+    r1 = _surrogate_eval(big, bcfg, bdrive, sur, local, 2_000)
+    r1.update({"neurons": big.n, "synapses": big.m, "timed_steps": 2_000})
+    res["same_network_1m_neurons"] = r1
     sur.close()
     return res
 
@@ -615,6 +649,16 @@ def run_reference(a):
 
 def main():
     a = args_()
+    if a.only:
+        import torch
+        torch.cuda.set_device(0)
+        if a.only == "c1c4":
+            print(json.dumps(run_extra_configs(0)), flush=True)
+        elif a.only == "c3":
+            print(json.dumps(run_batch_config(0, 0, 1, None)), flush=True)
+        else:
+            print(json.dumps(run_surrogate_config(0, a.sur_train_steps, a.sur_only_1m)), flush=True)
+        return
     if a.impl == "reference":
         run_reference(a)
     else:

@@ -65,6 +65,17 @@ ns_status ns_sur_set_norm(ns_sur* s, const float in_mean[5], const float in_scal
  * the normalised increments of every step. */
 ns_status ns_sur_train(ns_sur* s, uint32_t n_steps, float lr, float lr_decay, float* loss_out);
 
+/* Data-parallel training, one process per GPU: ns_sur_grad_step draws one
+ * minibatch from the training set and writes its loss gradient (flat order)
+ * to grad_dev (device, NS_SUR_PARAMS floats) without an update; the caller
+ * sums the gradients over ranks (one all-reduce of 17,796 floats) and
+ * ns_sur_apply_gradient takes one Adam step with scale * grad_dev. Ranks
+ * start from the same weights (ns_sur_set_params) and draw minibatches from
+ * distinct streams (ns_sur_set_sample_seed). */
+ns_status ns_sur_set_sample_seed(ns_sur* s, uint64_t seed);
+ns_status ns_sur_grad_step(ns_sur* s, float* grad_dev, float* loss_out);
+ns_status ns_sur_apply_gradient(ns_sur* s, const float* grad_dev, float scale, float lr);
+
 /* Gradient of the minibatch loss at the current weights for the given batch
  * (host x[batch][5] raw states, y[batch][4] raw targets), without an update:
  * grad_out (host, NS_SUR_PARAMS) in the flat parameter order; loss_out (host
@@ -102,9 +113,12 @@ ns_status ns_set_surrogate(ns_handle* h, const ns_sur* s, float v_lo, float v_hi
                            float residual_mv);
 
 /* What advances in-envelope neurons over a macro-step: 0 = the MLP (after
- * ns_set_surrogate), 1 = one Rush-Larsen step of the macro-step's length
+ * ns_set_surrogate); 1 = one Rush-Larsen step of the macro-step's length
  * (0.1 ms) with the same held current, envelope, residual check and fallback
- * — the plain method in the surrogate's cost class, for comparison. */
+ * — the plain method in the surrogate's cost class, for comparison; 2 = ten
+ * Rush-Larsen steps of 0.01 ms with the held current — the function the MLP
+ * is trained to reproduce, which separates the MLP's error from the error of
+ * holding the synaptic current over a macro-step. */
 ns_status ns_set_macro_step_mode(ns_handle* h, int32_t mode);
 
 /* Neuron macro-steps taken by the surrogate and by the Rush-Larsen fallback

@@ -103,6 +103,9 @@ SIGNATURES = {
     "ns_sur_get_params": (C.c_int32, [_P, _P]),
     "ns_sur_set_params": (C.c_int32, [_P, _P]),
     "ns_sur_predict": (C.c_int32, [_P, _P, C.c_uint64, _P]),
+    "ns_sur_set_sample_seed": (C.c_int32, [_P, C.c_uint64]),
+    "ns_sur_grad_step": (C.c_int32, [_P, _P, _P]),
+    "ns_sur_apply_gradient": (C.c_int32, [_P, _P, C.c_float, C.c_float]),
     "ns_tc_gemm_bf16": (C.c_int32, [_P, _P, _P, _P, _P, C.c_uint32, C.c_uint32, C.c_uint32,
                                     C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int32, _P]),
     "ns_set_surrogate": (C.c_int32, [_P, _P, C.c_float, C.c_float, C.c_float]),

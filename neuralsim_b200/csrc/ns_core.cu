@@ -59,6 +59,9 @@ struct ns_handle {
   // learned HH macro-step (ns_set_surrogate)
   bool sur_on = false;
   ns::SurDev sd{};
+  uint32_t* hstep = nullptr;        // [n_pad] hand-over steps of the surrogate window
+  uint32_t* fb_list = nullptr;      // [n_pad] neurons handed over in a window
+  uint32_t* fb_count = nullptr;     // their number
   std::vector<void*> sur_allocs;
 };
 
@@ -518,10 +521,18 @@ uint32_t window_len(const ns_config& c) {
 // Enqueues a window of Wc steps starting at graph-node offset j0.
 cudaError_t enqueue_window(ns_handle* h, uint32_t j0, uint32_t Wc) {
   const uint32_t nseg = h->d.nseg;
-  if (h->sur_on)
+  if (h->sur_on) {
+    h->sd.hstep = h->hstep;
+    h->sd.fb_list = h->fb_list;
+    h->sd.fb_count = h->fb_count;
     ns::k_window_sur<<<nseg, ns::kWinThreads, ns::kSurSmem, h->st>>>(h->d, h->sd, j0, Wc);
-  else
+    ns::k_window_fb<<<nseg, ns::kWinThreads, 0, h->st>>>(h->d, h->sd, j0, Wc);
+    const uint64_t pairs = (uint64_t)Wc * nseg;
+    ns::k_window_sort<<<(unsigned)((pairs + 255) / 256), 256, 0, h->st>>>(h->d, h->sd, j0, Wc);
+    h->launches += 2;
+  } else {
     pick_window(h->cfg.model, h->cfg.input_mode)<<<nseg, ns::kWinThreads, 0, h->st>>>(h->d, j0, Wc);
+  }
   pick_window_rows(h->cfg.input_mode, h->cfg.weight_format)
       <<<h->win_rows_blocks, 256, 0, h->st>>>(h->d, j0, Wc);
   ns::k_window_scan<<<Wc, 256, 0, h->st>>>(h->d, Wc);
@@ -571,7 +582,7 @@ ns_status run_steps(ns_handle* h, uint32_t n, uint32_t sched) {
     if (r) return r;
     while (left >= S) {
       CK(cudaGraphLaunch(ex, h->st));
-      if (h->win) h->launches += ((S + h->wcur - 1) / h->wcur) * (h->d.log_idx ? 5 : 4) + 1;
+      if (h->win) h->launches += ((S + h->wcur - 1) / h->wcur) * ((h->d.log_idx ? 5 : 4) + (h->sur_on ? 2 : 0)) + 1;
       else h->launches += (uint64_t)S * launches_per_step(h, sched) + 1;
       left -= S;
     }
@@ -1035,6 +1046,7 @@ static ns_status alloc_dynamic(ns_handle* h) {
     CK(cudaMemsetAsync(d.acc, 0, acc_bytes, h->st));
     if (d.inbits) CK(cudaMemsetAsync(d.inbits, 0, h->alloc_bytes[d.inbits], h->st));
     if (d.contrib) CK(cudaMemsetAsync(d.contrib, 0, h->alloc_bytes[d.contrib], h->st));
+    if (h->fb_count) CK(cudaMemsetAsync(h->fb_count, 0, 4, h->st));
     CK(cudaMemsetAsync(h->ctl, 0, sizeof(ns::Ctl), h->st));
     CK(cudaStreamSynchronize(h->st));
     return NS_OK;
@@ -1077,6 +1089,13 @@ static ns_status alloc_dynamic(ns_handle* h) {
     if ((st = dalloc(h, B, &d.seg_lst, (uint64_t)h->win * h->n_pad))) return st;
     if ((st = dalloc(h, B, &d.seg_off, (uint64_t)h->win * (d.nseg + 1)))) return st;
     if ((st = dalloc(h, B, &d.step_total, h->win))) return st;
+    h->hstep = nullptr;
+    h->fb_list = nullptr;
+    h->fb_count = nullptr;
+    if (c.model == NS_MODEL_HH &&
+        ((st = dalloc(h, B, &h->hstep, h->n_pad)) || (st = dalloc(h, B, &h->fb_list, h->n_pad)) ||
+         (st = dalloc(h, B, &h->fb_count, 1))))
+      return st;
     int nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pick_window_rows(c.input_mode, c.weight_format), 256, 0) != cudaSuccess || nb < 1) nb = 4;
     h->win_rows_blocks = h->sms * nb;
@@ -1734,6 +1753,7 @@ ns_status ns_set_surrogate(ns_handle* h, const ns_sur* s, float v_lo, float v_hi
   if (!h->have_neurons || !h->have_csr) return fail(h, NS_ERR_STATE, "upload neurons and CSR first");
   if (h->win < (uint32_t)ns::kSub)
     return fail(h, NS_ERR_UNSUPPORTED, "the surrogate needs windowed stepping with a window of at least 10 steps");
+  if (!h->hstep) return fail(h, NS_ERR_STATE, "no hand-over buffer (upload the network first)");
   ns_sur_view v{};
   ns_status r = ns_sur_view_of(s, &v);
   if (r) return fail(h, r, "bad surrogate handle");
@@ -1780,7 +1800,13 @@ ns_status ns_set_surrogate(ns_handle* h, const ns_sur* s, float v_lo, float v_hi
     double sum = 0.0, pw = 1.0;
     for (int q = 0; q < ns::kSub; ++q) { sum += pw; pw *= dd; }
     sd.gbar[t] = (float)(sum / ns::kSub);
-    sd.gdec9[t] = (float)std::pow(dd, ns::kSub - 1);
+    sd.gdec10[t] = (float)std::pow(dd, ns::kSub);
+    for (int r = 0; r < ns::kSub; ++r) {
+      double part = 0.0, p2 = 1.0;
+      for (int q = 0; q < ns::kSub - r; ++q) { part += p2; p2 *= dd; }
+      sd.wmean[r][t] = (float)(part / ns::kSub);
+      sd.wend[r][t] = (float)std::pow(dd, ns::kSub - 1 - r);
+    }
   }
   CK(cudaFuncSetAttribute(ns::k_window_sur, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ns::kSurSmem));
   CK(cudaStreamSynchronize(h->st));
@@ -1794,7 +1820,8 @@ ns_status ns_set_surrogate(ns_handle* h, const ns_sur* s, float v_lo, float v_hi
 ns_status ns_set_macro_step_mode(ns_handle* h, int32_t mode) {
   if (!h) return NS_ERR_NULL_HANDLE;
   if (!h->sur_on) return fail(h, NS_ERR_STATE, "attach a surrogate first");
-  if (mode != 0 && mode != 1) return fail(h, NS_ERR_INVALID_ARG, "mode 0 (MLP) or 1 (coarse Rush-Larsen)");
+  if (mode < 0 || mode > 2)
+    return fail(h, NS_ERR_INVALID_ARG, "mode 0 (MLP), 1 (one Rush-Larsen step of 0.1 ms) or 2 (held-current Rush-Larsen)");
   CK(cudaSetDevice(h->dev));
   CK(cudaStreamSynchronize(h->st));
   h->sd.coarse = mode;

@@ -42,6 +42,31 @@ __host__ __device__ __forceinline__ U4 draw(uint64_t seed, uint32_t idx, uint64_
                 (uint32_t)(seed >> 32));
 }
 
+__host__ __device__ __forceinline__ uint32_t word_of(const U4& x, uint32_t q) {
+  return q == 0 ? x.x : (q == 1 ? x.y : (q == 2 ? x.z : x.w));
+}
+
+// Poisson drive kinds (one 32-bit word per neuron-step): one Philox draw
+// serves four consecutive steps of a neuron; step k uses word k mod 4 of the
+// draw at counter k / 4. Returned in .x.
+__host__ __device__ __forceinline__ U4 poisson_draw(uint64_t seed, uint32_t idx, uint64_t k) {
+  return U4{word_of(draw(seed, idx, k >> 2, kStreamDrive), (uint32_t)(k & 3u)), 0u, 0u, 0u};
+}
+
+// The same stream for a loop over consecutive steps of one neuron: the draw
+// is made once per four steps.
+struct PoissonWords {
+  U4 w;
+  uint64_t blk = ~0ull;
+  __device__ __forceinline__ uint32_t at(uint64_t seed, uint32_t idx, uint64_t k) {
+    if ((k >> 2) != blk) {
+      blk = k >> 2;
+      w = draw(seed, idx, blk, kStreamDrive);
+    }
+    return word_of(w, (uint32_t)(k & 3u));
+  }
+};
+
 // 24-bit uniforms, exact in float: [0,1) and (0,1).
 __host__ __device__ __forceinline__ float unif(uint32_t x) { return (float)(x >> 8) * 0x1p-24f; }
 __host__ __device__ __forceinline__ float unif_open(uint32_t x) {

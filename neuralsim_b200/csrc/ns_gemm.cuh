@@ -56,6 +56,14 @@ __device__ __forceinline__ uint16_t f32_to_bf16_rn(float x) {
   return *reinterpret_cast<const uint16_t*>(&b);
 }
 
+// x = hi + lo with hi = bf16(x): the BF16 pair carries ~16 significant bits
+// of x into a tensor-core product whose weight column is duplicated.
+__device__ __forceinline__ void split_bf16(float x, uint16_t& hi, uint16_t& lo) {
+  const __nv_bfloat16 h = __float2bfloat16_rn(x);
+  hi = *reinterpret_cast<const uint16_t*>(&h);
+  lo = f32_to_bf16_rn(x - __bfloat162float(h));
+}
+
 // Copies rows [0, R) x K-chunk [k0, k0 + KC) of a K-major bf16 matrix into
 // the canonical no-swizzle layout of an R x KC tile (16-byte pieces).
 template <int R, int KC>

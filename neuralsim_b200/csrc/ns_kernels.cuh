@@ -186,12 +186,6 @@ __device__ __forceinline__ void drive_key(const NsDev& d, uint64_t i, uint64_t& 
   }
 }
 
-__device__ __forceinline__ U4 make_drive_draw(const NsDev& d, uint64_t i0, uint64_t k) {
-  if (d.drive_kind == 3) return draw(d.seed, (uint32_t)(i0 >> 1), k, kStreamDrive);
-  if (d.drive_kind == 0) return U4{0u, 0u, 0u, 0u};
-  return draw(d.seed, (uint32_t)i0, k, kStreamDrive);
-}
-
 template <int MODEL>
 __device__ __forceinline__ bool model_step(const NsDev& d, NState& s, const float* p, int rsteps,
                                            float Iin, float kick, bool delta) {
@@ -305,7 +299,8 @@ __device__ __forceinline__ bool update_one(const NsDev& d, uint64_t k, uint64_t 
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
       float inc = S[t] * kSyn[t].gmax;
-      if (kSyn[t].mg) inc = inc * (1.0f / (1.0f + (1.0f / 3.57f) * expf(-0.062f * vi)));
+      // Mg block only on a delivered increment (0 times a finite factor is 0)
+      if (kSyn[t].mg && inc != 0.0f) inc = inc * (1.0f / (1.0f + (1.0f / 3.57f) * expf(-0.062f * vi)));
       float g = G[t] * d.Gdec[t] + inc;
       if (t == 0) g = g + addg;
       G[t] = g;
@@ -448,11 +443,16 @@ __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
     U4 y2[2];
     float z[2] = {0.f, 0.f};
     if (d.net_of == nullptr) {
-      const U4 x = make_drive_draw(d, i0, k);
-      if (d.drive_kind == 3) gauss_pair(x, z[0], z[1]);
-      y2[0] = x;
-      y2[1] = (d.drive_kind == 1 || d.drive_kind == 2 || d.drive_kind == 4)
-                  ? draw(d.seed, (uint32_t)(i0 + 1), k, kStreamDrive) : x;
+      y2[0] = y2[1] = U4{0u, 0u, 0u, 0u};
+      if (d.drive_kind == 3) {
+        gauss_pair(draw(d.seed, (uint32_t)(i0 >> 1), k, kStreamDrive), z[0], z[1]);
+      } else if (d.drive_kind == 1) {
+        y2[0] = draw(d.seed, (uint32_t)i0, k, kStreamDrive);
+        y2[1] = draw(d.seed, (uint32_t)(i0 + 1), k, kStreamDrive);
+      } else if (d.drive_kind != 0) {
+        y2[0] = poisson_draw(d.seed, (uint32_t)i0, k);
+        y2[1] = poisson_draw(d.seed, (uint32_t)(i0 + 1), k);
+      }
     } else {
       // batch: the pair may straddle two networks, so each neuron draws
       // from its own network's stream (Gaussian pairs by local index)
@@ -466,8 +466,10 @@ __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
           float g0, g1;
           gauss_pair(draw(sd, li >> 1, k, kStreamDrive), g0, g1);
           z[e] = (li & 1u) ? g1 : g0;
-        } else if (d.drive_kind != 0) {
+        } else if (d.drive_kind == 1) {
           y2[e] = draw(sd, li, k, kStreamDrive);
+        } else if (d.drive_kind != 0) {
+          y2[e] = poisson_draw(sd, li, k);
         }
       }
     }

@@ -56,6 +56,7 @@ struct ns_sur {
   float dt = 0.01f;
   uint32_t B = 0;
   uint64_t seed = 0;
+  uint64_t sample_seed = 0;             // minibatch sampling stream
   uint64_t t = 0;                       // Adam steps taken
   Norm norm{};
   std::vector<void*> allocs;
@@ -117,13 +118,23 @@ __global__ void k_sur_targets(const float* X, float* Y, uint64_t n, HhP hp, floa
   }
 }
 
-// Batch assembly: normalised inputs (Xp [B][16], XT [16][B], zero padded)
-// and normalised target increments Tn [B][4]. Row b takes sample
+// One Rush-Larsen step of the macro-step's length with the current held:
+// the base the MLP's output corrects.
+__device__ __forceinline__ void sur_base(const float* x, const HhP& hp, float dt_macro, float* b) {
+  float v = x[0], m = x[1], h = x[2], n = x[3];
+  ns::hh_rl_step(v, m, h, n, x[4], hp.p, dt_macro);
+  b[0] = v; b[1] = m; b[2] = h; b[3] = n;
+}
+
+// Batch assembly: normalised inputs (Xp [B][16], XT [16][B]; column k < 5
+// holds the BF16 value of input k, column 5 + k its BF16 remainder, the
+// rest zero) and normalised targets Tn [B][4]: the state 0.1 ms later minus
+// the base. Row b takes sample
 // hash(seed, step, b) mod n when sampling, else row first + b (zeros past
 // n_valid).
 __global__ void k_sur_gather(uint32_t B, const float* X, const float* Y, uint64_t n, int sample,
                              uint64_t seed, uint64_t step, uint64_t first, uint64_t n_valid,
-                             Norm nm, uint16_t* Xp, uint16_t* XT, float* Tn) {
+                             Norm nm, HhP hp, float dt_macro, uint16_t* Xp, uint16_t* XT, float* Tn) {
   const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= B) return;
   uint64_t idx;
@@ -139,18 +150,25 @@ __global__ void k_sur_gather(uint32_t B, const float* X, const float* Y, uint64_
   for (int k = 0; k < 5; ++k) x[k] = valid ? X[idx * 5 + k] : 0.0f;
 #pragma unroll
   for (int k = 0; k < 4; ++k) y[k] = (valid && Y) ? Y[idx * 4 + k] : 0.0f;
+  uint16_t col[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) col[k] = 0;
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    const float xn = valid ? (x[k] - nm.in_mean[k]) / nm.in_scale[k] : 0.0f;
+    ns::gemm::split_bf16(xn, col[k], col[5 + k]);
+  }
 #pragma unroll
   for (int k = 0; k < 16; ++k) {
-    float xn = 0.0f;
-    if (k < 5 && valid) xn = (x[k] - nm.in_mean[k]) / nm.in_scale[k];
-    const uint16_t q = ns::gemm::f32_to_bf16_rn(xn);
-    Xp[(uint64_t)b * 16 + k] = q;
-    XT[(uint64_t)k * B + b] = q;
+    Xp[(uint64_t)b * 16 + k] = col[k];
+    XT[(uint64_t)k * B + b] = col[k];
   }
   if (Tn) {
+    float base[4] = {0.f, 0.f, 0.f, 0.f};
+    if (valid) sur_base(x, hp, dt_macro, base);
 #pragma unroll
     for (int k = 0; k < 4; ++k)
-      Tn[(uint64_t)b * 4 + k] = valid ? ((y[k] - x[k]) - nm.out_mean[k]) / nm.out_scale[k] : 0.0f;
+      Tn[(uint64_t)b * 4 + k] = valid ? ((y[k] - base[k]) - nm.out_mean[k]) / nm.out_scale[k] : 0.0f;
   }
 }
 
@@ -226,7 +244,7 @@ __global__ void k_transpose16(const uint16_t* in, uint16_t* out, uint32_t R, uin
 // Flat gradient from the GEMM accumulators, in parameter order.
 __device__ __forceinline__ float grad_of(uint32_t q, const float* gW1, const float* gW2,
                                          const float* gW3, const float* gB) {
-  if (q < (uint32_t)kPB1) return gW1[(q / 5) * 16 + (q % 5)];
+  if (q < (uint32_t)kPB1) return gW1[(q / 5) * 16 + (q % 5)] + gW1[(q / 5) * 16 + 5 + (q % 5)];
   if (q < (uint32_t)kPW2) return gB[q - kPB1];
   if (q < (uint32_t)kPB2) return gW2[q - kPW2];
   if (q < (uint32_t)kPW3) return gB[128 + (q - kPB2)];
@@ -239,7 +257,8 @@ __device__ __forceinline__ void write_bf16(uint32_t q, float w, uint16_t* W1p, u
                                            uint16_t* W2T, uint16_t* W3p, uint16_t* W3T) {
   const uint16_t b = ns::gemm::f32_to_bf16_rn(w);
   if (q < (uint32_t)kPB1) {
-    W1p[(q / 5) * 16 + (q % 5)] = b;
+    W1p[(q / 5) * 16 + (q % 5)] = b;       // weight of the input's BF16 value
+    W1p[(q / 5) * 16 + 5 + (q % 5)] = b;   // and of its remainder
   } else if (q >= (uint32_t)kPW2 && q < (uint32_t)kPB2) {
     const uint32_t o = (q - kPW2) / kH, i = (q - kPW2) % kH;
     W2b[o * kH + i] = b;
@@ -268,6 +287,23 @@ __global__ void k_sur_adam(float* P, float* M, float* V, const float* gW1, const
   write_bf16(q, w, W1p, W2b, W2T, W3p, W3T);
 }
 
+// Adam from a flat gradient (data-parallel training: the gradient summed
+// over ranks by the caller)
+__global__ void k_sur_adam_flat(float* P, float* M, float* V, const float* g_in, float scale,
+                                float lr, float c1, float c2, uint16_t* W1p, uint16_t* W2b,
+                                uint16_t* W2T, uint16_t* W3p, uint16_t* W3T) {
+  const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= NS_SUR_PARAMS) return;
+  const float g = g_in[q] * scale;
+  const float m = 0.9f * M[q] + 0.1f * g;
+  const float v = 0.999f * V[q] + 0.001f * g * g;
+  M[q] = m;
+  V[q] = v;
+  const float w = P[q] - lr * (m / c1) / (sqrtf(v / c2) + 1e-8f);
+  P[q] = w;
+  write_bf16(q, w, W1p, W2b, W2T, W3p, W3T);
+}
+
 __global__ void k_sur_refresh(const float* P, uint16_t* W1p, uint16_t* W2b, uint16_t* W2T,
                               uint16_t* W3p, uint16_t* W3T) {
   const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -276,13 +312,15 @@ __global__ void k_sur_refresh(const float* P, uint16_t* W1p, uint16_t* W2b, uint
 
 // raw states 0.1 ms later from the network output
 __global__ void k_sur_decode(uint32_t B, uint64_t first, uint64_t n, const float* X, const float* Yo,
-                             const float* b3, Norm nm, float* out) {
+                             const float* b3, Norm nm, HhP hp, float dt_macro, float* out) {
   const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
   const uint64_t i = first + b;
   if (b >= B || i >= n) return;
+  float base[4];
+  sur_base(X + i * 5, hp, dt_macro, base);
 #pragma unroll
   for (int k = 0; k < 4; ++k)
-    out[i * 4 + k] = X[i * 5 + k] + (Yo[(uint64_t)b * 16 + k] + b3[k]) * nm.out_scale[k] + nm.out_mean[k];
+    out[i * 4 + k] = base[k] + (Yo[(uint64_t)b * 16 + k] + b3[k]) * nm.out_scale[k] + nm.out_mean[k];
 }
 
 template <int N, int KC, int EPI>
@@ -433,6 +471,7 @@ ns_status ns_sur_create(int device, const float hh_params[7], float dt_fine_ms, 
   s->dt = dt_fine_ms;
   s->B = batch;
   s->seed = seed;
+  s->sample_seed = seed;
   for (int k = 0; k < 5; ++k) { s->norm.in_mean[k] = 0.f; s->norm.in_scale[k] = 1.f; }
   for (int k = 0; k < 4; ++k) { s->norm.out_mean[k] = 0.f; s->norm.out_scale[k] = 1.f; }
   auto bad = [&](cudaError_t e) {
@@ -568,8 +607,9 @@ ns_status ns_sur_train(ns_sur* s, uint32_t n_steps, float lr, float lr_decay, fl
   SCK(cudaMemsetAsync(s->errw, 0, 4, s->st));
   float l = lr;
   for (uint32_t q = 0; q < n_steps; ++q) {
-    k_sur_gather<<<(s->B + 255) / 256, 256, 0, s->st>>>(s->B, s->X, s->Y, s->n_data, 1, s->seed,
-                                                        s->t, 0, 0, s->norm, s->Xp, s->XT, s->Tn);
+    k_sur_gather<<<(s->B + 255) / 256, 256, 0, s->st>>>(s->B, s->X, s->Y, s->n_data, 1,
+                                                        s->sample_seed, s->t, 0, 0, s->norm, s->hh,
+                                                        s->dt * NS_SUR_SUBSTEPS, s->Xp, s->XT, s->Tn);
     SCK(forward(s));
     SCK(backward_update(s, s->lossv + q, l, nullptr));
     l *= lr_decay;
@@ -578,6 +618,48 @@ ns_status ns_sur_train(ns_sur* s, uint32_t n_steps, float lr, float lr_decay, fl
     SCK(cudaMemcpyAsync(loss_out, s->lossv, (size_t)n_steps * 4, cudaMemcpyDeviceToHost, s->st));
   SCK(cudaStreamSynchronize(s->st));
   return check_err(s);
+}
+
+ns_status ns_sur_set_sample_seed(ns_sur* s, uint64_t seed) {
+  if (!s) return NS_ERR_NULL_HANDLE;
+  s->sample_seed = seed;
+  return NS_OK;
+}
+
+ns_status ns_sur_grad_step(ns_sur* s, float* grad_dev, float* loss_out) {
+  if (!s) return NS_ERR_NULL_HANDLE;
+  if (!s->X) return sfail(s, NS_ERR_STATE, "no training set");
+  if (!grad_dev) return sfail(s, NS_ERR_INVALID_ARG, "null gradient buffer");
+  SCK(cudaSetDevice(s->dev));
+  if (s->loss_cap < 1) {
+    SCK(cudaMalloc(&s->lossv, 4));
+    s->loss_cap = 1;
+  }
+  SCK(cudaMemsetAsync(s->lossv, 0, 4, s->st));
+  SCK(cudaMemsetAsync(s->errw, 0, 4, s->st));
+  k_sur_gather<<<(s->B + 255) / 256, 256, 0, s->st>>>(s->B, s->X, s->Y, s->n_data, 1, s->sample_seed,
+                                                      s->t, 0, 0, s->norm, s->hh, s->dt * NS_SUR_SUBSTEPS, s->Xp, s->XT, s->Tn);
+  SCK(forward(s));
+  SCK(backward_update(s, s->lossv, 0.0f, grad_dev));
+  float l = 0.0f;
+  SCK(cudaMemcpyAsync(&l, s->lossv, 4, cudaMemcpyDeviceToHost, s->st));
+  SCK(cudaStreamSynchronize(s->st));
+  if (loss_out) *loss_out = l;
+  return check_err(s);
+}
+
+ns_status ns_sur_apply_gradient(ns_sur* s, const float* grad_dev, float scale, float lr) {
+  if (!s) return NS_ERR_NULL_HANDLE;
+  if (!grad_dev) return sfail(s, NS_ERR_INVALID_ARG, "null gradient buffer");
+  if (!(lr > 0.0f) || !std::isfinite(scale)) return sfail(s, NS_ERR_INVALID_ARG, "lr > 0 and a finite scale");
+  SCK(cudaSetDevice(s->dev));
+  s->t += 1;
+  const double c1 = 1.0 - std::pow(0.9, (double)s->t), c2 = 1.0 - std::pow(0.999, (double)s->t);
+  k_sur_adam_flat<<<(NS_SUR_PARAMS + 255) / 256, 256, 0, s->st>>>(
+      s->P, s->Am, s->Av, grad_dev, scale, lr, (float)c1, (float)c2, s->W1p, s->W2b, s->W2T, s->W3p, s->W3T);
+  SCK(cudaGetLastError());
+  SCK(cudaStreamSynchronize(s->st));
+  return NS_OK;
 }
 
 ns_status ns_sur_gradient(ns_sur* s, const float* x, const float* y, float* grad_out, float* loss_out) {
@@ -594,7 +676,7 @@ ns_status ns_sur_gradient(ns_sur* s, const float* x, const float* y, float* grad
   SCK(cudaMalloc(&lslot, 4));
   cudaMemsetAsync(lslot, 0, 4, s->st);
   k_sur_gather<<<(s->B + 255) / 256, 256, 0, s->st>>>(s->B, s->Xs, s->Ys, s->B, 0, 0, 0, 0, s->B,
-                                                      s->norm, s->Xp, s->XT, s->Tn);
+                                                      s->norm, s->hh, s->dt * NS_SUR_SUBSTEPS, s->Xp, s->XT, s->Tn);
   cudaError_t e = forward(s);
   if (e == cudaSuccess) e = backward_update(s, lslot, 0.0f, s->G);
   float lh = 0.0f;
@@ -619,10 +701,11 @@ ns_status ns_sur_predict(ns_sur* s, const float* x, uint64_t n, float* y) {
   if (e == cudaSuccess) e = cudaMemcpyAsync(xd, x, n * 20, cudaMemcpyHostToDevice, s->st);
   for (uint64_t f = 0; f < n && e == cudaSuccess; f += s->B) {
     k_sur_gather<<<(s->B + 255) / 256, 256, 0, s->st>>>(s->B, xd, nullptr, n, 0, 0, 0, f, n, s->norm,
-                                                        s->Xp, s->XT, nullptr);
+                                                        s->hh, s->dt * NS_SUR_SUBSTEPS, s->Xp, s->XT, nullptr);
     e = forward(s);
     if (e == cudaSuccess) {
-      k_sur_decode<<<(s->B + 255) / 256, 256, 0, s->st>>>(s->B, f, n, xd, s->Yo, s->P + kPB3, s->norm, yd);
+      k_sur_decode<<<(s->B + 255) / 256, 256, 0, s->st>>>(s->B, f, n, xd, s->Yo, s->P + kPB3, s->norm,
+                                                           s->hh, s->dt * NS_SUR_SUBSTEPS, yd);
       e = cudaGetLastError();
     }
   }

@@ -54,11 +54,12 @@ __global__ void __launch_bounds__(kWinThreads) k_window(NsDev d, uint32_t j0, ui
   uint64_t dseed;
   uint32_t dli;
   drive_key(d, i, dseed, dli);
+  PoissonWords pw;
   const uint64_t words = d.n_pad >> 5;
   unsigned long long my_spk = 0;
-  for (uint32_t s = 0; s < W; ++s) {
+  uint32_t slot = (uint32_t)(k0 % d.D);   // advanced by one (mod D) per step
+  for (uint32_t s = 0; s < W; ++s, slot = (slot + 1u == d.D) ? 0u : slot + 1u) {
     const uint64_t k = k0 + s;
-    const uint32_t slot = (uint32_t)(k % d.D);
     int nk = 0;
     if (d.drive_kind == 1) {
       // reference-shaped global kicks (engine.rs:280-287): lane j computes kick j
@@ -104,8 +105,10 @@ __global__ void __launch_bounds__(kWinThreads) k_window(NsDev d, uint32_t j0, ui
       float z0, z1;
       gauss_pair(draw(dseed, dli >> 1, k, kStreamDrive), z0, z1);
       z = (dli & 1u) ? z1 : z0;
-    } else if (d.drive_kind != 0) {
+    } else if (d.drive_kind == 1) {
       y = draw(dseed, dli, k, kStreamDrive);
+    } else if (d.drive_kind != 0) {
+      y.x = pw.at(dseed, dli, k);
     }
     float addI, kick, addg;
     drive_of(d, y, z, inh, addI, kick, addg);

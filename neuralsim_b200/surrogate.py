@@ -29,6 +29,35 @@ def _p(a):
     return None if a is None else C.c_void_p(a.ctypes.data)
 
 
+def _hh_rates(v):
+    x = (v + 40.0) / 10.0
+    xs = np.where(x == 0.0, 1.0, x)
+    am = np.where(x == 0.0, 1.0, xs / (-np.expm1(-xs)))
+    bm = 4.0 * np.exp(-(v + 65.0) / 18.0)
+    ah = 0.07 * np.exp(-(v + 65.0) / 20.0)
+    bh = 1.0 / (1.0 + np.exp(-(v + 35.0) / 10.0))
+    y = (v + 55.0) / 10.0
+    ys = np.where(y == 0.0, 1.0, y)
+    an = np.where(y == 0.0, 0.1, 0.1 * ys / (-np.expm1(-ys)))
+    bn = 0.125 * np.exp(-(v + 65.0) / 80.0)
+    return am, bm, ah, bh, an, bn
+
+
+def coarse_base(x, hh_params, dt_macro):
+    """One Rush-Larsen step of the macro-step's length with the current held:
+    the base whose correction the MLP predicts. x [n][5] -> [n][4]."""
+    x = np.asarray(x, np.float64)
+    v, m, h, n, I = (x[:, k] for k in range(5))
+    gna, gk, gl, ena, ek, el, cm = hh_params
+    am, bm, ah, bh, an, bn = _hh_rates(v)
+    sm, sh, sn = am + bm, ah + bh, an + bn
+    m = am / sm + (m - am / sm) * np.exp(-dt_macro * sm)
+    h = ah / sh + (h - ah / sh) * np.exp(-dt_macro * sh)
+    n = an / sn + (n - an / sn) * np.exp(-dt_macro * sn)
+    iion = gna * m ** 3 * h * (v - ena) + gk * n ** 4 * (v - ek) + gl * (v - el)
+    return np.stack([v + dt_macro * (I - iion) / cm, m, h, n], 1)
+
+
 def macro_current(G, v, dt_fine):
     """Synaptic current held over a macro-step of SUBSTEPS fine steps: the
     mean of each decaying conductance over the macro-step times its driving
@@ -48,6 +77,7 @@ class Surrogate:
         self.batch = int(batch)
         self._h = C.c_void_p()
         hp = np.asarray(hh_params, np.float32)
+        self.hh_params = tuple(float(q) for q in hp)
         st = self.lib.ns_sur_create(int(device), _p(hp), float(dt_fine), self.batch, int(seed),
                                     C.byref(self._h))
         if st != A.NS_OK:
@@ -76,9 +106,9 @@ class Surrogate:
 
     def fit_norm(self, x, y):
         """Normalisation from a training set: inputs to zero mean / unit
-        scale, increments likewise."""
+        scale, the corrections to the coarse base step likewise."""
         x = np.asarray(x, np.float64)
-        dy = np.asarray(y, np.float64) - x[:, :4]
+        dy = np.asarray(y, np.float64) - coarse_base(x, self.hh_params, SUBSTEPS * self.dt_fine)
         self.set_norm(x.mean(0), np.maximum(x.std(0), 1e-6), dy.mean(0), np.maximum(dy.std(0), 1e-9))
 
     def train(self, steps, lr=2e-3, lr_decay=None, lr_final=1e-4):
@@ -99,6 +129,21 @@ class Surrogate:
         l = np.zeros(1, np.float32)
         self._check(self.lib.ns_sur_gradient(self._h, _p(x), _p(y), _p(g), _p(l)))
         return g, float(l[0])
+
+    def set_sample_seed(self, seed):
+        self._check(self.lib.ns_sur_set_sample_seed(self._h, int(seed)))
+
+    def grad_step(self, grad):
+        """Gradient of one sampled minibatch into `grad` (a CUDA float32
+        tensor of N_PARAMS values); returns the minibatch loss."""
+        l = np.zeros(1, np.float32)
+        self._check(self.lib.ns_sur_grad_step(self._h, C.c_void_p(grad.data_ptr()), _p(l)))
+        return float(l[0])
+
+    def apply_gradient(self, grad, scale, lr):
+        """One Adam step with scale * grad (a CUDA float32 tensor)."""
+        self._check(self.lib.ns_sur_apply_gradient(self._h, C.c_void_p(grad.data_ptr()),
+                                                   float(scale), float(lr)))
 
     @property
     def params(self):
@@ -154,10 +199,12 @@ def sample_states(engine, n_snapshots, every_steps, rng=None, per_snapshot=None)
 
 def train_for_network(net, cfg, drive, warm_steps=2000, snapshots=100, every_steps=50,
                       v_lo=V_LO, v_hi=V_HI, margin=3.0, batch=8192, steps=4000, lr=2e-3,
-                      seed=46, per_snapshot=None):
+                      seed=46, per_snapshot=None, focus_v=-62.0, focus_repeat=4):
     """Samples states from a plain Rush-Larsen run of the network (after
     warm_steps), keeps those with V within the envelope (plus a margin),
-    computes their targets on the device and trains a surrogate. The network's
+    computes their targets on the device and trains a surrogate. States with
+    V above focus_v (the approach to threshold, where an error moves a spike
+    time most) enter the training set focus_repeat times. The network's
     neurons share one HH parameter row (the first neuron's). Returns
     (surrogate, states, targets, losses)."""
     from .engine import SimulationEngine
@@ -169,12 +216,48 @@ def train_for_network(net, cfg, drive, warm_steps=2000, snapshots=100, every_ste
         eng.close()
     keep = (x[:, 0] >= v_lo - margin) & (x[:, 0] <= v_hi + margin)
     x = x[keep]
+    if focus_repeat > 1:
+        near = x[x[:, 0] > focus_v]
+        x = np.concatenate([x] + [near] * (focus_repeat - 1))
     sur = Surrogate(hh_params=net.params[0], dt_fine=cfg.dt_ms, batch=batch, seed=seed,
                     device=cfg.device)
     y = sur.set_data(x)
     sur.fit_norm(x, y)
     losses = sur.train(steps, lr)
     return sur, x, y, losses
+
+
+def train_data_parallel(sur, steps, lr=2e-3, lr_final=1e-4, rank=0, world=1, group=None,
+                        grad=None):
+    """Data-parallel training, one process per GPU: every rank computes the
+    gradient of its own minibatch, one all-reduce (sum) of the 17,796 FP32
+    gradients averages them, and every rank takes the same Adam step. The
+    ranks must hold the same weights before the first step (broadcast from
+    rank 0 here) and sample from distinct streams. Returns the mean loss of
+    every step over the ranks. `grad`: the gradient buffer (a CUDA tensor);
+    allocated here when None."""
+    import torch
+    if grad is None:
+        grad = torch.zeros(N_PARAMS, dtype=torch.float32, device="cuda")
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        p = torch.from_numpy(sur.params).to(grad.device)
+        dist.broadcast(p, 0, group=group)
+        sur.params = p.cpu().numpy()
+    decay = (lr_final / lr) ** (1.0 / max(steps, 1))
+    losses = np.zeros(steps, np.float64)
+    l_t = torch.zeros(1, dtype=torch.float64, device=grad.device)
+    for q in range(steps):
+        loss = sur.grad_step(grad)
+        if dist is not None:
+            dist.all_reduce(grad, group=group)
+            l_t.fill_(loss)
+            dist.all_reduce(l_t, group=group)
+            loss = float(l_t.item())
+        sur.apply_gradient(grad, 1.0 / world, lr * decay ** q)
+        losses[q] = loss / world
+    return losses
 
 
 def tc_gemm(A_, B_, C_=None, H_=None, bias=None, splits=1, epilogue=0, stream=None):

@@ -270,9 +270,9 @@ template <> inline DriveOut<float> neuron_drive<float>(const or_config& c, const
       draw(c.seed, (uint32_t)i, k, STREAM_DRIVE, x);
       if (unif_f(x[0]) < (float)c.p) d.add_I = unif_f(x[1]) * (float)c.amp;
       break;
-    case 2:
-      draw(c.seed, (uint32_t)i, k, STREAM_DRIVE, x);
-      if (x[0] < prob_threshold(c.p)) d.kick = (float)c.amp;
+    case 2:  // Poisson kinds: one draw serves steps 4q .. 4q+3, word k mod 4
+      draw(c.seed, (uint32_t)i, k >> 2, STREAM_DRIVE, x);
+      if (x[k & 3] < prob_threshold(c.p)) d.kick = (float)c.amp;
       break;
     case 3: {
       draw(c.seed, (uint32_t)(i >> 1), k, STREAM_DRIVE, x);
@@ -288,8 +288,8 @@ template <> inline DriveOut<float> neuron_drive<float>(const or_config& c, const
       break;
     }
     case 4:
-      draw(c.seed, (uint32_t)i, k, STREAM_DRIVE, x);
-      if (x[0] < prob_threshold(c.p)) d.add_g = (float)c.amp;
+      draw(c.seed, (uint32_t)i, k >> 2, STREAM_DRIVE, x);
+      if (x[k & 3] < prob_threshold(c.p)) d.add_g = (float)c.amp;
       break;
     default: break;
   }
@@ -305,9 +305,9 @@ template <> inline DriveOut<double> neuron_drive<double>(const or_config& c, con
       draw(c.seed, (uint32_t)i, k, STREAM_DRIVE, x);
       if (unif_d(x[0]) < (double)(float)c.p) d.add_I = unif_d(x[1]) * c.amp;
       break;
-    case 2:
-      draw(c.seed, (uint32_t)i, k, STREAM_DRIVE, x);
-      if (x[0] < prob_threshold(c.p)) d.kick = c.amp;
+    case 2:  // Poisson kinds: one draw serves steps 4q .. 4q+3, word k mod 4
+      draw(c.seed, (uint32_t)i, k >> 2, STREAM_DRIVE, x);
+      if (x[k & 3] < prob_threshold(c.p)) d.kick = c.amp;
       break;
     case 3: {
       draw(c.seed, (uint32_t)(i >> 1), k, STREAM_DRIVE, x);
@@ -321,8 +321,8 @@ template <> inline DriveOut<double> neuron_drive<double>(const or_config& c, con
       break;
     }
     case 4:
-      draw(c.seed, (uint32_t)i, k, STREAM_DRIVE, x);
-      if (x[0] < prob_threshold(c.p)) d.add_g = c.amp;
+      draw(c.seed, (uint32_t)i, k >> 2, STREAM_DRIVE, x);
+      if (x[k & 3] < prob_threshold(c.p)) d.add_g = c.amp;
       break;
     default: break;
   }

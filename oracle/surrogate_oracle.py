@@ -34,13 +34,14 @@ def dsilu(z):
     return s + z * s * (1.0 - s)
 
 
-def normalise(x, y, norm):
-    """Normalised inputs and (if y is given) normalised target increments."""
+def normalise(x, y, norm, base):
+    """Normalised inputs and (if y is given) normalised targets: the state
+    0.1 ms later minus `base` (one Rush-Larsen step of 0.1 ms)."""
     x = np.asarray(x, np.float64)
     xn = (x - norm["in_mean"]) / norm["in_scale"]
     tn = None
     if y is not None:
-        tn = ((np.asarray(y, np.float64) - x[:, :4]) - norm["out_mean"]) / norm["out_scale"]
+        tn = ((np.asarray(y, np.float64) - base) - norm["out_mean"]) / norm["out_scale"]
     return xn, tn
 
 

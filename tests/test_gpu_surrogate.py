@@ -83,7 +83,8 @@ def test_gradient_matches_fp64_oracle(lib):
     s.fit_norm(x, y)
     g, loss = s.gradient(x, y)
     nm = {k: v.astype(np.float64) for k, v in s.norm.items()}
-    xn, tn = so.normalise(x, y, nm)
+    base = so.rush_larsen(x.astype(np.float64), S.SQUID, 0.1, 1)
+    xn, tn = so.normalise(x, y, nm, base)
     want_loss, want = so.loss_and_grad(s.params.astype(np.float64), xn, tn)
     assert abs(loss - want_loss) <= 0.02 * want_loss
     o = 0
@@ -148,15 +149,15 @@ def test_network_spike_times_against_plain(lib):
     net, cfg, drive = tnets.hh_cond(n=2000, k=50)
     cfg.window_steps = 100
     sur, x, y, losses = S.train_for_network(net, cfg, drive, warm_steps=2000, snapshots=60,
-                                            every_steps=50, batch=8192, steps=2000)
+                                            every_steps=50, batch=8192, steps=6000)
     steps = 5000
     res = {}
-    for mode in ("plain", "surrogate", "coarse"):
+    for mode in ("plain", "surrogate", "coarse", "held"):
         eng = SimulationEngine(net, cfg, drive)
         if mode != "plain":
             eng.attach_surrogate(sur)
-            if mode == "coarse":
-                eng.macro_step_mode(1)
+            if mode != "surrogate":
+                eng.macro_step_mode(1 if mode == "coarse" else 2)
         eng.run(steps)
         res[mode] = eng.read_raster(0, steps)
         if mode != "plain":
@@ -169,7 +170,9 @@ def test_network_spike_times_against_plain(lib):
     assert n_plain > 500
     err_s = ds.mean() * cfg.dt_ms
     err_c = dc.mean() * cfg.dt_ms if len(dc) else np.inf
-    print("surrogate", err_s, ua, ub, res["surrogate_counts"], "coarse", err_c, uca, ucb)
+    dh, uha, uhb = tnets.match_spikes(res["plain"], res["held"], w)
+    print("surrogate", err_s, ua, ub, res["surrogate_counts"], "coarse", err_c, uca, ucb,
+          "held-current RL", dh.mean() * cfg.dt_ms, uha, uhb)
     assert res["surrogate_counts"][0] > 0
     assert err_s <= 0.2
     assert err_s <= err_c

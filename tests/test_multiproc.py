@@ -97,3 +97,67 @@ def test_run_sharded_gloo_world2(lib, oracle_lib):
         p.join(timeout=60)
         assert p.exitcode == 0
     assert got[0] == want and got[1] == want
+
+
+class _FakeSurrogate:
+    """Stands in for a device surrogate: a rank-dependent gradient per step
+    and a record of the applied (scaled) gradients."""
+
+    def __init__(self, rank):
+        self.rank = rank
+        self._p = np.full(17796, float(rank + 1), np.float32)
+        self.applied = []
+
+    @property
+    def params(self):
+        return self._p.copy()
+
+    @params.setter
+    def params(self, p):
+        self._p = np.asarray(p, np.float32).copy()
+
+    def grad_step(self, grad):
+        grad.fill_(float(self.rank + 1))
+        return 0.5 * (self.rank + 1)
+
+    def apply_gradient(self, grad, scale, lr):
+        self.applied.append((float(grad[0]) * scale, lr))
+
+
+def _dp_worker(rank, world, port, q):
+    import datetime
+    import torch
+    import torch.distributed as dist
+    from neuralsim_b200.surrogate import train_data_parallel
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        s = _FakeSurrogate(rank)
+        losses = train_data_parallel(s, 3, lr=1e-3, lr_final=1e-4, rank=rank, world=world,
+                                     grad=torch.zeros(17796))
+        q.put((rank, float(s.params[0]), s.applied, [float(x) for x in losses]))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_data_parallel_surrogate_training_gloo_world2():
+    # every rank applies the mean of the ranks' gradients, starting from
+    # rank 0's weights; the reported loss is the mean over ranks
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_dp_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = dict((r[0], r[1:]) for r in (q.get(timeout=120) for _ in procs))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for r in (0, 1):
+        p0, applied, losses = got[r]
+        assert p0 == 1.0                                   # broadcast from rank 0
+        assert [a for a, _ in applied] == [1.5, 1.5, 1.5]  # mean of 1 and 2
+        assert np.allclose(losses, 0.75)
+    assert got[0][1] == got[1][1]
