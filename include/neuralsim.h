@@ -268,6 +268,16 @@ ns_status ns_get_step(ns_handle* h, uint64_t* step);
 /* Per-neuron firing-rate estimate (engine.rs:637-642), FP64 on the device;
  * maintained only when homeostasis is enabled. */
 ns_status ns_download_rates(ns_handle* h, double* rates_out);
+/* Mean firing rate (Hz) of every network of the handle (n_nets entries; 1
+ * for a single network) over the logged steps first_step .. first_step +
+ * n_steps - 1, as the reference's per-neuron rate estimate averaged over a
+ * network's neurons reports it after those steps from rate 0
+ * (engine.rs:637-645: r += (1000/dt * spiked - r) * dt/100 each step). The
+ * fitness of Population::evolve_generation's RateHomeostasis evaluator
+ * (src/evolution/fitness.rs:59-76) is a function of it. Computed on the
+ * device from the spike log. */
+ns_status ns_network_rates(ns_handle* h, uint64_t first_step, uint32_t n_steps, double* mean_rate_out);
+
 /* Weight mean / std over all synapses (engine.rs:658-669), on demand. */
 ns_status ns_weight_stats(ns_handle* h, double* mean, double* stddev);
 

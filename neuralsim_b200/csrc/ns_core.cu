@@ -730,6 +730,34 @@ ns_status autotune_window(ns_handle* h, uint32_t budget, uint32_t* used) {
   return NS_OK;
 }
 
+// Per-(step, network) spike counts of a stretch of the spike log (integer
+// atomics: the result does not depend on their order).
+__global__ void k_net_counts(const uint32_t* log_idx, const unsigned long long* log_off, uint32_t n_steps,
+                             const uint32_t* net_of, uint32_t n_nets, uint32_t* counts) {
+  for (uint32_t s = blockIdx.x; s < n_steps; s += gridDim.x) {
+    const unsigned long long a = log_off[s], b = log_off[s + 1];
+    for (unsigned long long e = a + threadIdx.x; e < b; e += blockDim.x) {
+      const uint32_t q = net_of ? net_of[log_idx[e]] : 0u;
+      atomicAdd(&counts[(uint64_t)s * n_nets + q], 1u);
+    }
+  }
+}
+
+// Mean firing-rate EMA of every network (engine.rs:637-645: per neuron
+// r += (1000/dt * spiked - r) * dt/100 from r = 0, then the mean over the
+// network's neurons): each spike at step k of K contributes
+// 10 (1 - dt/100)^(K-1-k). Summed in step order, one thread per network.
+__global__ void k_net_rates(const uint32_t* counts, uint32_t n_steps, uint32_t n_nets,
+                            const unsigned long long* net_base, uint64_t n, double a, double* out) {
+  const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n_nets) return;
+  double r = 0.0;
+  for (uint32_t s = 0; s < n_steps; ++s)
+    r = r * (1.0 - a) + 10.0 * (double)counts[(uint64_t)s * n_nets + q];
+  const double nq = net_base ? (double)(net_base[q + 1] - net_base[q]) : (double)n;
+  out[q] = r / nq;
+}
+
 ns_status ready(ns_handle* h) {
   if (!h->have_neurons || !h->have_csr) return fail(h, NS_ERR_STATE, "upload neurons and CSR first");
   if (h->n == 0) return fail(h, NS_ERR_STATE, "empty network");
@@ -1621,6 +1649,41 @@ ns_status ns_upload_state(ns_handle* h, const ns_neuron_soa* in, const float* w_
   c.sim_time = (double)step * h->cfg.dt_ms;
   CK(cudaMemcpyAsync(h->ctl, &c, sizeof(c), cudaMemcpyHostToDevice, h->st));
   CK(cudaStreamSynchronize(h->st));
+  return NS_OK;
+}
+
+ns_status ns_network_rates(ns_handle* h, uint64_t first_step, uint32_t n_steps, double* mean_rate_out) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  if (!mean_rate_out || n_steps == 0) return fail(h, NS_ERR_INVALID_ARG, "null output or no steps");
+  if (!h->d.log_idx) return fail(h, NS_ERR_STATE, "spike log disabled (spike_log_capacity = 0)");
+  ns_status r = ready(h);
+  if (r) return r;
+  CK(cudaSetDevice(h->dev));
+  ns::Ctl c{};
+  CK(cudaMemcpyAsync(&c, h->ctl, sizeof(c), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  if (first_step < c.log_first || first_step + n_steps > c.log_first + c.log_steps)
+    return fail(h, NS_ERR_INVALID_ARG, "requested steps are not in the log");
+  const uint32_t nn = h->n_nets ? h->n_nets : 1u;
+  uint32_t* counts = nullptr;
+  double* out = nullptr;
+  cudaError_t e = cudaMalloc(&counts, (size_t)n_steps * nn * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&out, (size_t)nn * 8);
+  if (e == cudaSuccess) e = cudaMemsetAsync(counts, 0, (size_t)n_steps * nn * 4, h->st);
+  if (e == cudaSuccess) {
+    const uint64_t s0 = first_step - c.log_first;
+    k_net_counts<<<std::min<uint32_t>(n_steps, 4096u), 256, 0, h->st>>>(
+        h->d.log_idx, h->d.log_off + s0, n_steps, h->n_nets ? h->d.net_of : nullptr, nn, counts);
+    k_net_rates<<<(nn + 127) / 128, 128, 0, h->st>>>(counts, n_steps, nn,
+                                                      h->n_nets ? h->d.net_base : nullptr, h->n,
+                                                      h->cfg.dt_ms / 100.0, out);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(mean_rate_out, out, (size_t)nn * 8, cudaMemcpyDeviceToHost, h->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+  if (counts) cudaFree(counts);
+  if (out) cudaFree(out);
+  CK(e);
   return NS_OK;
 }
 

@@ -18,8 +18,15 @@ namespace ns {
 
 constexpr int kWinThreads = 256;   // neurons per segment (one block)
 
+// LIF and Izhikevich windows are throughput-bound on large batches: 64
+// registers keep 4 blocks resident per SM. The HH window is bound by one
+// long dependent chain per neuron; 3 blocks per SM hold a 100k-neuron
+// network in one wave.
+template <int MODEL>
+constexpr int window_min_blocks() { return MODEL == 2 ? 3 : 4; }
+
 template <int MODEL, int MODE>
-__global__ void __launch_bounds__(kWinThreads) k_window(NsDev d, uint32_t j0, uint32_t W) {
+__global__ void __launch_bounds__(kWinThreads, window_min_blocks<MODEL>()) k_window(NsDev d, uint32_t j0, uint32_t W) {
   __shared__ uint32_t s_wcnt[kWinThreads / 32];
   __shared__ Kick s_kick[32];
   __shared__ int s_nk;

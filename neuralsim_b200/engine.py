@@ -335,6 +335,15 @@ class SimulationEngine:
         self._check(self.lib.ns_get_window(self._h, C.byref(w), _ptr(cand), _ptr(us)))
         return int(w.value), {int(c): float(t) for c, t in zip(cand, us) if c}
 
+    def network_rates(self, first_step, n_steps):
+        """Mean firing rate (Hz) of every network of the handle after the
+        logged steps, as the reference's per-neuron rate estimate averaged
+        over a network reports it (src/simulation/engine.rs:637-645)."""
+        n = len(getattr(self, "networks", [None]))
+        out = np.zeros(n, np.float64)
+        self._check(self.lib.ns_network_rates(self._h, int(first_step), int(n_steps), _ptr(out)))
+        return out
+
     # -- learned HH macro-step (include/neuralsim_surrogate.h) --
     def attach_surrogate(self, sur, v_lo=-85.0, v_hi=-52.0, residual_mv=0.5):
         """Advance in-envelope neurons with the trained surrogate `sur`

@@ -111,3 +111,35 @@ def test_c3_full_size_batch_runs(lib):
     out = b.run(steps)
     assert out.steps_done == steps
     b.close()
+
+
+def _rates_from_raster(raster, n, steps, dt):
+    # the reference's per-neuron estimate (engine.rs:637-645) from rate 0,
+    # averaged over the network
+    idx, off = raster
+    cnt = np.diff(np.asarray(off, np.int64))
+    a = dt / 100.0
+    r = 0.0
+    for s in range(steps):
+        r = r * (1.0 - a) + 10.0 * cnt[s]
+    return r / n
+
+
+def test_network_rates_and_population_fitness(lib):
+    from neuralsim_b200.population import RateHomeostasis, evaluate_batch
+    nets, seeds, cfg, drive = lif_batch(n_nets=5)
+    steps = 400
+    b = BatchEngine(nets, seeds, cfg, drive)
+    b.run(steps)
+    rates = b.network_rates(0, steps)
+    parts = b.read_rasters(0, steps)
+    for q, net in enumerate(nets):
+        want = _rates_from_raster(parts[q], net.n, steps, cfg.dt_ms)
+        assert abs(rates[q] - want) <= 1e-12 * max(1.0, abs(want))
+    assert rates.max() > 1.0
+    b.close()
+    # a lifetime of 400 steps of 0.1 ms: the population evaluation's fitness
+    ev = RateHomeostasis(target_rate=20.0, lifetime_ms=steps * cfg.dt_ms)
+    fit, r2 = evaluate_batch(nets, seeds, cfg, drive, ev)
+    assert np.allclose(r2, rates, rtol=1e-12, atol=0)
+    assert np.allclose(fit, ev.fitness(rates), rtol=0, atol=0)

@@ -161,3 +161,19 @@ def test_data_parallel_surrogate_training_gloo_world2():
         assert [a for a, _ in applied] == [1.5, 1.5, 1.5]  # mean of 1 and 2
         assert np.allclose(losses, 0.75)
     assert got[0][1] == got[1][1]
+
+
+def test_rate_homeostasis_fitness_matches_reference_formula():
+    # src/evolution/fitness.rs:59-76
+    from neuralsim_b200.population import RateHomeostasis
+    ev = RateHomeostasis(target_rate=5.0)
+    r = np.array([0.0, 0.5, 1.0, 5.0, 7.5, 499.0, 501.0])
+    want = []
+    for x in r:
+        f = 1.0 / (1.0 + abs(x - 5.0))
+        if x < 1.0:
+            f *= 0.1
+        if x > 500.0:
+            f *= 0.1
+        want.append(f)
+    assert np.allclose(ev.fitness(r), want, rtol=0, atol=1e-15)
