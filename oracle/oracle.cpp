@@ -1159,6 +1159,34 @@ void or_lit_state(void* s, double* v, double* u, double* m, double* h, double* n
     if (I) I[i] = L->I[i];
   }
 }
+// Warm start (timing samples only): neuron state, per-neuron STDP traces
+// and last spike times (each plastic synapse takes its source's pre-trace
+// and its target's post-trace, the per-neuron reformulation), weights, the
+// clock and the step count. Pending delayed input starts empty.
+void or_lit_set_state(void* s, const double* v, const double* u, const double* pre,
+                      const double* post, const double* last_spike_time, const double* w,
+                      double time, uint64_t step) {
+  Lit* L = (Lit*)s;
+  for (uint64_t i = 0; i < L->n; ++i) {
+    if (v) L->v[i] = v[i];
+    if (u) L->u[i] = u[i];
+    if (last_spike_time) L->last_spike_time[i] = last_spike_time[i];
+  }
+  for (uint64_t q = 0; q < L->m; ++q) {
+    LitSyn& y = L->syn[q];
+    if (w) y.weight = w[q];
+    if (pre) y.pre_trace = pre[y.source];
+    if (post) y.post_trace = post[y.target];
+    if (last_spike_time) {
+      y.last_pre = last_spike_time[y.source];
+      y.last_post = last_spike_time[y.target];
+    }
+  }
+  std::fill(L->ring.begin(), L->ring.end(), 0.0);
+  L->time = time;
+  L->step = step;
+}
+
 void or_lit_weights(void* s, double* w) {
   Lit* L = (Lit*)s;
   for (uint64_t q = 0; q < L->m; ++q) w[q] = L->syn[q].weight;

@@ -124,6 +124,9 @@ uint64_t or_lit_log_size(void* s);
 uint64_t or_lit_log_steps(void* s);
 void or_lit_log(void* s, uint32_t* idx, uint64_t* offsets);
 void or_lit_state(void* s, double* v, double* u, double* m, double* h, double* n, double* I);
+void or_lit_set_state(void* s, const double* v, const double* u, const double* pre,
+                      const double* post, const double* last_spike_time, const double* w,
+                      double time, uint64_t step);
 void or_lit_weights(void* s, double* w);
 void or_lit_rates(void* s, double* rates);
 uint64_t or_lit_events(void* s);

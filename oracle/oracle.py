@@ -92,6 +92,7 @@ def load():
         "or_lit_log": (None, [vp, vp, vp]),
         "or_lit_state": (None, [vp] * 7),
         "or_lit_weights": (None, [vp, vp]),
+        "or_lit_set_state": (None, [vp, vp, vp, vp, vp, vp, vp, C.c_double, u64]),
         "or_lit_rates": (None, [vp, vp]),
         "or_lit_events": (u64, [vp]),
         "or_lit_stats": (None, [vp, vp]),
@@ -235,6 +236,14 @@ class LiteralOracle(_Base):
         self.L.or_lit_state(self.h, _p(out["v"]), _p(out["u"]), _p(out["m"]), _p(out["h"]),
                             _p(out["n"]), _p(out["I"]))
         return out
+
+    def set_state(self, v, u, pre, post, last_spike_time, w, time, step):
+        """Warm start for timing samples: neuron state, per-neuron traces and
+        last spike times (ms), weights, clock (ms) and step count."""
+        f = lambda a: None if a is None else np.ascontiguousarray(a, np.float64)
+        arrs = [f(x) for x in (v, u, pre, post, last_spike_time, w)]
+        self._keep = arrs
+        self.L.or_lit_set_state(self.h, *[_p(a) for a in arrs], float(time), int(step))
 
     def stats(self):
         o = np.zeros(8)
