@@ -23,7 +23,7 @@ constexpr int kWinThreads = 256;   // neurons per segment (one block)
 // long dependent chain per neuron; 3 blocks per SM hold a 100k-neuron
 // network in one wave.
 template <int MODEL>
-constexpr int window_min_blocks() { return MODEL == 2 ? 3 : 4; }
+__host__ __device__ constexpr int window_min_blocks() { return MODEL == 2 ? 3 : 4; }
 
 template <int MODEL, int MODE>
 __global__ void __launch_bounds__(kWinThreads, window_min_blocks<MODEL>()) k_window(NsDev d, uint32_t j0, uint32_t W) {
@@ -65,6 +65,7 @@ __global__ void __launch_bounds__(kWinThreads, window_min_blocks<MODEL>()) k_win
   const uint64_t words = d.n_pad >> 5;
   unsigned long long my_spk = 0;
   uint32_t slot = (uint32_t)(k0 % d.D);   // advanced by one (mod D) per step
+  uint32_t pref = 0;                       // lane l: input word of step (s & ~31) + l
   for (uint32_t s = 0; s < W; ++s, slot = (slot + 1u == d.D) ? 0u : slot + 1u) {
     const uint64_t k = k0 + s;
     int nk = 0;
@@ -88,12 +89,19 @@ __global__ void __launch_bounds__(kWinThreads, window_min_blocks<MODEL>()) k_win
       __syncthreads();
       nk = s_nk;
     }
-    // delivered input: read (and clear) the slot only when its bit is set
-    uint32_t* wp = d.inbits + (uint64_t)slot * words + (i >> 5);
-    uint32_t word = 0;
-    if (lane == 0) word = *wp;
-    word = __shfl_sync(0xffffffffu, word, 0);
-    if (lane == 0 && word) *wp = 0u;
+    // delivered input: the warp's "has input" words of the window are final
+    // before it starts (delay >= window), so lane l fetches (and clears) the
+    // word of step s + l once per 32 steps, off the per-step chain
+    if ((s & 31u) == 0) {
+      pref = 0u;
+      if (s + lane < W) {
+        const uint32_t sl = (slot + lane) % d.D;
+        uint32_t* wp = d.inbits + (uint64_t)sl * words + (i >> 5);
+        pref = *wp;
+        if (pref) *wp = 0u;
+      }
+    }
+    const uint32_t word = __shfl_sync(0xffffffffu, pref, s & 31u);
     float S[NT];
 #pragma unroll
     for (int t = 0; t < NT; ++t) S[t] = 0.f;
