@@ -149,11 +149,36 @@ typedef struct ns_config {
    * and its successive halves down to 2 (ns_get_window), 1 = off (one pass
    * per step), W > 1 = on with that W. Results are identical either way. */
   uint32_t window_steps;
+  /* R-STDP (RStdpRule / EligibilityTrace, src/synapse/plasticity.rs:166-221).
+   * A synapse that carries an eligibility trace updates it at each of its
+   * STDP updates: e = e*exp(-dt/eligibility_tau) + delta, delta being the
+   * unclamped weight change (engine.rs:519-533, where the engine passes 200
+   * ms). While |reward| > 0.001 at a step, every such synapse takes
+   * w = clamp(w + rstdp_lr*reward*e, rstdp_w_min, rstdp_w_max) and e = 0
+   * after the step's STDP and consolidation (engine.rs:546-561). The reward
+   * decays by reward_decay per step whenever any plasticity is on
+   * (engine.rs:563) and becomes min(reward + 1, 1) after a step with at
+   * least reward_threshold output spikes (engine.rs:626-631); reward_signal
+   * is its value before the first step (with_reward_signal, :151-154). */
+  int32_t rstdp_enabled;
+  double rstdp_lr, rstdp_w_min, rstdp_w_max, eligibility_tau;
+  uint64_t reward_threshold;
+  double reward_decay, reward_signal;
+  /* Consolidation (ConsolidationRule, plasticity.rs:269-290), applied to
+   * every synapse after STDP each step (engine.rs:539-545):
+   * w += (consolidation_target - w) * dt / consolidation_tau * consolidation_drift.
+   * The device keeps this O(1) per step: weights are stored in a per-step
+   * affine frame (see ns_download_state for the plain values). */
+  int32_t consolidation_enabled;
+  double consolidation_tau, consolidation_target, consolidation_drift;
 } ns_config;
 
 /* Fills cfg with the reference defaults: LIF, DIRECT_DECAY, dt 0.5 ms
  * (engine.rs:96), decay 0.92, StdpRule::default, homeostasis 5 Hz / 5000 ms,
- * contribution_tau 1000 ms, seed 42 (engine.rs:99). */
+ * contribution_tau 1000 ms, seed 42 (engine.rs:99); R-STDP and consolidation
+ * off with RStdpRule::default / ConsolidationRule::default parameters
+ * (plasticity.rs:177-189, :276-284), eligibility tau 200 ms, reward
+ * threshold 5 and decay 0.95 (engine.rs:113-116). */
 void ns_config_default(ns_config* cfg);
 
 /* Neuron SoA (NeuronArray, src/neuron/mod.rs:126-163, in f32 as init_gpu
@@ -280,6 +305,37 @@ ns_status ns_network_rates(ns_handle* h, uint64_t first_step, uint32_t n_steps, 
 
 /* Weight mean / std over all synapses (engine.rs:658-669), on demand. */
 ns_status ns_weight_stats(ns_handle* h, double* mean, double* stddev);
+
+/* --- the rest of phase 2: R-STDP eligibility and reward, short-term
+ *     plasticity (engine.rs:457-463, :519-563, :626-631) ---------------- */
+/* Which synapses carry an eligibility trace (SynapseState.eligibility is
+ * Some, src/synapse/mod.rs:72, set by with_rstdp, :114-119) and its values,
+ * CSR order. eligible NULL = every plastic synapse; values NULL = 0. Needs
+ * rstdp_enabled; ns_upload_csr resets to (every plastic synapse, 0). */
+ns_status ns_upload_eligibility(ns_handle* h, const uint8_t* eligible, const float* values);
+/* Current eligibility values (m floats; 0 for synapses without a trace). */
+ns_status ns_download_eligibility(ns_handle* h, float* values_out);
+/* SimulationEngine::apply_reward (engine.rs:158-175): every eligible synapse
+ * takes w = clamp(w + rstdp_lr*reward*e, rstdp_w_min, rstdp_w_max), e = 0,
+ * now, whatever the size of reward. */
+ns_status ns_apply_reward(ns_handle* h, double reward);
+/* The engine's reward_signal now (after the last step's phase 3), and the
+ * sum over the steps since creation / the last ns_set_reward of the reward
+ * after each step (RewardAccumulation's fitness, evolution/fitness.rs:110-118).
+ * Maintained by the step-synchronous path when R-STDP or consolidation is
+ * on; NS_ERR_UNSUPPORTED otherwise, after windowed steps and for batches. */
+ns_status ns_get_reward(ns_handle* h, double* reward, double* reward_sum);
+/* Sets reward_signal (with_reward_signal) and clears the sum. */
+ns_status ns_set_reward(ns_handle* h, double reward);
+/* Short-term plasticity (Tsodyks-Markram ShortTermPlasticity,
+ * plasticity.rs:85-116). In the current modes the reference scales each
+ * delivered weight by the EPSP of one step of a COPY of the synapse's STP
+ * state (engine.rs:457-463); the copy is dropped, so the factor
+ * (u + u_se*(1-u)/tau_facil*dt) * r is a per-synapse constant, taken in
+ * every non-conductance input mode (conductance mode ignores STP, as the
+ * reference does). stp: m rows (u_se, tau_rec, tau_facil, u, r), CSR order;
+ * has_stp NULL = every synapse has STP. stp NULL removes STP. */
+ns_status ns_upload_stp(ns_handle* h, const uint8_t* has_stp, const double* stp);
 
 /* --- traversal trace: runs ONE step and records the CSR position of every
  *     propagation event in traversal order (spikers ascending, each row in

@@ -39,6 +39,12 @@ class NsConfig(C.Structure):
         ("contribution_tau", C.c_double), ("spike_log_capacity", C.c_uint64),
         ("spike_log_steps", C.c_uint32), ("graph_chunk", C.c_uint32),
         ("step_schedule", C.c_uint32), ("window_steps", C.c_uint32),
+        ("rstdp_enabled", C.c_int32), ("rstdp_lr", C.c_double), ("rstdp_w_min", C.c_double),
+        ("rstdp_w_max", C.c_double), ("eligibility_tau", C.c_double),
+        ("reward_threshold", C.c_uint64), ("reward_decay", C.c_double),
+        ("reward_signal", C.c_double), ("consolidation_enabled", C.c_int32),
+        ("consolidation_tau", C.c_double), ("consolidation_target", C.c_double),
+        ("consolidation_drift", C.c_double),
     ]
 
 
@@ -121,6 +127,12 @@ SIGNATURES = {
     "ns_get_step": (C.c_int32, [_P, _U64P]),
     "ns_download_rates": (C.c_int32, [_P, _P]),
     "ns_weight_stats": (C.c_int32, [_P, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "ns_upload_eligibility": (C.c_int32, [_P, C.c_void_p, C.c_void_p]),
+    "ns_download_eligibility": (C.c_int32, [_P, C.c_void_p]),
+    "ns_apply_reward": (C.c_int32, [_P, C.c_double]),
+    "ns_get_reward": (C.c_int32, [_P, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "ns_set_reward": (C.c_int32, [_P, C.c_double]),
+    "ns_upload_stp": (C.c_int32, [_P, C.c_void_p, C.c_void_p]),
     "ns_step_traced": (C.c_int32, [_P, _P, C.c_uint64, _U64P]),
     "ns_launch_count": (C.c_int32, [_P, _U64P]),
     "ns_get_schedule": (C.c_int32, [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_double)]),

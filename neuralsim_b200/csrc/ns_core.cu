@@ -63,6 +63,10 @@ struct ns_handle {
   uint32_t* fb_list = nullptr;      // [n_pad] neurons handed over in a window
   uint32_t* fb_count = nullptr;     // their number
   std::vector<void*> sur_allocs;
+  // R-STDP eligibility and short-term plasticity arrays
+  std::vector<void*> ext_allocs;    // elig + elig_flag (R-STDP)
+  std::vector<void*> stp_allocs;    // stp_f
+  bool win_ran = false;             // windowed steps ran (reward not maintained)
 };
 
 namespace {
@@ -126,10 +130,12 @@ cudaError_t snapshot_take(ns_handle* h, Snapshot& sn) {
   add(h->d.acc);
   add(h->d.contrib);
   add(h->d.inbits);
-  if (h->cfg.stdp_enabled || h->cfg.homeostasis_enabled) {
+  if (h->cfg.stdp_enabled || h->cfg.homeostasis_enabled || h->cfg.rstdp_enabled ||
+      h->cfg.consolidation_enabled) {
     add(h->d.w16);
     add(h->d.w32);
   }
+  add(h->d.elig);
   sn.regions.push_back({h->ctl, sizeof(ns::Ctl)});
   for (auto& r : sn.regions) {
     void* c = nullptr;
@@ -262,15 +268,58 @@ __global__ void k_in_list(const uint32_t* pos, uint64_t cnt, const uint64_t* rp,
 }
 
 __global__ void k_weight_sum(const float* w32, const uint16_t* w16, uint64_t m, double mean,
-                             int pass, double* out) {
+                             int pass, int cons, float A, float B, double* out) {
   double acc = 0.0;
   for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < m;
        e += (uint64_t)gridDim.x * blockDim.x) {
-    double x = w16 ? (double)ns::bf16_bits_to_f32(w16[e]) : (double)w32[e];
+    float u = w16 ? ns::bf16_bits_to_f32(w16[e]) : w32[e];
+    if (cons) u = u * A + B;  // plain weight of the consolidation frame
+    double x = (double)u;
     acc += pass == 0 ? x : (x - mean) * (x - mean);
   }
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
   if ((threadIdx.x & 31) == 0) atomicAdd(out, acc);
+}
+
+// Eligibility flags from the plastic flags: every plastic synapse carries a
+// trace (with_rstdp, src/synapse/mod.rs:114-119). One thread per row.
+__global__ void k_elig_from_plastic(const uint64_t* rp, uint64_t n, const uint8_t* row_plastic,
+                                    const uint8_t* plastic, uint8_t* flag) {
+  for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < n;
+       j += (uint64_t)gridDim.x * blockDim.x) {
+    const uint8_t r = row_plastic[j];
+    for (uint64_t e = rp[j]; e < rp[j + 1]; ++e)
+      flag[e] = r == 1 ? 1 : (r == 2 && plastic ? (plastic[e] ? 1 : 0) : 0);
+  }
+}
+
+// SimulationEngine::apply_reward (engine.rs:158-175) between steps, in the
+// consolidation frame (A, B, 1/A) of the next step; only weights the reward
+// moves are written.
+template <bool BF16>
+__global__ void k_apply_reward(NsDev d, float lrr, int cons, float A, float B, float iA) {
+  for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < d.m;
+       s += (uint64_t)gridDim.x * blockDim.x) {
+    if (!d.elig_flag[s]) continue;
+    float x = BF16 ? ns::bf16_bits_to_f32(d.w16[s]) : d.w32[s];
+    if (cons) x = x * A + B;
+    const float ev = d.elig[s];
+    if (!(ev != 0.0f || x < d.rw_min || x > d.rw_max)) continue;
+    x = ns::clampw(x + lrr * ev, d.rw_min, d.rw_max);
+    d.elig[s] = 0.0f;
+    if (cons) x = (x - B) * iA;
+    if (BF16) d.w16[s] = ns::f32_to_bf16_bits(x);
+    else d.w32[s] = x;
+  }
+}
+
+// Stored values to plain weights (w = u*A + B), in place.
+__global__ void k_weights_to_plain(float* w32, uint16_t* w16, uint64_t m, float A, float B) {
+  for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < m;
+       e += (uint64_t)gridDim.x * blockDim.x) {
+    if (w16) w16[e] = ns::f32_to_bf16_bits(ns::bf16_bits_to_f32(w16[e]) * A + B);
+    else w32[e] = w32[e] * A + B;
+  }
 }
 
 // Builds an incoming index sorted by (target, CSR position): deterministic.
@@ -365,6 +414,15 @@ std::vector<float> trace_table(double tau, double dt) {
   return t;
 }
 
+// per-step consolidation factor a = 1 - dt*drift/tau (plasticity.rs:286-289)
+double cons_a_of(const ns_config& c) {
+  return c.consolidation_enabled ? 1.0 - (c.dt_ms / c.consolidation_tau) * c.consolidation_drift : 1.0;
+}
+// the reward decays whenever some plasticity is on (engine.rs:496-563)
+bool plast_any_of(const ns_config& c) {
+  return c.stdp_enabled || c.homeostasis_enabled || c.rstdp_enabled || c.consolidation_enabled;
+}
+
 void fill_scalars(ns_handle* h) {
   NsDev& d = h->d;
   const ns_config& c = h->cfg;
@@ -395,6 +453,66 @@ void fill_scalars(ns_handle* h) {
   d.kick_min = h->drive.kick_min; d.kick_max = h->drive.kick_max;
   d.p_thr = prob_threshold((double)h->drive.p);
   d.ctl = h->ctl;
+  d.rstdp = c.rstdp_enabled ? 1 : 0;
+  d.cons = c.consolidation_enabled ? 1 : 0;
+  d.plast_any = plast_any_of(c) ? 1 : 0;
+  d.ce = (float)std::exp(-c.dt_ms / c.eligibility_tau);
+  d.rw_min = (float)c.rstdp_w_min; d.rw_max = (float)c.rstdp_w_max;
+  d.reward_decay = c.reward_decay;
+  d.rstdp_lr = c.rstdp_lr;
+  d.reward_thr = c.reward_threshold;
+  d.cons_a = cons_a_of(c);
+  d.cons_T = c.consolidation_target;
+  // the walks may apply the reward (mode 1) when no rule can move an
+  // eligible weight out of [rstdp_w_min, rstdp_w_max] between rewarded steps
+  d.fuse = ((!c.stdp_enabled || (c.rstdp_w_min <= c.w_min && c.w_max <= c.rstdp_w_max)) &&
+            (!c.homeostasis_enabled || (c.rstdp_w_min <= 0.0 && 10.0 <= c.rstdp_w_max)) &&
+            (!c.consolidation_enabled ||
+             (c.rstdp_w_min <= c.consolidation_target && c.consolidation_target <= c.rstdp_w_max)))
+               ? 1 : 0;
+}
+
+// R-STDP / consolidation / short-term plasticity need the EXT walk variants
+bool ext_on(const ns_handle* h) {
+  return h->cfg.rstdp_enabled || h->cfg.consolidation_enabled || h->d.stp_f != nullptr;
+}
+bool tail_on(const ns_handle* h) { return h->cfg.rstdp_enabled || h->cfg.consolidation_enabled; }
+
+// reward after the last step (phase 3 of engine.rs:626-631), from the
+// control block as the next step's setup computes it
+double reward_now(const ns_handle* h, const ns::Ctl& c) {
+  const uint64_t K = c.step_base;
+  if (K == c.origin) return c.rew_init;
+  const double Rp = c.rew[(K - 1) & 1];
+  const double Rd = plast_any_of(h->cfg) ? Rp * h->cfg.reward_decay : Rp;
+  return (c.outs[(K - 1) & 3] >= h->cfg.reward_threshold) ? std::fmin(Rd + 1.0, 1.0) : Rd;
+}
+
+// consolidation frame of the next step: A, B = target*(1 - A), 1/A
+void frame_now(const ns_handle* h, const ns::Ctl& c, float f[3]) {
+  double A = 1.0;
+  if (h->cfg.consolidation_enabled && c.step_base != c.cons_k0)
+    A = c.consA[(c.step_base - 1) & 1] * cons_a_of(h->cfg);
+  f[0] = (float)A;
+  f[1] = (float)(h->cfg.consolidation_target * (1.0 - A));
+  f[2] = (float)(1.0 / A);
+}
+
+// Sets the reward origin (reward value and eligibility state at step
+// `origin`), the reward sum and the step whose consolidation frame is the
+// identity.
+cudaError_t set_ext_ctl(ns_handle* h, uint64_t origin, double rew, unsigned ezero, double sum,
+                        uint64_t cons_k0) {
+  auto put = [&](size_t off, const void* src, size_t bytes) {
+    return cudaMemcpyAsync((char*)h->ctl + off, src, bytes, cudaMemcpyHostToDevice, h->st);
+  };
+  cudaError_t e = put(offsetof(ns::Ctl, origin), &origin, 8);
+  if (e == cudaSuccess) e = put(offsetof(ns::Ctl, rew_init), &rew, 8);
+  if (e == cudaSuccess) e = put(offsetof(ns::Ctl, ezero_init), &ezero, 4);
+  if (e == cudaSuccess) e = put(offsetof(ns::Ctl, reward_sum), &sum, 8);
+  if (e == cudaSuccess) e = put(offsetof(ns::Ctl, cons_k0), &cons_k0, 8);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+  return e;
 }
 
 typedef void (*neuron_fn)(NsDev, uint32_t);
@@ -410,25 +528,40 @@ neuron_fn pick_neuron(uint32_t model, uint32_t mode) {
   return nullptr;
 }
 
-prop_fn pick_prop(uint32_t mode, uint32_t wf) {
+// EXT variants carry R-STDP eligibility, the consolidation frame and STP
+prop_fn pick_prop(uint32_t mode, uint32_t wf, bool ext) {
   bool cond = mode == NS_INPUT_CONDUCTANCE_REF || mode == NS_INPUT_CONDUCTANCE_FRESH;
   bool bf = wf == NS_WEIGHT_BF16;
-  if (cond) return bf ? ns::k_rows<true, true> : ns::k_rows<true, false>;
-  return bf ? ns::k_rows<false, true> : ns::k_rows<false, false>;
+#define NSR(C, B) (ext ? ns::k_rows<C, B, true> : ns::k_rows<C, B, false>)
+  if (cond) return bf ? NSR(true, true) : NSR(true, false);
+  return bf ? NSR(false, true) : NSR(false, false);
+#undef NSR
 }
 
-ltd_fn pick_ltd(uint32_t wf) { return wf == NS_WEIGHT_BF16 ? ns::k_ltd<true> : ns::k_ltd<false>; }
+ltd_fn pick_ltd(uint32_t wf, bool ext) {
+  if (wf == NS_WEIGHT_BF16) return ext ? ns::k_ltd<true, true> : ns::k_ltd<true, false>;
+  return ext ? ns::k_ltd<false, true> : ns::k_ltd<false, false>;
+}
 
 // fused kernel at 6 (schedule 1) or 4 (schedule 3) resident blocks per SM
-prop_fn pick_fused(uint32_t mode, uint32_t wf, uint32_t sched) {
+prop_fn pick_fused(uint32_t mode, uint32_t wf, uint32_t sched, bool ext) {
   bool cond = mode == NS_INPUT_CONDUCTANCE_REF || mode == NS_INPUT_CONDUCTANCE_FRESH;
   bool bf = wf == NS_WEIGHT_BF16;
+#define NSF(C, B, M) (ext ? ns::k_prop_fused<C, B, M, true> : ns::k_prop_fused<C, B, M, false>)
   if (sched == 3) {
-    if (cond) return bf ? ns::k_prop_fused<true, true, 4> : ns::k_prop_fused<true, false, 4>;
-    return bf ? ns::k_prop_fused<false, true, 4> : ns::k_prop_fused<false, false, 4>;
+    if (cond) return bf ? NSF(true, true, 4) : NSF(true, false, 4);
+    return bf ? NSF(false, true, 4) : NSF(false, false, 4);
   }
-  if (cond) return bf ? ns::k_prop_fused<true, true, 6> : ns::k_prop_fused<true, false, 6>;
-  return bf ? ns::k_prop_fused<false, true, 6> : ns::k_prop_fused<false, false, 6>;
+  if (cond) return bf ? NSF(true, true, 6) : NSF(true, false, 6);
+  return bf ? NSF(false, true, 6) : NSF(false, false, 6);
+#undef NSF
+}
+
+void launch_tail(ns_handle* h, const NsDev& d, uint32_t j, cudaStream_t s) {
+  if (h->cfg.weight_format == NS_WEIGHT_BF16)
+    ns::k_tail<true><<<h->sms * 8, 256, 0, s>>>(d, j);
+  else
+    ns::k_tail<false><<<h->sms * 8, 256, 0, s>>>(d, j);
 }
 
 void launch_homeo(ns_handle* h, const NsDev& d, uint32_t j, cudaStream_t s) {
@@ -441,7 +574,9 @@ void launch_homeo(ns_handle* h, const NsDev& d, uint32_t j, cudaStream_t s) {
 // Split schedule: LTD of step k overlaps the neuron kernel of step k+1 when
 // nothing in between reads the weights (homeostasis rescales them, so it
 // serialises).
-bool overlap_ltd(const ns_handle* h) { return h->cfg.stdp_enabled && !h->cfg.homeostasis_enabled; }
+bool overlap_ltd(const ns_handle* h) {
+  return h->cfg.stdp_enabled && !h->cfg.homeostasis_enabled && !tail_on(h);
+}
 
 // schedule a step uses (fused at 6 blocks/SM until the autotuner decides)
 uint32_t sched_of(const ns_handle* h) { return h->sched == 0 ? 1u : h->sched; }
@@ -457,13 +592,15 @@ cudaError_t enqueue_step(ns_handle* h, uint32_t j, bool* ltd_pending, uint32_t s
     if (e != cudaSuccess) return e;
     *ltd_pending = false;
   }
+  const bool ext = ext_on(h);
+  if (tail_on(h)) ns::k_setup<<<1, 32, 0, h->st>>>(h->d, j);
   if (sched == 1 || sched == 3) {
-    pick_fused(h->cfg.input_mode, h->cfg.weight_format, sched)
+    pick_fused(h->cfg.input_mode, h->cfg.weight_format, sched, ext)
         <<<h->fused_blocks[sched == 3 ? 1 : 0], 256, 0, h->st>>>(h->d, j);
   } else {
-    pick_prop(h->cfg.input_mode, h->cfg.weight_format)<<<h->prop_blocks, 256, 0, h->st>>>(h->d, j);
+    pick_prop(h->cfg.input_mode, h->cfg.weight_format, ext)<<<h->prop_blocks, 256, 0, h->st>>>(h->d, j);
     if (h->cfg.stdp_enabled) {
-      ltd_fn lf = pick_ltd(h->cfg.weight_format);
+      ltd_fn lf = pick_ltd(h->cfg.weight_format, ext);
       if (overlap_ltd(h)) {
         cudaError_t e = cudaEventRecord(h->ev_rows, h->st);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(h->st2, h->ev_rows, 0);
@@ -477,6 +614,7 @@ cudaError_t enqueue_step(ns_handle* h, uint32_t j, bool* ltd_pending, uint32_t s
       }
     }
   }
+  if (tail_on(h)) launch_tail(h, h->d, j, h->st);
   if (h->cfg.homeostasis_enabled) launch_homeo(h, h->d, j, h->st);
   return cudaGetLastError();
 }
@@ -489,7 +627,8 @@ cudaError_t join_ltd(ns_handle* h, bool* ltd_pending) {
 
 uint64_t launches_per_step(const ns_handle* h, uint32_t sched) {
   const bool split = sched == 2 || sched == 4;
-  return 2u + ((split && h->cfg.stdp_enabled) ? 1u : 0u) + (h->cfg.homeostasis_enabled ? 1u : 0u);
+  return 2u + ((split && h->cfg.stdp_enabled) ? 1u : 0u) + (h->cfg.homeostasis_enabled ? 1u : 0u) +
+         (tail_on(h) ? 2u : 0u);
 }
 
 typedef void (*window_fn)(NsDev, uint32_t, uint32_t);
@@ -513,6 +652,7 @@ window_fn pick_window_rows(uint32_t mode, uint32_t wf) {
 // Window length the handle's configuration allows (0 = step-synchronous).
 uint32_t window_len(const ns_config& c) {
   if (c.stdp_enabled || c.homeostasis_enabled || c.delay_steps < 2 || c.window_steps == 1) return 0;
+  if (c.rstdp_enabled || c.consolidation_enabled) return 0;
   if (c.input_mode == NS_INPUT_CONDUCTANCE_REF) return 0;
   uint32_t w = c.window_steps > 1 ? std::min(c.window_steps, c.delay_steps) : c.delay_steps;
   return std::min<uint32_t>(w, 1024u);
@@ -575,6 +715,7 @@ ns_status get_graph(ns_handle* h, uint32_t S, uint32_t sched, cudaGraphExec_t* o
 // remainder. Enqueues only.
 ns_status run_steps(ns_handle* h, uint32_t n, uint32_t sched) {
   const uint32_t S = h->cfg.graph_chunk;
+  if (h->win && n) h->win_ran = true;
   uint32_t left = n;
   if (left >= S) {
     cudaGraphExec_t ex;
@@ -693,6 +834,7 @@ ns_status autotune_window(ns_handle* h, uint32_t budget, uint32_t* used) {
   if (nc < 2 || budget < T) return NS_OK;
   Snapshot sn;
   CK(snapshot_take(h, sn));
+  h->win_ran = true;
   cudaEvent_t e0, e1;
   cudaError_t ce = cudaEventCreate(&e0);
   if (ce == cudaSuccess) ce = cudaEventCreate(&e1);
@@ -763,6 +905,8 @@ ns_status ready(ns_handle* h) {
   if (h->n == 0) return fail(h, NS_ERR_STATE, "empty network");
   if (h->sur_on && h->drive.kind != NS_DRIVE_NONE && h->drive.kind != NS_DRIVE_POISSON_CONDUCTANCE)
     return fail(h, NS_ERR_UNSUPPORTED, "the surrogate macro-step takes no drive or the Poisson conductance drive");
+  if (h->n_nets && h->cfg.rstdp_enabled)
+    return fail(h, NS_ERR_UNSUPPORTED, "R-STDP's reward is global to one network; batches do not take it");
   if (h->n_nets && h->drive.kind == NS_DRIVE_REF_UNIFORM)
     return fail(h, NS_ERR_UNSUPPORTED, "the reference-uniform drive's kicks are global to one network; batches take per-neuron drives");
   return NS_OK;
@@ -795,6 +939,17 @@ void ns_config_default(ns_config* c) {
   c->spike_log_capacity = 0;
   c->spike_log_steps = 0;
   c->graph_chunk = 1000;
+  c->rstdp_enabled = 0;     // RStdpRule::default, plasticity.rs:177-189
+  c->rstdp_lr = 0.1;
+  c->rstdp_w_min = 0.0; c->rstdp_w_max = 10.0;
+  c->eligibility_tau = 200.0;  // engine.rs:521, :532
+  c->reward_threshold = 5;     // engine.rs:115
+  c->reward_decay = 0.95;      // engine.rs:116
+  c->reward_signal = 0.0;
+  c->consolidation_enabled = 0;  // ConsolidationRule::default, plasticity.rs:276-284
+  c->consolidation_tau = 10000.0;
+  c->consolidation_target = 0.5;
+  c->consolidation_drift = 0.001;
 }
 
 const char* ns_status_string(ns_status s) {
@@ -842,6 +997,14 @@ ns_status ns_create(const ns_config* cfg, ns_handle** out) {
     return fail(h, NS_ERR_INVALID_ARG, "bad STDP parameters");
   if (c.homeostasis_enabled && (!(c.homeostatic_tau > 0) || !(c.contribution_tau > 0)))
     return fail(h, NS_ERR_INVALID_ARG, "bad homeostasis parameters");
+  if (c.rstdp_enabled && (!(c.eligibility_tau > 0) || !is_fin(c.rstdp_lr) || !(c.rstdp_w_min <= c.rstdp_w_max) ||
+                          !is_fin(c.reward_decay) || !is_fin(c.reward_signal)))
+    return fail(h, NS_ERR_INVALID_ARG, "bad R-STDP parameters");
+  if (c.consolidation_enabled &&
+      (!(c.consolidation_tau > 0) || !is_fin(c.consolidation_target) || !is_fin(c.consolidation_drift) ||
+       !(c.dt_ms / c.consolidation_tau * c.consolidation_drift < 1.0) ||
+       !(c.dt_ms / c.consolidation_tau * c.consolidation_drift >= 0.0)))
+    return fail(h, NS_ERR_INVALID_ARG, "bad consolidation parameters (need 0 <= dt*drift/tau < 1)");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
     return fail(h, NS_ERR_NO_DEVICE, "no CUDA device is visible");
@@ -865,17 +1028,18 @@ ns_status ns_create(const ns_config* cfg, ns_handle** out) {
   {
     // grid-stride kernels get exactly the resident capacity of the device
     int nb = 0;
-    prop_fn pf = pick_prop(c.input_mode, c.weight_format);
+    const bool ext = c.rstdp_enabled || c.consolidation_enabled;
+    prop_fn pf = pick_prop(c.input_mode, c.weight_format, ext);
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pf, 256, 0) != cudaSuccess || nb < 1) nb = 4;
     h->prop_blocks = h->sms * nb;
     nb = 0;
     for (int v = 0; v < 2; ++v) {
       nb = 0;
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pick_fused(c.input_mode, c.weight_format, v ? 3u : 1u), 256, 0) != cudaSuccess || nb < 1) nb = 4;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pick_fused(c.input_mode, c.weight_format, v ? 3u : 1u, ext), 256, 0) != cudaSuccess || nb < 1) nb = 4;
       h->fused_blocks[v] = h->sms * nb;
     }
     nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pick_ltd(c.weight_format), 256, 0) != cudaSuccess || nb < 1) nb = 4;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pick_ltd(c.weight_format, ext), 256, 0) != cudaSuccess || nb < 1) nb = 4;
     h->ltd_blocks = h->sms * nb;
     h->ltd_narrow_blocks = h->sms * 2;
     nb = 0;
@@ -907,6 +1071,8 @@ ns_status ns_destroy(ns_handle* h) {
   free_bag(h->log_allocs);
   free_bag(h->batch_allocs);
   free_bag(h->sur_allocs);
+  free_bag(h->ext_allocs);
+  free_bag(h->stp_allocs);
   if (h->ctl) cudaFree(h->ctl);
   if (h->st2) cudaStreamSynchronize(h->st2);
   if (h->ev_rows) cudaEventDestroy(h->ev_rows);
@@ -935,6 +1101,7 @@ ns_status ns_set_drive(ns_handle* h, const ns_drive* dr) {
 }
 
 static ns_status alloc_dynamic(ns_handle* h);
+static ns_status set_eligibility(ns_handle* h, const uint8_t* eligible, const float* values);
 
 ns_status ns_upload_neurons(ns_handle* h, const ns_neuron_soa* s) {
   if (!h) return NS_ERR_NULL_HANDLE;
@@ -1076,7 +1243,8 @@ static ns_status alloc_dynamic(ns_handle* h) {
     if (d.contrib) CK(cudaMemsetAsync(d.contrib, 0, h->alloc_bytes[d.contrib], h->st));
     if (h->fb_count) CK(cudaMemsetAsync(h->fb_count, 0, 4, h->st));
     CK(cudaMemsetAsync(h->ctl, 0, sizeof(ns::Ctl), h->st));
-    CK(cudaStreamSynchronize(h->st));
+    CK(set_ext_ctl(h, 0, h->cfg.reward_signal, 0u, 0.0, 0));
+    h->win_ran = false;
     return NS_OK;
   }
   drop_graphs(h);
@@ -1129,9 +1297,10 @@ static ns_status alloc_dynamic(ns_handle* h) {
     h->win_rows_blocks = h->sms * nb;
     cudaGetLastError();
   }
-  // reset the control block: counters, log, tickets
+  // reset the control block: counters, log, tickets; reward and frame origin
   CK(cudaMemsetAsync(h->ctl, 0, sizeof(ns::Ctl), h->st));
-  CK(cudaStreamSynchronize(h->st));
+  CK(set_ext_ctl(h, 0, h->cfg.reward_signal, 0u, 0.0, 0));
+  h->win_ran = false;
   return NS_OK;
 }
 
@@ -1276,6 +1445,16 @@ ns_status ns_upload_csr(ns_handle* h, uint64_t n, uint64_t m, const uint64_t* ro
     h->d = dn;
   }
   h->have_csr = true;
+  // short-term plasticity belongs to the previous synapse list
+  if (h->d.stp_f) {
+    drop_graphs(h);
+    free_bag(h->stp_allocs);
+    h->d.stp_f = nullptr;
+  }
+  if (h->cfg.rstdp_enabled) {
+    ns_status r = set_eligibility(h, nullptr, nullptr);
+    if (r) return r;
+  }
   if (h->have_neurons) return alloc_dynamic(h);
   return NS_OK;
 }
@@ -1448,12 +1627,15 @@ ns_status ns_step_traced(ns_handle* h, uint64_t* pos_out, uint64_t cap, uint64_t
   }
   NsDev d = h->d;
   neuron_fn nf = pick_neuron(h->cfg.model, h->cfg.input_mode);
-  prop_fn pf = pick_prop(h->cfg.input_mode, h->cfg.weight_format);
+  const bool ext = ext_on(h);
+  prop_fn pf = pick_prop(h->cfg.input_mode, h->cfg.weight_format, ext);
   nf<<<h->ntiles, ns::kThreads, 0, h->st>>>(d, 0);
+  if (tail_on(h)) ns::k_setup<<<1, 32, 0, h->st>>>(d, 0);
   ns::k_trace_offsets<<<1, 32, 0, h->st>>>(d, off);
   d.trace_pos = pos; d.trace_off = off; d.trace_cap = cap;
   pf<<<h->prop_blocks, 256, 0, h->st>>>(d, 0);
-  if (h->cfg.stdp_enabled) pick_ltd(h->cfg.weight_format)<<<h->ltd_blocks, 256, 0, h->st>>>(d, 0);
+  if (h->cfg.stdp_enabled) pick_ltd(h->cfg.weight_format, ext)<<<h->ltd_blocks, 256, 0, h->st>>>(d, 0);
+  if (tail_on(h)) launch_tail(h, d, 0, h->st);
   if (h->cfg.homeostasis_enabled) launch_homeo(h, d, 0, h->st);
   ns::k_advance<<<1, 1, 0, h->st>>>(h->ctl, 1);
   h->launches += launches_per_step(h, 2) + 2;
@@ -1592,6 +1774,14 @@ ns_status ns_download_state(ns_handle* h, ns_neuron_soa* o, float* w_out) {
     } else {
       CK(dn(w_out, d.w32, h->m * 4));
     }
+    if (h->cfg.consolidation_enabled) {
+      // plain weights of the next step's consolidation frame
+      ns::Ctl cc{};
+      CK(dn(&cc, h->ctl, sizeof(cc)));
+      float fr[3];
+      frame_now(h, cc, fr);
+      for (uint64_t q = 0; q < h->m; ++q) w_out[q] = w_out[q] * fr[0] + fr[1];
+    }
   }
   return NS_OK;
 }
@@ -1626,6 +1816,18 @@ ns_status ns_upload_state(ns_handle* h, const ns_neuron_soa* in, const float* w_
     const uint64_t rows = (uint64_t)h->ntypes_acc * h->cfg.delay_steps;
     for (uint64_t q = 0; q < rows; ++q) CK(upl(d.acc + q * h->n_pad, in->pending_input + q * n, n * 8));
   }
+  // the reward carries over; the consolidation frame restarts at `step`
+  ns::Ctl old_c{};
+  CK(copy_sync(h, &old_c, h->ctl, sizeof(old_c), cudaMemcpyDeviceToHost));
+  const double rew_keep = reward_now(h, old_c);
+  const double sum_keep = old_c.reward_sum + (old_c.step_base > old_c.origin ? rew_keep : 0.0);
+  if (h->cfg.consolidation_enabled && !w_in && h->m) {
+    float fr[3];
+    frame_now(h, old_c, fr);
+    k_weights_to_plain<<<h->sms * 8, 256, 0, h->st>>>(d.w32, d.w16, h->m, fr[0], fr[1]);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->st));
+  }
   if (w_in && h->m) {
     float* tmpw = nullptr;
     CK(cudaMalloc(&tmpw, h->m * 4));
@@ -1647,8 +1849,183 @@ ns_status ns_upload_state(ns_handle* h, const ns_neuron_soa* in, const float* w_
   ns::Ctl c{};
   c.step_base = step;
   c.sim_time = (double)step * h->cfg.dt_ms;
+  c.origin = step;
+  c.rew_init = rew_keep;
+  c.ezero_init = 0u;
+  c.reward_sum = sum_keep;
+  c.cons_k0 = step;
   CK(cudaMemcpyAsync(h->ctl, &c, sizeof(c), cudaMemcpyHostToDevice, h->st));
   CK(cudaStreamSynchronize(h->st));
+  return NS_OK;
+}
+
+// R-STDP eligibility arrays: flags (from `eligible`, or every plastic
+// synapse) and values (or 0). Reuses same-sized buffers.
+static ns_status set_eligibility(ns_handle* h, const uint8_t* eligible, const float* values) {
+  NsDev& d = h->d;
+  const uint64_t mp = h->m_pad;
+  const bool reuse = !h->ext_allocs.empty() && d.elig && h->alloc_bytes[d.elig] == std::max<size_t>(mp * 4, 16);
+  if (!reuse) {
+    drop_graphs(h);
+    free_bag(h->ext_allocs);
+    d.elig = nullptr; d.elig_flag = nullptr;
+    float* ev = nullptr;
+    uint8_t* fl = nullptr;
+    ns_status st;
+    if ((st = dalloc(h, h->ext_allocs, &ev, mp)) || (st = dalloc(h, h->ext_allocs, &fl, mp))) return st;
+    d.elig = ev; d.elig_flag = fl;
+  }
+  uint8_t* fl = const_cast<uint8_t*>(d.elig_flag);
+  CK(cudaMemsetAsync(fl, 0, mp, h->st));
+  CK(cudaMemsetAsync(d.elig, 0, mp * 4, h->st));
+  if (h->m) {
+    if (eligible) {
+      CK(cudaMemcpyAsync(fl, eligible, h->m, cudaMemcpyHostToDevice, h->st));
+    } else {
+      k_elig_from_plastic<<<h->sms * 4, 256, 0, h->st>>>(d.row_ptr, h->n, d.row_plastic, d.plastic, fl);
+      CK(cudaGetLastError());
+    }
+    if (values) CK(cudaMemcpyAsync(d.elig, values, h->m * 4, cudaMemcpyHostToDevice, h->st));
+  }
+  CK(cudaStreamSynchronize(h->st));
+  return NS_OK;
+}
+
+// Moves the reward origin to the current step (reward and sum carry over).
+static ns_status rebase_reward(ns_handle* h, unsigned ezero) {
+  ns::Ctl c{};
+  CK(copy_sync(h, &c, h->ctl, sizeof(c), cudaMemcpyDeviceToHost));
+  const double now = reward_now(h, c);
+  const double sum = c.reward_sum + (c.step_base > c.origin ? now : 0.0);
+  CK(set_ext_ctl(h, c.step_base, now, ezero, sum, c.cons_k0));
+  return NS_OK;
+}
+
+ns_status ns_upload_eligibility(ns_handle* h, const uint8_t* eligible, const float* values) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  if (!h->cfg.rstdp_enabled) return fail(h, NS_ERR_STATE, "R-STDP is not enabled in the config");
+  if (!h->have_csr) return fail(h, NS_ERR_STATE, "upload the CSR first");
+  if (values)
+    for (uint64_t q = 0; q < h->m; ++q)
+      if (!is_fin(values[q])) return fail(h, NS_ERR_NONFINITE, "non-finite eligibility value");
+  CK(cudaSetDevice(h->dev));
+  CK(cudaStreamSynchronize(h->st));
+  ns_status r = set_eligibility(h, eligible, values);
+  if (r) return r;
+  if (h->have_neurons && h->ctl) return rebase_reward(h, 0u);
+  return NS_OK;
+}
+
+ns_status ns_download_eligibility(ns_handle* h, float* values_out) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  if (!values_out) return fail(h, NS_ERR_INVALID_ARG, "null output");
+  if (!h->have_csr) return fail(h, NS_ERR_STATE, "upload the CSR first");
+  CK(cudaSetDevice(h->dev));
+  CK(cudaStreamSynchronize(h->st));
+  if (!h->d.elig) {
+    std::fill(values_out, values_out + h->m, 0.0f);
+    return NS_OK;
+  }
+  if (h->m) CK(copy_sync(h, values_out, h->d.elig, h->m * 4, cudaMemcpyDeviceToHost));
+  return NS_OK;
+}
+
+ns_status ns_apply_reward(ns_handle* h, double reward) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  if (!is_fin(reward)) return fail(h, NS_ERR_NONFINITE, "non-finite reward");
+  ns_status r = ready(h);
+  if (r) return r;
+  if (!h->cfg.rstdp_enabled || !h->d.elig) return NS_OK;  // no R-STDP rule: nothing to do
+  CK(cudaSetDevice(h->dev));
+  CK(cudaStreamSynchronize(h->st));
+  fill_scalars(h);
+  ns::Ctl c{};
+  CK(copy_sync(h, &c, h->ctl, sizeof(c), cudaMemcpyDeviceToHost));
+  float fr[3];
+  frame_now(h, c, fr);
+  const float lrr = (float)(h->cfg.rstdp_lr * reward);
+  const int cons = h->cfg.consolidation_enabled ? 1 : 0;
+  if (h->cfg.weight_format == NS_WEIGHT_BF16)
+    k_apply_reward<true><<<h->sms * 8, 256, 0, h->st>>>(h->d, lrr, cons, fr[0], fr[1], fr[2]);
+  else
+    k_apply_reward<false><<<h->sms * 8, 256, 0, h->st>>>(h->d, lrr, cons, fr[0], fr[1], fr[2]);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(h->st));
+  h->launches += 1;
+  return rebase_reward(h, 1u);
+}
+
+ns_status ns_get_reward(ns_handle* h, double* reward, double* reward_sum) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  if (!reward || !reward_sum) return fail(h, NS_ERR_INVALID_ARG, "null output");
+  ns_status r = ready(h);
+  if (r) return r;
+  if (h->n_nets || h->win_ran || !tail_on(h))
+    return fail(h, NS_ERR_UNSUPPORTED,
+                "the reward is maintained by the step-synchronous path of one network with R-STDP or consolidation");
+  CK(cudaSetDevice(h->dev));
+  ns::Ctl c{};
+  CK(copy_sync(h, &c, h->ctl, sizeof(c), cudaMemcpyDeviceToHost));
+  const double now = reward_now(h, c);
+  *reward = now;
+  *reward_sum = c.reward_sum + (c.step_base > c.origin ? now : 0.0);
+  return NS_OK;
+}
+
+ns_status ns_set_reward(ns_handle* h, double reward) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  if (!is_fin(reward)) return fail(h, NS_ERR_NONFINITE, "non-finite reward");
+  ns_status r = ready(h);
+  if (r) return r;
+  CK(cudaSetDevice(h->dev));
+  ns::Ctl c{};
+  CK(copy_sync(h, &c, h->ctl, sizeof(c), cudaMemcpyDeviceToHost));
+  const uint64_t K = c.step_base;
+  const unsigned ez = K == c.origin ? c.ezero_init : (c.mode[(K - 1) & 1] != 0u ? 1u : 0u);
+  CK(set_ext_ctl(h, K, reward, ez, 0.0, c.cons_k0));
+  return NS_OK;
+}
+
+ns_status ns_upload_stp(ns_handle* h, const uint8_t* has_stp, const double* stp) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  if (!h->have_csr) return fail(h, NS_ERR_STATE, "upload the CSR first");
+  CK(cudaSetDevice(h->dev));
+  CK(cudaStreamSynchronize(h->st));
+  const bool cond = h->cfg.input_mode == NS_INPUT_CONDUCTANCE_REF ||
+                    h->cfg.input_mode == NS_INPUT_CONDUCTANCE_FRESH;
+  if (!stp || cond) {
+    // no STP, or conductance mode, where the reference does not apply it
+    if (h->d.stp_f) {
+      drop_graphs(h);
+      free_bag(h->stp_allocs);
+      h->d.stp_f = nullptr;
+    }
+    return NS_OK;
+  }
+  // one step of a copy of the state: (u + u_se*(1-u)/tau_facil*dt) * r
+  std::vector<float> f(h->m_pad, 1.0f);
+  for (uint64_t q = 0; q < h->m; ++q) {
+    if (has_stp && !has_stp[q]) continue;
+    const double* x = stp + 5 * q;
+    const double u = x[3] + x[0] * (1.0 - x[3]) / x[2] * h->cfg.dt_ms;
+    const double e = u * x[4];
+    if (!is_fin(e)) return fail(h, NS_ERR_NONFINITE, "non-finite STP factor");
+    f[q] = (float)e;
+  }
+  if (!h->d.stp_f) {
+    drop_graphs(h);
+    float* p = nullptr;
+    ns_status st;
+    if ((st = dalloc(h, h->stp_allocs, &p, h->m_pad))) return st;
+    h->d.stp_f = p;
+  }
+  CK(copy_sync(h, const_cast<float*>(h->d.stp_f), f.data(), h->m_pad * 4, cudaMemcpyHostToDevice));
+  if (h->win) {
+    // the window kernels deliver plain weights: STP runs the step path
+    drop_graphs(h);
+    h->win = 0;
+    h->wcur = 0;
+  }
   return NS_OK;
 }
 
@@ -1708,13 +2085,19 @@ ns_status ns_weight_stats(ns_handle* h, double* mean, double* stddev) {
   double* acc = nullptr;
   CK(cudaMalloc(&acc, 16));
   CK(cudaMemsetAsync(acc, 0, 16, h->st));
-  k_weight_sum<<<h->sms * 8, 256, 0, h->st>>>(h->d.w32, h->d.w16, h->m, 0.0, 0, acc);
+  ns::Ctl cc{};
+  CK(cudaMemcpyAsync(&cc, h->ctl, sizeof(cc), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  float fr[3];
+  frame_now(h, cc, fr);
+  const int cons = h->cfg.consolidation_enabled ? 1 : 0;
+  k_weight_sum<<<h->sms * 8, 256, 0, h->st>>>(h->d.w32, h->d.w16, h->m, 0.0, 0, cons, fr[0], fr[1], acc);
   double s = 0;
   cudaError_t e = cudaMemcpyAsync(&s, acc, 8, cudaMemcpyDeviceToHost, h->st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
   const double mu = s / (double)h->m;
   if (e == cudaSuccess) {
-    k_weight_sum<<<h->sms * 8, 256, 0, h->st>>>(h->d.w32, h->d.w16, h->m, mu, 1, acc + 1);
+    k_weight_sum<<<h->sms * 8, 256, 0, h->st>>>(h->d.w32, h->d.w16, h->m, mu, 1, cons, fr[0], fr[1], acc + 1);
     e = cudaMemcpyAsync(&s, acc + 1, 8, cudaMemcpyDeviceToHost, h->st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
   }
@@ -1752,22 +2135,26 @@ ns_status ns_profile_steps(ns_handle* h, uint32_t n_steps, double* kernel_ms, ui
   CK(cudaSetDevice(h->dev));
   fill_scalars(h);
   neuron_fn nf = pick_neuron(h->cfg.model, h->cfg.input_mode);
-  prop_fn pf = pick_prop(h->cfg.input_mode, h->cfg.weight_format);
-  ltd_fn lf = pick_ltd(h->cfg.weight_format);
-  // kernels in order neuron, rows, ltd, homeostasis; serial, one event pair each
-  const bool on[4] = {true, true, h->cfg.stdp_enabled != 0, h->cfg.homeostasis_enabled != 0};
+  const bool ext = ext_on(h);
+  prop_fn pf = pick_prop(h->cfg.input_mode, h->cfg.weight_format, ext);
+  ltd_fn lf = pick_ltd(h->cfg.weight_format, ext);
+  // kernels in order neuron, rows, ltd (+ the R-STDP / consolidation tail),
+  // homeostasis; serial, one event pair each
+  const bool on[4] = {true, true, h->cfg.stdp_enabled != 0 || tail_on(h), h->cfg.homeostasis_enabled != 0};
   std::vector<cudaEvent_t> ev((size_t)n_steps * 8);
   for (auto& e : ev) CK(cudaEventCreate(&e));
   for (uint32_t j = 0; j < n_steps; ++j) {
     cudaEvent_t* e = &ev[(size_t)j * 8];
     CK(cudaEventRecord(e[0], h->st));
     nf<<<h->ntiles, ns::kThreads, 0, h->st>>>(h->d, j);
+    if (tail_on(h)) ns::k_setup<<<1, 32, 0, h->st>>>(h->d, j);
     CK(cudaEventRecord(e[1], h->st));
     CK(cudaEventRecord(e[2], h->st));
     pf<<<h->prop_blocks, 256, 0, h->st>>>(h->d, j);
     CK(cudaEventRecord(e[3], h->st));
     CK(cudaEventRecord(e[4], h->st));
-    if (on[2]) lf<<<h->ltd_blocks, 256, 0, h->st>>>(h->d, j);
+    if (h->cfg.stdp_enabled) lf<<<h->ltd_blocks, 256, 0, h->st>>>(h->d, j);
+    if (tail_on(h)) launch_tail(h, h->d, j, h->st);
     CK(cudaEventRecord(e[5], h->st));
     CK(cudaEventRecord(e[6], h->st));
     if (on[3]) launch_homeo(h, h->d, j, h->st);
@@ -1787,7 +2174,7 @@ ns_status ns_profile_steps(ns_handle* h, uint32_t n_steps, double* kernel_ms, ui
       ++nl;
     }
   for (auto& e : ev) cudaEventDestroy(e);
-  h->launches += nl + 1;
+  h->launches += nl + 1 + (tail_on(h) ? (h->cfg.stdp_enabled ? 2u : 1u) * (uint64_t)n_steps : 0);
   return check_device_status(h);
 }
 

@@ -42,6 +42,18 @@ struct Ctl {
   unsigned long long log_size;    // indices held
   unsigned long long log_steps;   // steps held
   unsigned long long log_first;   // global step of the first logged step
+  // reward (R-STDP), R-STDP mode and consolidation frame; step k at [k & 1]
+  double rew[2];                  // reward seen by phase 2 of step k
+  double consA[2];                // frame scale A_k = a^(k - cons_k0)
+  float frame[2][8];              // A_k, B_k, 1/A_k, A_k+1, B_k+1, 1/A_k+1, lr*R_k
+  unsigned int mode[2];           // 0 no reward, 1 applied in the STDP walks, 2 full pass
+  unsigned long long outs[4];     // output spikes of step k at [k & 3]
+  double reward_sum;              // reward after each step since `origin`
+  double rew_init;                // reward at step `origin`
+  unsigned long long origin;
+  unsigned long long cons_k0;     // step whose frame is the identity
+  unsigned int ezero_init;        // eligibility all 0 and in range at `origin`
+  unsigned int tail_done;         // blocks of k_tail finished (renormalisation)
 };
 
 struct Kick { uint32_t target; float amt; };
@@ -114,6 +126,15 @@ struct NsDev {
   uint32_t* seg_off;               // [W][nseg + 1]
   uint32_t* step_total;            // [W]
   uint32_t nseg, wmax;
+  // R-STDP (plasticity.rs:166-221), consolidation (:269-290) and
+  // short-term plasticity (:85-116)
+  int rstdp, cons, fuse, plast_any;
+  float ce, rw_min, rw_max, pad_f;  // exp(-dt/eligibility_tau), R-STDP clamp
+  double reward_decay, rstdp_lr, cons_a, cons_T;
+  unsigned long long reward_thr;
+  float* elig;                     // eligibility values [m_pad]
+  const uint8_t* elig_flag;        // synapse carries an eligibility trace [m_pad]
+  const float* stp_f;              // STP factor per synapse, or null
 };
 
 __device__ __forceinline__ bool bit_of(const uint32_t* bm, uint32_t i) {
@@ -315,6 +336,53 @@ __device__ __forceinline__ bool update_one(const NsDev& d, uint64_t k, uint64_t 
   const bool sp = model_step<MODEL>(d, st, par, rs, Iv, kk, MODE == 1);
   st.I = Iv;
   return sp;
+}
+
+// ---------------------------------------------------------------------------
+// Per-step bookkeeping of the rest of phase 2, run by one thread (k_setup,
+// between the neuron kernel and the walks of the step):
+//  - the reward seen by step k: the previous step's reward decayed
+//    (engine.rs:563, whenever plasticity is on), raised to min(r + 1, 1) when
+//    that step had at least reward_threshold output spikes (:626-631);
+//  - the R-STDP mode of step k: 0 when |reward| <= 0.001 (engine.rs:547-548);
+//    1 when every eligibility trace was zero before the step (the previous
+//    step applied the reward), so the walks apply it to the synapses they
+//    touch; 2 otherwise (a full pass after the walks);
+//  - the consolidation frame: A_k = a^(k - k0), B_k = target*(1 - A_k), with
+//    a = 1 - dt*drift/tau (ConsolidationRule::apply, plasticity.rs:286-289).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void phase2_setup(const NsDev& d, unsigned long long k) {
+  // the output spikes of step k-1 were counted by its walks (flush_counters)
+  Ctl* c = d.ctl;
+  double R;
+  unsigned ez;
+  if (k == c->origin) {
+    R = c->rew_init;
+    ez = c->ezero_init;
+  } else {
+    const double Rp = c->rew[(k - 1) & 1];
+    const double Rd = d.plast_any ? Rp * d.reward_decay : Rp;
+    R = (c->outs[(k - 1) & 3] >= d.reward_thr) ? fmin(Rd + 1.0, 1.0) : Rd;
+    c->reward_sum += R;
+    ez = c->mode[(k - 1) & 1] != 0u ? 1u : 0u;
+  }
+  c->rew[k & 1] = R;
+  c->outs[(k + 2) & 3] = 0ull;
+  const bool active = d.rstdp && fabs(R) > 0.001;
+  c->mode[k & 1] = !active ? 0u : ((ez && d.fuse) ? 1u : 2u);
+  float* f = c->frame[k & 1];
+  f[6] = (float)(d.rstdp_lr * R);
+  if (d.cons) {
+    const double A0 = (k == c->cons_k0) ? 1.0 : c->consA[(k - 1) & 1] * d.cons_a;
+    const double A1 = A0 * d.cons_a;
+    c->consA[k & 1] = A0;
+    f[0] = (float)A0; f[1] = (float)(d.cons_T * (1.0 - A0)); f[2] = (float)(1.0 / A0);
+    f[3] = (float)A1; f[4] = (float)(d.cons_T * (1.0 - A1)); f[5] = (float)(1.0 / A1);
+  }
+}
+
+__global__ void k_setup(NsDev d, uint32_t jstep) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) phase2_setup(d, d.ctl->step_base + jstep);
 }
 
 // ---------------------------------------------------------------------------
@@ -684,15 +752,42 @@ __device__ __forceinline__ StepCtx step_ctx(const NsDev& d, uint32_t jstep) {
   return c;
 }
 
+// Value to store for a synapse whose weight this step's STDP set to w1 (a
+// plain weight): w1 in the consolidation frame of step k; or, when the walks
+// apply the reward (mode 1) to a synapse with an eligibility trace, the
+// weight after the step's consolidation and reward, in the frame of step k+1
+// (engine.rs:539-561). The reward changes a weight only where e != 0 or the
+// weight lies outside [rstdp_w_min, rstdp_w_max] (elsewhere clamp(w + 0) is
+// w). ev: the synapse's eligibility, zeroed when the reward is applied.
+template <bool BF16>
+__device__ __forceinline__ float ext_store(const NsDev& d, const float* fr, uint32_t mode, float w1,
+                                           bool el, float& ev) {
+  if (mode == 1u && el) {
+    float u1 = d.cons ? (w1 - fr[1]) * fr[2] : w1;
+    if (BF16) u1 = bf16_bits_to_f32(f32_to_bf16_bits(u1));
+    float x = d.cons ? u1 * fr[3] + fr[4] : u1;
+    if (ev != 0.0f || x < d.rw_min || x > d.rw_max) {
+      x = clampw(x + fr[6] * ev, d.rw_min, d.rw_max);
+      ev = 0.0f;
+      return d.cons ? (x - fr[4]) * fr[5] : x;
+    }
+    return u1;
+  }
+  return d.cons ? (w1 - fr[1]) * fr[2] : w1;
+}
+
 // Row walk of spiking source j (the item-th spike of the step): bookkeeping
 // (log entry, last spike step, trace bump), then the CSR row in 128-entry
 // chunks: accumulation into the delay slot and LTP (LTP then LTD when the
 // target spiked in this step too).
-template <bool COND, bool BF16>
+template <bool COND, bool BF16, bool EXT>
 __device__ __forceinline__ void row_item(const NsDev& d, const StepCtx& c, uint32_t item, uint32_t j,
                                          int lane, unsigned long long& ev, uint32_t& outs) {
   const bool STDP = c.stdp, HOMEO = c.homeo;
   const uint64_t k = c.k;
+  // EXT: consolidation frame / reward of this step, eligibility, STP
+  const float* fr = EXT ? d.ctl->frame[k & 1] : nullptr;
+  const uint32_t mode = EXT ? d.ctl->mode[k & 1] : 0u;
   const uint64_t beg = __ldg(d.row_ptr + j), end = __ldg(d.row_ptr + j + 1);
   const uint8_t rp = STDP ? __ldg(d.row_plastic + j) : 0;
   const uint8_t rt = COND ? __ldg(d.row_type + j) : 0;
@@ -725,6 +820,11 @@ __device__ __forceinline__ void row_item(const NsDev& d, const StepCtx& c, uint3
     if (rv) {
       c4 = __ldg(reinterpret_cast<const uint4*>(d.col + e0));
       load_w4(d, BF16, e0, w);
+      if (EXT && d.cons) {
+        const float A0 = fr[0], B0 = fr[1];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) w[q] = w[q] * A0 + B0;
+      }
     }
     const uint32_t cc[4] = {c4.x, c4.y, c4.z, c4.w};
     bool inr[4];
@@ -744,7 +844,10 @@ __device__ __forceinline__ void row_item(const NsDev& d, const StepCtx& c, uint3
       const uint64_t e = e0 + q;
       int ty = 0;
       if (COND) ty = (rt == 255) ? (int)__ldg(d.type + e) : (int)rt;
-      const float val = (COND && (ty == 1 || ty == 2)) ? fabsf(w[q]) : w[q];
+      float val = (COND && (ty == 1 || ty == 2)) ? fabsf(w[q]) : w[q];
+      // short-term plasticity: one step of a copy of the synapse's state
+      // scales the delivered current (engine.rs:457-463)
+      if (EXT && !COND && d.stp_f) val = val * __ldg(d.stp_f + e);
       atomicAdd(d.acc + ((uint64_t)ty * d.D + c.slot) * d.n_pad + cc[q],
                 (unsigned long long)to_fix(val));
       if (d.inbits)
@@ -760,7 +863,7 @@ __device__ __forceinline__ void row_item(const NsDev& d, const StepCtx& c, uint3
           if (kSyn[ty].mg) g = g * (1.0f / (1.0f + (1.0f / 3.57f) * expf(-0.062f * d.v[cc[q]])));
           mag = fabsf(g);
         } else {
-          mag = fabsf(w[q]);
+          mag = fabsf(val);
         }
         d.contrib[e] = d.contrib[e] * d.cd + mag * d.one_m_cd;
       }
@@ -769,14 +872,40 @@ __device__ __forceinline__ void row_item(const NsDev& d, const StepCtx& c, uint3
       pj = __shfl_sync(0xffffffffu, pj, 0);
       float wn[4];
       bool chg = false, all4 = true;
+      // eligibility traces of the plastic synapses that carry one
+      bool el[4] = {false, false, false, false};
+      float evl[4] = {0.f, 0.f, 0.f, 0.f};
+      if (EXT && d.rstdp && (pl[0] | pl[1] | pl[2] | pl[3])) {
+        const uchar4 f4 = *reinterpret_cast<const uchar4*>(d.elig_flag + e0);
+        el[0] = pl[0] && f4.x; el[1] = pl[1] && f4.y; el[2] = pl[2] && f4.z; el[3] = pl[3] && f4.w;
+        if (el[0] | el[1] | el[2] | el[3]) {
+          const float4 v4 = *reinterpret_cast<const float4*>(d.elig + e0);
+          evl[0] = v4.x; evl[1] = v4.y; evl[2] = v4.z; evl[3] = v4.w;
+        }
+      }
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
         wn[q] = w[q];
         if (!pl[q]) { all4 = false; continue; }
-        float w1 = clampw(w[q] + d.a_plus * fabsf(tq[q]), d.w_min, d.w_max);
-        if (neg(tq[q])) w1 = clampw(w1 + d.neg_a_minus * pj, d.w_min, d.w_max);
-        wn[q] = w1;
+        const float dp = d.a_plus * fabsf(tq[q]);
+        float w1 = clampw(w[q] + dp, d.w_min, d.w_max);
+        if (EXT && el[q]) evl[q] = evl[q] * d.ce + dp;   // EligibilityTrace::update, engine.rs:519-522
+        if (neg(tq[q])) {
+          const float dm = d.neg_a_minus * pj;
+          w1 = clampw(w1 + dm, d.w_min, d.w_max);
+          if (EXT && el[q]) evl[q] = evl[q] * d.ce + dm;  // engine.rs:531-533
+        }
+        wn[q] = EXT ? ext_store<BF16>(d, fr, mode, w1, el[q], evl[q]) : w1;
         chg = true;
+      }
+      if (EXT && (el[0] | el[1] | el[2] | el[3])) {
+        if (el[0] & el[1] & el[2] & el[3]) {
+          *reinterpret_cast<float4*>(d.elig + e0) = make_float4(evl[0], evl[1], evl[2], evl[3]);
+        } else {
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            if (el[q]) d.elig[e0 + q] = evl[q];
+        }
       }
       if (chg) {
         if (BF16) {
@@ -806,8 +935,10 @@ __device__ __forceinline__ void row_item(const NsDev& d, const StepCtx& c, uint3
 
 // LTD over the plastic incoming synapses of spiking target j whose source did
 // not spike (those whose source spiked are handled by the source's row walk).
-template <bool BF16>
+template <bool BF16, bool EXT>
 __device__ __forceinline__ void ltd_item(const NsDev& d, const StepCtx& c, uint32_t j, int lane) {
+  const float* fr = EXT ? d.ctl->frame[c.k & 1] : nullptr;
+  const uint32_t mode = EXT ? d.ctl->mode[c.k & 1] : 0u;
   const uint64_t ib = __ldg(d.in_ptr + j), ie = __ldg(d.in_ptr + j + 1);
   for (uint64_t q0 = ib; q0 < ie; q0 += 128) {
     uint2 sp[4];
@@ -824,19 +955,31 @@ __device__ __forceinline__ void ltd_item(const NsDev& d, const StepCtx& c, uint3
       pre[u] = act[u] ? c.rec_k[sp[u].x].x : 0.0f;
       if (BF16) wv[u] = act[u] ? bf16_bits_to_f32(d.w16[sp[u].y]) : 0.0f;
       else wv[u] = act[u] ? d.w32[sp[u].y] : 0.0f;
+      if (EXT && d.cons) wv[u] = wv[u] * fr[0] + fr[1];
     }
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       if (!act[u] || neg(pre[u])) continue;
-      const float w1 = clampw(wv[u] + d.neg_a_minus * pre[u], d.w_min, d.w_max);
-      if (BF16) d.w16[sp[u].y] = f32_to_bf16_bits(w1);
-      else d.w32[sp[u].y] = w1;
+      const float dm = d.neg_a_minus * pre[u];
+      const float w1 = clampw(wv[u] + dm, d.w_min, d.w_max);
+      float st = w1;
+      if (EXT) {
+        const uint32_t pos = sp[u].y;
+        const bool el = d.rstdp && d.elig_flag[pos];
+        float evq = el ? d.elig[pos] : 0.0f;
+        if (el) evq = evq * d.ce + dm;   // EligibilityTrace::update, engine.rs:531-533
+        st = ext_store<BF16>(d, fr, mode, w1, el, evq);
+        if (el) d.elig[pos] = evq;
+      }
+      if (BF16) d.w16[sp[u].y] = f32_to_bf16_bits(st);
+      else d.w32[sp[u].y] = st;
     }
   }
 }
 
-__device__ __forceinline__ void flush_counters(const NsDev& d, unsigned long long ev, uint32_t outs,
-                                               unsigned long long* s_ev, uint32_t* s_out) {
+__device__ __forceinline__ void flush_counters(const NsDev& d, uint64_t k, unsigned long long ev,
+                                               uint32_t outs, unsigned long long* s_ev,
+                                               uint32_t* s_out) {
   const int lane = threadIdx.x & 31;
   for (int o = 16; o > 0; o >>= 1) {
     ev += __shfl_down_sync(0xffffffffu, ev, o);
@@ -849,13 +992,16 @@ __device__ __forceinline__ void flush_counters(const NsDev& d, unsigned long lon
   __syncthreads();
   if (threadIdx.x == 0) {
     if (*s_ev) atomicAdd(&d.ctl->events_total, *s_ev);
-    if (*s_out) atomicAdd(&d.ctl->out_total, (unsigned long long)*s_out);
+    if (*s_out) {
+      atomicAdd(&d.ctl->out_total, (unsigned long long)*s_out);
+      atomicAdd(&d.ctl->outs[k & 3], (unsigned long long)*s_out);
+    }
   }
 }
 
 // Kernel 2 (fused schedule): row walks [0, cnt) and LTD lists [cnt, 2 cnt)
 // as warp work items of one grid-stride kernel.
-template <bool COND, bool BF16, int MINB>
+template <bool COND, bool BF16, int MINB, bool EXT>
 __global__ void __launch_bounds__(256, MINB) k_prop_fused(NsDev d, uint32_t jstep) {
   __shared__ uint32_t s_toff[kSmemTiles + 1];
   __shared__ unsigned long long s_ev;
@@ -872,15 +1018,15 @@ __global__ void __launch_bounds__(256, MINB) k_prop_fused(NsDev d, uint32_t jste
   for (uint32_t item = wglob; item < items; item += nw) {
     const uint32_t rank = item < c.cnt ? item : item - c.cnt;
     const uint32_t j = sv.at(rank);
-    if (item < c.cnt) row_item<COND, BF16>(d, c, item, j, lane, ev, outs);
-    else ltd_item<BF16>(d, c, j, lane);
+    if (item < c.cnt) row_item<COND, BF16, EXT>(d, c, item, j, lane, ev, outs);
+    else ltd_item<BF16, EXT>(d, c, j, lane);
   }
-  flush_counters(d, ev, outs, &s_ev, &s_out);
+  flush_counters(d, c.k, ev, outs, &s_ev, &s_out);
 }
 
 // Kernel 2a / 2b (split schedule): the row walks, then the LTD lists on a
 // second stream beside the next step's neuron kernel.
-template <bool COND, bool BF16>
+template <bool COND, bool BF16, bool EXT>
 __global__ void __launch_bounds__(256, 4) k_rows(NsDev d, uint32_t jstep) {
   __shared__ uint32_t s_toff[kSmemTiles + 1];
   __shared__ unsigned long long s_ev;
@@ -894,11 +1040,11 @@ __global__ void __launch_bounds__(256, 4) k_rows(NsDev d, uint32_t jstep) {
   unsigned long long ev = 0ull;
   uint32_t outs = 0u;
   for (uint32_t item = wglob; item < c.cnt; item += nw)
-    row_item<COND, BF16>(d, c, item, sv.at(item), lane, ev, outs);
-  flush_counters(d, ev, outs, &s_ev, &s_out);
+    row_item<COND, BF16, EXT>(d, c, item, sv.at(item), lane, ev, outs);
+  flush_counters(d, c.k, ev, outs, &s_ev, &s_out);
 }
 
-template <bool BF16>
+template <bool BF16, bool EXT>
 __global__ void __launch_bounds__(256, 5) k_ltd(NsDev d, uint32_t jstep) {
   __shared__ uint32_t s_toff[kSmemTiles + 1];
   const int lane = threadIdx.x & 31;
@@ -906,7 +1052,63 @@ __global__ void __launch_bounds__(256, 5) k_ltd(NsDev d, uint32_t jstep) {
   const SpikeView sv = spike_view(d, c.k, c.cnt, s_toff);
   const uint32_t wglob = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const uint32_t nw = gridDim.x * (blockDim.x >> 5);
-  for (uint32_t item = wglob; item < c.cnt; item += nw) ltd_item<BF16>(d, c, sv.at(item), lane);
+  for (uint32_t item = wglob; item < c.cnt; item += nw) ltd_item<BF16, EXT>(d, c, sv.at(item), lane);
+}
+
+// ---------------------------------------------------------------------------
+// Kernel 2c (R-STDP / consolidation): after the step's walks. Mode 2: the
+// reward of engine.rs:546-561 over every synapse with an eligibility trace,
+// in the frame of step k+1 (changing only weights it moves). Renormalisation:
+// when A_k+1 < 2^-16 every stored value becomes its plain weight and the
+// frame of step k+1 the identity (the last block records it). Returns at once
+// in every other step.
+// ---------------------------------------------------------------------------
+template <bool BF16>
+__global__ void __launch_bounds__(256) k_tail(NsDev d, uint32_t jstep) {
+  const unsigned long long k = d.ctl->step_base + jstep;
+  const uint32_t mode = d.ctl->mode[k & 1];
+  const bool renorm = d.cons && d.ctl->consA[k & 1] * d.cons_a < 0x1p-16;
+  if (mode != 2u && !renorm) return;
+  const float* fr = d.ctl->frame[k & 1];
+  const float A1 = fr[3], B1 = fr[4], iA1 = fr[5], lrr = fr[6];
+  const bool cons = d.cons != 0;
+  for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < d.m;
+       s += (uint64_t)gridDim.x * blockDim.x) {
+    const bool ap = mode == 2u && d.elig_flag[s];
+    if (!ap && !renorm) continue;
+    float x = BF16 ? bf16_bits_to_f32(d.w16[s]) : d.w32[s];
+    if (cons) x = x * A1 + B1;
+    bool chg = false;
+    if (ap) {
+      const float evq = d.elig[s];
+      if (evq != 0.0f || x < d.rw_min || x > d.rw_max) {
+        x = clampw(x + lrr * evq, d.rw_min, d.rw_max);
+        d.elig[s] = 0.0f;
+        chg = true;
+      }
+    }
+    if (renorm || chg) {
+      const float st = (renorm || !cons) ? x : (x - B1) * iA1;
+      if (BF16) d.w16[s] = f32_to_bf16_bits(st);
+      else d.w32[s] = st;
+    }
+  }
+  if (renorm) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      const unsigned done = atomicAdd(&d.ctl->tail_done, 1u);
+      if (done == gridDim.x - 1) {
+        __threadfence();
+        Ctl* c = d.ctl;
+        c->cons_k0 = k + 1;
+        c->frame[k & 1][3] = 1.0f;
+        c->frame[k & 1][4] = 0.0f;
+        c->frame[k & 1][5] = 1.0f;
+        c->tail_done = 0u;
+      }
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -916,7 +1118,12 @@ __global__ void __launch_bounds__(256, 5) k_ltd(NsDev d, uint32_t jstep) {
 // ---------------------------------------------------------------------------
 template <bool BF16>
 __global__ void __launch_bounds__(256) k_homeostasis(NsDev d, uint32_t jstep) {
-  (void)jstep;
+  // weights in the consolidation frame of step k+1 (identity without it)
+  const unsigned long long kst = d.ctl->step_base + jstep;
+  const bool cons = d.cons != 0;
+  const float A1 = cons ? d.ctl->frame[kst & 1][3] : 1.0f;
+  const float B1 = cons ? d.ctl->frame[kst & 1][4] : 0.0f;
+  const float iA1 = cons ? d.ctl->frame[kst & 1][5] : 1.0f;
   // one thread per target; sums in ascending CSR position, as the reference
   // walks synapses_by_target (engine.rs:86-92)
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < d.n;
@@ -935,12 +1142,12 @@ __global__ void __launch_bounds__(256) k_homeostasis(NsDev d, uint32_t jstep) {
         const float rel = (float)((double)d.contrib[s] / mean);
         const float arg = nerr * rel * d.dt_f / d.h_tau_f;
         const float scale = exp_f(arg);
-        if (BF16) {
-          const float w = bf16_bits_to_f32(d.w16[s]) * scale;
-          d.w16[s] = f32_to_bf16_bits(clampw(w, 0.0f, 10.0f));
-        } else {
-          d.w32[s] = clampw(d.w32[s] * scale, 0.0f, 10.0f);
-        }
+        float u = BF16 ? bf16_bits_to_f32(d.w16[s]) : d.w32[s];
+        if (cons) u = u * A1 + B1;
+        float w = clampw(u * scale, 0.0f, 10.0f);
+        if (cons) w = (w - B1) * iA1;
+        if (BF16) d.w16[s] = f32_to_bf16_bits(w);
+        else d.w32[s] = w;
       }
     }
     const double inst = bit_of(d.bitmap, (uint32_t)i) ? 1000.0 / d.dt : 0.0;

@@ -39,6 +39,9 @@ class Network:
     n0: np.ndarray = None
     inhibitory: np.ndarray = None
     is_output: np.ndarray = None
+    eligible: np.ndarray = None   # (m,) uint8: synapse carries an R-STDP eligibility trace
+    stp: np.ndarray = None        # (m, 5) float64: u_se, tau_rec, tau_facil, u, r
+    has_stp: np.ndarray = None    # (m,) uint8, None = every synapse (when stp is given)
     name: str = "NeuralSim Network"
 
     @property
@@ -54,7 +57,9 @@ class Network:
         self.row_ptr = np.ascontiguousarray(self.row_ptr, dtype=np.uint64)
         self.col = np.ascontiguousarray(self.col, dtype=np.uint32)
         self.w = np.ascontiguousarray(self.w, dtype=np.float32)
-        for name in ("syn_type", "plastic", "inhibitory", "is_output"):
+        if self.stp is not None:
+            self.stp = np.ascontiguousarray(self.stp, dtype=np.float64).reshape(-1, 5)
+        for name in ("syn_type", "plastic", "inhibitory", "is_output", "eligible", "has_stp"):
             a = getattr(self, name)
             if a is not None:
                 setattr(self, name, np.ascontiguousarray(a, dtype=np.uint8))
@@ -93,6 +98,20 @@ class SimConfig:
     graph_chunk: int = 1000
     step_schedule: int = 0      # 0 autotune, 1 fused, 2 split, 3 fused (4 blocks/SM)
     window_steps: int = 0       # 0 auto (= delay), 1 off, W > 1 explicit
+    # R-STDP (RStdpRule::default, plasticity.rs:177-189; engine.rs:113-116, :521)
+    rstdp_enabled: bool = False
+    rstdp_lr: float = 0.1
+    rstdp_w_min: float = 0.0
+    rstdp_w_max: float = 10.0
+    eligibility_tau: float = 200.0
+    reward_threshold: int = 5
+    reward_decay: float = 0.95
+    reward_signal: float = 0.0
+    # consolidation (ConsolidationRule::default, plasticity.rs:276-284)
+    consolidation_enabled: bool = False
+    consolidation_tau: float = 10000.0
+    consolidation_target: float = 0.5
+    consolidation_drift: float = 0.001
 
     def to_c(self):
         c = A.NsConfig()
@@ -173,6 +192,10 @@ class SimulationEngine:
         self._check(self.lib.ns_upload_csr(
             self._h, net.n, net.m, _ptr(net.row_ptr), _ptr(net.col), _ptr(net.w),
             _ptr(net.syn_type), _ptr(net.plastic)))
+        if self.config.rstdp_enabled and net.eligible is not None:
+            self._check(self.lib.ns_upload_eligibility(self._h, _ptr(net.eligible), None))
+        if net.stp is not None:
+            self._check(self.lib.ns_upload_stp(self._h, _ptr(net.has_stp), _ptr(net.stp)))
 
     def _check(self, st):
         A.check(st, self._h)
@@ -286,6 +309,33 @@ class SimulationEngine:
                 setattr(soa, name, _ptr(st[name]))
         soa.params_per_neuron = PARAMS_PER_NEURON[self.config.model]
         self._check(self.lib.ns_upload_state(self._h, C.byref(soa), _ptr(st.get("w")), int(step)))
+
+    # -- R-STDP reward and eligibility (engine.rs:151-175, :546-563, :626-631) --
+    def eligibility(self):
+        e = np.zeros(max(self.network.m, 1), np.float32)
+        self._check(self.lib.ns_download_eligibility(self._h, _ptr(e)))
+        return e[:self.network.m]
+
+    def upload_eligibility(self, eligible=None, values=None):
+        el = None if eligible is None else np.ascontiguousarray(eligible, np.uint8)
+        va = None if values is None else np.ascontiguousarray(values, np.float32)
+        self._check(self.lib.ns_upload_eligibility(self._h, _ptr(el), _ptr(va)))
+
+    def apply_reward(self, reward: float):
+        self._check(self.lib.ns_apply_reward(self._h, float(reward)))
+
+    @property
+    def reward_signal(self) -> float:
+        return self.reward()[0]
+
+    def reward(self):
+        """(reward_signal now, sum of the reward after each step)."""
+        r, s = C.c_double(), C.c_double()
+        self._check(self.lib.ns_get_reward(self._h, C.byref(r), C.byref(s)))
+        return r.value, s.value
+
+    def set_reward(self, reward: float):
+        self._check(self.lib.ns_set_reward(self._h, float(reward)))
 
     def rates(self):
         r = np.zeros(self.network.n, np.float64)

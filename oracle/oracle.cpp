@@ -369,11 +369,67 @@ template <class R> struct Fast {
   std::vector<uint64_t> log_off{0};
   uint64_t step = 0, events = 0;
   std::vector<Kick> kicks;
+  // R-STDP, consolidation, STP (engine.rs:457-463, :519-563, :626-631)
+  std::vector<uint8_t> elig;   // synapse carries an eligibility trace
+  std::vector<R> e;            // eligibility values
+  std::vector<R> stpf;         // STP factor per synapse (empty: no STP)
+  R ce = 0;                    // exp(-dt / elig_tau)
+  bool plast_any = false, fuse_ok = false;
+  uint64_t origin = 0;         // step at which rew_init / ezero_init hold
+  double rew_init = 0;
+  int ezero_init = 0;
+  double rew_prev = 0, reward_sum = 0, R_k = 0;
+  uint64_t outs_prev = 0;
+  int mode_prev = 0, mode = 0; // 0 no reward, 1 in the STDP walks, 2 full pass
+  R lrr = 0;
+  double cons_a = 1.0, consA_prev = 1.0, consA_cur = 1.0;
+  uint64_t cons_k0 = 0;
+  R fr[6] = {1, 0, 1, 1, 0, 1};  // weight frame of step k and k+1: A, B, 1/A
   bool cond() const { return c.input_mode == 3 || c.input_mode == 4; }
 
   R wget(uint64_t s) const { return bf16 ? (R)bf16_to_f32(wb[s]) : w[s]; }
   void wset(uint64_t s, R x) {
     if (bf16) wb[s] = f32_to_bf16_rne((float)x); else w[s] = x;
+  }
+  // Consolidation frame: the stored value u of a synapse stands for the
+  // weight u*A + B of the frame (A = a^(k - k0), B = target*(1 - A)), so the
+  // per-step drift of every weight toward the target is a change of frame.
+  R wplain(uint64_t s, int f) const {
+    R u = wget(s);
+    return c.cons ? u * fr[3 * f] + fr[3 * f + 1] : u;
+  }
+  void wstore(uint64_t s, R x, int f) { wset(s, c.cons ? (x - fr[3 * f + 1]) * fr[3 * f + 2] : x); }
+  // frame of a step from its A (double), as the device rounds it
+  void frame_of(double A, R* out) const {
+    out[0] = (R)A;
+    out[1] = (R)(c.cons_target * (1.0 - A));
+    out[2] = (R)(1.0 / A);
+  }
+  // mode-1 apply of one synapse touched by this step's STDP: w1 plain in
+  // frame k; returns the stored value's plain weight in frame k+1 after the
+  // reward (engine.rs:546-561 after the consolidation of :539-545)
+  // The reward changes a weight only where e != 0 or the weight lies outside
+  // [rstdp_w_min, rstdp_w_max]; elsewhere clamp(w + lr*r*0) == w exactly.
+  bool reward_moves(R x, R ev) const {
+    return ev != R(0) || x < (R)c.rstdp_wmin || x > (R)c.rstdp_wmax;
+  }
+  R storage_round(R x) const { return bf16 ? (R)bf16_to_f32(f32_to_bf16_rne((float)x)) : x; }
+  void store_touched(uint64_t s, R w1) {
+    if (mode == 1 && elig[s]) {
+      // the value the STDP walk stores, read in the frame of step k+1: the
+      // same numbers the full pass would see
+      const R u1 = storage_round(c.cons ? (w1 - fr[1]) * fr[2] : w1);
+      R x = c.cons ? u1 * fr[3] + fr[4] : u1;
+      if (reward_moves(x, e[s])) {
+        x = clampw<R>(x + lrr * e[s], (R)c.rstdp_wmin, (R)c.rstdp_wmax);
+        e[s] = R(0);
+        wstore(s, x, 1);
+      } else {
+        wset(s, u1);
+      }
+    } else {
+      wstore(s, w1, 0);
+    }
   }
 
   void init(const or_config& cfg, const or_net& net) {
@@ -454,6 +510,112 @@ template <class R> struct Fast {
     };
     if (c.stdp) { table(c.tau_plus, Ep); table(c.tau_minus, Em); }
     spiked.assign(n, 0);
+    // R-STDP state
+    elig.assign(m, 0);
+    e.assign(m, R(0));
+    if (c.rstdp)
+      for (uint64_t s = 0; s < m; ++s) elig[s] = net.eligible ? (net.eligible[s] ? 1 : 0) : plastic[s];
+    ce = (R)std::exp(-c.dt / c.elig_tau);
+    plast_any = c.stdp || c.homeo || c.rstdp || c.cons;
+    fuse_ok = (!c.stdp || (c.rstdp_wmin <= c.w_min && c.w_max <= c.rstdp_wmax)) &&
+              (!c.homeo || (c.rstdp_wmin <= 0.0 && 10.0 <= c.rstdp_wmax)) &&
+              (!c.cons || (c.rstdp_wmin <= c.cons_target && c.cons_target <= c.rstdp_wmax));
+    origin = 0; rew_init = c.reward_init; ezero_init = 0;
+    if (c.cons) cons_a = 1.0 - (c.dt / c.cons_tau) * c.cons_drift;
+    cons_k0 = 0;
+    // STP: one step of a copy of the synapse's state (engine.rs:457-463)
+    stpf.clear();
+    if (net.stp && !cond()) {
+      stpf.assign(m, R(1));
+      for (uint64_t s = 0; s < m; ++s) {
+        if (net.has_stp && !net.has_stp[s]) continue;
+        stpf[s] = (R)stp_factor(net.stp + 5 * s, c.dt);
+      }
+    }
+  }
+
+  static double stp_factor(const double* q, double dt) {
+    // (u + u_se*(1-u)/tau_facil*dt) * r, ShortTermPlasticity::step(dt, true)
+    double u = q[3] + q[0] * (1.0 - q[3]) / q[2] * dt;
+    return u * q[4];
+  }
+
+  // reward, R-STDP mode and consolidation frame of step k (the device's
+  // per-step setup in the neuron kernel's last tile)
+  void setup(uint64_t k) {
+    double Rr;
+    int ez;
+    if (k == origin) {
+      Rr = rew_init;
+      ez = ezero_init;
+    } else {
+      double Rd = plast_any ? rew_prev * c.reward_decay : rew_prev;
+      Rr = (outs_prev >= c.reward_thr) ? std::fmin(Rd + 1.0, 1.0) : Rd;
+      reward_sum += Rr;
+      ez = mode_prev != 0;
+    }
+    R_k = Rr;
+    bool active = c.rstdp && std::fabs(Rr) > 0.001;
+    mode = !active ? 0 : ((ez && fuse_ok) ? 1 : 2);
+    lrr = (R)(c.rstdp_lr * Rr);
+    if (c.cons) {
+      consA_cur = (k == cons_k0) ? 1.0 : consA_prev * cons_a;
+      frame_of(consA_cur, fr);
+      frame_of(consA_cur * cons_a, fr + 3);
+    }
+  }
+
+  // mode-2 reward pass over every eligible synapse and the frame
+  // renormalisation (the device's tail kernel)
+  void tail(uint64_t k) {
+    const bool renorm = c.cons && consA_cur * cons_a < 0x1p-16;
+    if (mode != 2 && !renorm) return;
+    for (uint64_t s = 0; s < m; ++s) {
+      const bool ap = mode == 2 && elig[s];
+      if (!ap && !renorm) continue;
+      R x = wplain(s, 1);
+      bool chg = false;
+      if (ap && reward_moves(x, e[s])) {
+        x = clampw<R>(x + lrr * e[s], (R)c.rstdp_wmin, (R)c.rstdp_wmax);
+        e[s] = R(0);
+        chg = true;
+      }
+      if (renorm) wset(s, x);
+      else if (chg) wstore(s, x, 1);
+    }
+    if (renorm) {
+      cons_k0 = k + 1;
+      fr[3] = R(1); fr[4] = R(0); fr[5] = R(1);
+    }
+  }
+
+  // reward after the last step (phase 3 of engine.rs:626-631)
+  double reward_now() const {
+    if (step == origin) return rew_init;
+    double Rd = plast_any ? rew_prev * c.reward_decay : rew_prev;
+    return (outs_prev >= c.reward_thr) ? std::fmin(Rd + 1.0, 1.0) : Rd;
+  }
+
+  // SimulationEngine::apply_reward between steps, in the frame of the next step
+  void apply_reward(double reward) {
+    if (!c.rstdp) return;
+    const double now = reward_now();
+    R f[3] = {1, 0, 1};
+    if (c.cons) frame_of(step == cons_k0 ? 1.0 : consA_prev * cons_a, f);
+    const R l = (R)(c.rstdp_lr * reward);
+    for (uint64_t s = 0; s < m; ++s) {
+      if (!elig[s]) continue;
+      R u = wget(s);
+      R x = c.cons ? u * f[0] + f[1] : u;
+      if (!reward_moves(x, e[s])) continue;
+      x = clampw<R>(x + l * e[s], (R)c.rstdp_wmin, (R)c.rstdp_wmax);
+      e[s] = R(0);
+      wset(s, c.cons ? (x - f[1]) * f[2] : x);
+    }
+    if (step > origin) reward_sum += now;
+    origin = step;
+    rew_init = now;
+    ezero_init = 1;
   }
 
   R table_at(const std::vector<R>& t, int64_t dk) const {
@@ -590,27 +752,30 @@ template <class R> struct Fast {
       for (uint64_t s = rp[j]; s < rp[j + 1]; ++s) {
         if (trace) { if (*ntr < cap) trace[*ntr] = s; ++*ntr; }
         uint32_t i = col[s];
-        R ws = wget(s);
+        R ws = wplain(s, 0);
         int t = cond() ? type[s] : 0;
         R val = ws;
         if (cond() && (t == 1 || t == 2)) val = std::fabs(ws);
+        if (!stpf.empty()) val = val * stpf[s];
         accumulate((uint64_t)t * D + slot, i, val);
         ++events;
         if (c.homeo) {
           R mag;
           if (cond()) mag = std::fabs(ws * (R)kDyn[t].gmax * mg_block<R>(t, v[i]));
-          else mag = std::fabs(ws);
+          else mag = std::fabs(val);
           contrib[s] = contrib[s] * cd + mag * one_m_cd;
         }
         if (c.stdp && plastic[s]) {
           R w1;
-          if (!spiked[i]) {
-            w1 = clampw<R>(ws + ap * post[i], wlo, whi);
-          } else {
-            w1 = clampw<R>(ws + ap * qdec[i], wlo, whi);
-            w1 = clampw<R>(w1 + nam * pre[j], wlo, whi);
+          const R dp = ap * (spiked[i] ? qdec[i] : post[i]);
+          w1 = clampw<R>(ws + dp, wlo, whi);
+          if (elig[s]) e[s] = e[s] * ce + dp;
+          if (spiked[i]) {
+            const R dm = nam * pre[j];
+            w1 = clampw<R>(w1 + dm, wlo, whi);
+            if (elig[s]) e[s] = e[s] * ce + dm;
           }
-          wset(s, w1);
+          store_touched(s, w1);
         }
       }
     }
@@ -624,8 +789,11 @@ template <class R> struct Fast {
         uint64_t s = in_pos[q];
         uint32_t j = in_src[q];
         if (spiked[j]) continue;
-        R ws = wget(s);
-        wset(s, clampw<R>(ws + nam * pre[j], wlo, whi));
+        R ws = wplain(s, 0);
+        const R dm = nam * pre[j];
+        R w1 = clampw<R>(ws + dm, wlo, whi);
+        if (elig[s]) e[s] = e[s] * ce + dm;
+        store_touched(s, w1);
       }
     }
   }
@@ -646,8 +814,8 @@ template <class R> struct Fast {
           R rel = (R)((double)contrib[s] / mean);
           R arg = (R)(-err) * rel * (R)c.dt / (R)c.h_tau;
           R scale = scale_exp<R>(arg);
-          R ws = wget(s) * scale;
-          wset(s, clampw<R>(ws, R(0), R(10)));
+          R ws = wplain(s, 1) * scale;
+          wstore(s, clampw<R>(ws, R(0), R(10)), 1);
         }
       }
     }
@@ -662,9 +830,17 @@ template <class R> struct Fast {
     phase_a(k);
     log_idx.insert(log_idx.end(), spk.begin(), spk.end());
     log_off.push_back(log_idx.size());
+    setup(k);
     phase_b(k, trace, cap, ntr);
     phase_c();
+    tail(k);
     phase_d();
+    uint64_t outs = 0;
+    for (uint32_t j : spk) outs += outp[j] ? 1u : 0u;
+    outs_prev = outs;
+    rew_prev = R_k;
+    mode_prev = mode;
+    consA_prev = consA_cur;
     ++step;
   }
 };
@@ -680,6 +856,9 @@ struct LitSyn {
   uint8_t type, plastic;
   double pre_trace, post_trace, last_pre, last_post;
   double contribution_avg;
+  uint8_t elig, has_stp;   // eligibility trace (with_rstdp), ShortTermPlasticity
+  double e;                // EligibilityTrace.value
+  double stp[5];           // u_se, tau_rec, tau_facil, u, r
 };
 
 struct Lit {
@@ -707,6 +886,8 @@ struct Lit {
   double lfp = 0, weight_mean = 0, weight_std = 0, mean_rate = 0;
   uint64_t total_spikes = 0;
   int threads = 1;
+  double reward = 0, reward_sum = 0;   // engine.rs:71-77
+  bool plast_any = false;
 
   void init(const or_config& cfg, const or_net& net, int nthreads) {
     c = cfg; n = net.n; m = net.m; threads = nthreads > 0 ? nthreads : 1;
@@ -722,7 +903,13 @@ struct Lit {
         y.plastic = net.plastic ? net.plastic[s] : 0;
         y.pre_trace = 0; y.post_trace = 0; y.last_pre = -1e9; y.last_post = -1e9;
         y.contribution_avg = 0;
+        y.elig = c.rstdp ? (net.eligible ? (net.eligible[s] ? 1 : 0) : y.plastic) : 0;
+        y.e = 0;
+        y.has_stp = (net.stp && (!net.has_stp || net.has_stp[s])) ? 1 : 0;
+        for (int q = 0; q < 5; ++q) y.stp[q] = y.has_stp ? net.stp[5 * s + q] : 0.0;
       }
+    reward = c.reward_init;
+    plast_any = c.stdp || c.homeo || c.rstdp || c.cons;
     cond.assign(m, 0.0);
     ppn = net.ppn;
     par.resize(n * (uint64_t)ppn);
@@ -871,6 +1058,11 @@ struct Lit {
           y.contribution_avg = y.contribution_avg * cdec + std::fabs(gp) * (1.0 - cdec);
         } else {
           double cur = y.weight;
+          if (y.has_stp) {
+            // a copy of the synapse's STP state takes one step (engine.rs:457-463)
+            double su = y.stp[3], sr = y.stp[4];
+            cur *= or_stp_step(&su, &sr, y.stp[0], y.stp[1], y.stp[2], dt, 1);
+          }
           if (D == 1) {
             if (c.input_mode == 0) I[y.target] += cur;
             else ring[0 * n + y.target] += cur;
@@ -907,6 +1099,7 @@ struct Lit {
           double d = current_time - y.last_pre;
           y.pre_trace = y.pre_trace * std::exp(-d / c.tau_plus) + 1.0;
           y.last_pre = current_time;
+          if (y.elig) or_eligibility_update(&y.e, dt, c.elig_tau, delta);
         }
         if (post_fired) {
           double delta = -c.a_minus * y.pre_trace;
@@ -914,9 +1107,18 @@ struct Lit {
           double d = current_time - y.last_post;
           y.post_trace = y.post_trace * std::exp(-d / c.tau_minus) + 1.0;
           y.last_post = current_time;
+          if (y.elig) or_eligibility_update(&y.e, dt, c.elig_tau, delta);
         }
       }
     }
+    // consolidation of every synapse (engine.rs:539-545)
+    if (c.cons)
+      for (LitSyn& y : syn) or_consolidation_apply(&y.weight, c.cons_tau, c.cons_target, c.cons_drift, dt);
+    // R-STDP while the reward is on (engine.rs:546-561), then its decay (:563)
+    if (c.rstdp && std::fabs(reward) > 0.001)
+      for (LitSyn& y : syn)
+        if (y.elig) or_eligibility_apply(&y.e, reward, &y.weight, c.rstdp_lr, c.rstdp_wmin, c.rstdp_wmax);
+    if (plast_any) reward *= c.reward_decay;
     if (c.homeo) {
       for (uint64_t i = 0; i < n; ++i) {
         double rate = firing_rates[i];
@@ -937,7 +1139,11 @@ struct Lit {
     if (c.input_mode == 0 && D == 1) {
       for (uint64_t i = 0; i < n; ++i) I[i] *= c.current_decay;
     }
-    // Phase 3 (engine.rs:617-670)
+    // Phase 3 (engine.rs:617-670): reward from this step's output spikes
+    uint64_t outs = 0;
+    for (uint32_t j : spk) outs += outp[j] ? 1u : 0u;
+    if (outs >= c.reward_thr) reward = std::fmin(reward + 1.0, 1.0);
+    reward_sum += reward;
     for (uint64_t i = 0; i < n; ++i) {
       double inst = spiked[i] ? 1000.0 / dt : 0.0;
       firing_rates[i] += (inst - firing_rates[i]) * dt / 100.0;
@@ -958,6 +1164,16 @@ struct Lit {
     ++step;
   }
 };
+
+// plain weights in the frame of the next step
+template <class R> void fast_weights(const Fast<R>* F, double* w) {
+  R f[3] = {R(1), R(0), R(1)};
+  if (F->c.cons) F->frame_of(F->step == F->cons_k0 ? 1.0 : F->consA_prev * F->cons_a, f);
+  for (uint64_t q = 0; q < F->m; ++q) {
+    R u = F->wget(q);
+    w[q] = (double)(F->c.cons ? u * f[0] + f[1] : u);
+  }
+}
 
 }  // namespace
 
@@ -1120,9 +1336,18 @@ void or_fast_state(void* s, double* v, double* u, double* m, double* h, double* 
     }
   });
 }
-void or_fast_weights(void* s, double* w) {
-  FAST_DISPATCH(s, for (uint64_t q = 0; q < F->m; ++q) w[q] = (double)F->wget(q));
+void or_fast_weights(void* s, double* w) { FAST_DISPATCH(s, fast_weights(F, w)); }
+void or_fast_eligibility(void* s, double* e) {
+  FAST_DISPATCH(s, for (uint64_t q = 0; q < F->m; ++q) e[q] = (double)F->e[q]);
 }
+void or_fast_reward(void* s, double* out2) {
+  FAST_DISPATCH(s, {
+    const double now = F->reward_now();
+    out2[0] = now;
+    out2[1] = F->reward_sum + (F->step > F->origin ? now : 0.0);
+  });
+}
+void or_fast_apply_reward(void* s, double reward) { FAST_DISPATCH(s, F->apply_reward(reward)); }
 void or_fast_rates(void* s, double* rates) {
   FAST_DISPATCH(s, std::copy(F->rate.begin(), F->rate.end(), rates));
 }
@@ -1201,6 +1426,22 @@ void or_lit_stats(void* s, double* out8) {
   out8[0] = (double)L->total_spikes; out8[1] = L->time; out8[2] = L->mean_rate;
   out8[3] = L->weight_mean; out8[4] = L->weight_std; out8[5] = L->lfp;
   out8[6] = (double)L->events; out8[7] = (double)L->step;
+}
+void or_lit_eligibility(void* s, double* e) {
+  Lit* L = (Lit*)s;
+  for (uint64_t q = 0; q < L->m; ++q) e[q] = L->syn[q].e;
+}
+void or_lit_reward(void* s, double* out2) {
+  Lit* L = (Lit*)s;
+  out2[0] = L->reward;
+  out2[1] = L->reward_sum;
+}
+// SimulationEngine::apply_reward, engine.rs:158-175
+void or_lit_apply_reward(void* s, double reward) {
+  Lit* L = (Lit*)s;
+  if (!L->c.rstdp) return;
+  for (LitSyn& y : L->syn)
+    if (y.elig) or_eligibility_apply(&y.e, reward, &y.weight, L->c.rstdp_lr, L->c.rstdp_wmin, L->c.rstdp_wmax);
 }
 void or_lit_destroy(void* s) { delete (Lit*)s; }
 

@@ -50,6 +50,12 @@ typedef struct or_config {
   int32_t kick_min, kick_max;
   int32_t pad3;
   double p, amp, sigma_exc, sigma_inh, kick_chance, kick_strength;
+  /* R-STDP and consolidation (engine.rs:519-563, :626-631) */
+  int32_t rstdp, cons;
+  double rstdp_lr, rstdp_wmin, rstdp_wmax, elig_tau;
+  uint64_t reward_thr;
+  double reward_decay, reward_init;
+  double cons_tau, cons_target, cons_drift;
 } or_config;
 
 typedef struct or_net {
@@ -69,6 +75,9 @@ typedef struct or_net {
   const float* m0;
   const float* h0;
   const float* n0;
+  const uint8_t* eligible;   /* may be NULL: every plastic synapse (R-STDP) */
+  const double* stp;         /* m rows (u_se, tau_rec, tau_facil, u, r) or NULL */
+  const uint8_t* has_stp;    /* may be NULL: every synapse (when stp given) */
 } or_net;
 
 /* ---- Philox4x32-10 and drive math (restated) ---- */
@@ -116,6 +125,11 @@ void or_fast_state(void* s, double* v, double* u, double* m, double* h, double* 
 void or_fast_weights(void* s, double* w);
 void or_fast_rates(void* s, double* rates);
 uint64_t or_fast_events(void* s);
+/* eligibility values (m), reward now and the sum of the reward after each
+ * step (out2), and SimulationEngine::apply_reward as the device does it */
+void or_fast_eligibility(void* s, double* e);
+void or_fast_reward(void* s, double* out2);
+void or_fast_apply_reward(void* s, double reward);
 void or_fast_destroy(void* s);
 
 void* or_lit_create(const or_config* cfg, const or_net* net, int32_t threads);
@@ -131,6 +145,9 @@ void or_lit_weights(void* s, double* w);
 void or_lit_rates(void* s, double* rates);
 uint64_t or_lit_events(void* s);
 void or_lit_stats(void* s, double* out8);
+void or_lit_eligibility(void* s, double* e);
+void or_lit_reward(void* s, double* out2);
+void or_lit_apply_reward(void* s, double reward);
 void or_lit_destroy(void* s);
 
 #ifdef __cplusplus

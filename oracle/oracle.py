@@ -27,6 +27,10 @@ class OrConfig(C.Structure):
         ("drive_kind", C.c_int32), ("kick_min", C.c_int32), ("kick_max", C.c_int32),
         ("pad3", C.c_int32), ("p", C.c_double), ("amp", C.c_double), ("sigma_exc", C.c_double),
         ("sigma_inh", C.c_double), ("kick_chance", C.c_double), ("kick_strength", C.c_double),
+        ("rstdp", C.c_int32), ("cons", C.c_int32), ("rstdp_lr", C.c_double),
+        ("rstdp_wmin", C.c_double), ("rstdp_wmax", C.c_double), ("elig_tau", C.c_double),
+        ("reward_thr", C.c_uint64), ("reward_decay", C.c_double), ("reward_init", C.c_double),
+        ("cons_tau", C.c_double), ("cons_target", C.c_double), ("cons_drift", C.c_double),
     ]
 
 
@@ -37,6 +41,7 @@ class OrNet(C.Structure):
         ("params", C.c_void_p), ("ppn", C.c_int32), ("pad", C.c_int32),
         ("inhibitory", C.c_void_p), ("is_output", C.c_void_p), ("v0", C.c_void_p),
         ("u0", C.c_void_p), ("m0", C.c_void_p), ("h0", C.c_void_p), ("n0", C.c_void_p),
+        ("eligible", C.c_void_p), ("stp", C.c_void_p), ("has_stp", C.c_void_p),
     ]
 
 
@@ -84,6 +89,9 @@ def load():
         "or_fast_weights": (None, [vp, vp]),
         "or_fast_rates": (None, [vp, vp]),
         "or_fast_events": (u64, [vp]),
+        "or_fast_eligibility": (None, [vp, vp]),
+        "or_fast_reward": (None, [vp, vp]),
+        "or_fast_apply_reward": (None, [vp, C.c_double]),
         "or_fast_destroy": (None, [vp]),
         "or_lit_create": (vp, [C.POINTER(OrConfig), C.POINTER(OrNet), C.c_int32]),
         "or_lit_step": (None, [vp, C.c_int32]),
@@ -96,6 +104,9 @@ def load():
         "or_lit_rates": (None, [vp, vp]),
         "or_lit_events": (u64, [vp]),
         "or_lit_stats": (None, [vp, vp]),
+        "or_lit_eligibility": (None, [vp, vp]),
+        "or_lit_reward": (None, [vp, vp]),
+        "or_lit_apply_reward": (None, [vp, C.c_double]),
         "or_lit_destroy": (None, [vp]),
     }
     for name, (res, args) in sig.items():
@@ -135,6 +146,15 @@ def make_config(cfg, drive):
     c.p, c.amp = f(drive.p), f(drive.amplitude)
     c.sigma_exc, c.sigma_inh = f(drive.sigma_exc), f(drive.sigma_inh)
     c.kick_chance, c.kick_strength = f(drive.kick_chance), f(drive.kick_strength)
+    g = lambda name, dflt: getattr(cfg, name, dflt)
+    c.rstdp = 1 if g("rstdp_enabled", False) else 0
+    c.rstdp_lr, c.rstdp_wmin, c.rstdp_wmax = g("rstdp_lr", 0.1), g("rstdp_w_min", 0.0), g("rstdp_w_max", 10.0)
+    c.elig_tau = g("eligibility_tau", 200.0)
+    c.reward_thr, c.reward_decay = g("reward_threshold", 5), g("reward_decay", 0.95)
+    c.reward_init = g("reward_signal", 0.0)
+    c.cons = 1 if g("consolidation_enabled", False) else 0
+    c.cons_tau, c.cons_target = g("consolidation_tau", 10000.0), g("consolidation_target", 0.5)
+    c.cons_drift = g("consolidation_drift", 0.001)
     return c
 
 
@@ -154,6 +174,8 @@ class _Base:
         nt.inhibitory, nt.is_output = _p(net.inhibitory), _p(net.is_output)
         nt.v0, nt.u0 = _p(net.v0), _p(net.u0)
         nt.m0, nt.h0, nt.n0 = _p(net.m0), _p(net.h0), _p(net.n0)
+        nt.eligible = _p(getattr(net, "eligible", None))
+        nt.stp, nt.has_stp = _p(getattr(net, "stp", None)), _p(getattr(net, "has_stp", None))
         self._nt = nt
 
     def raster(self):
@@ -177,6 +199,20 @@ class _Base:
 
     def events(self):
         return int(getattr(self.L, self.prefix + "events")(self.h))
+
+    def eligibility(self):
+        e = np.zeros(max(self.m, 1), np.float64)
+        getattr(self.L, self.prefix + "eligibility")(self.h, _p(e))
+        return e[:self.m]
+
+    def reward(self):
+        """(reward_signal now, sum of the reward after each step)."""
+        o = np.zeros(2)
+        getattr(self.L, self.prefix + "reward")(self.h, _p(o))
+        return float(o[0]), float(o[1])
+
+    def apply_reward(self, reward):
+        getattr(self.L, self.prefix + "apply_reward")(self.h, float(reward))
 
     def close(self):
         if self.h:

@@ -48,6 +48,61 @@ def lif_reference_default(n=300, seed=42, stdp=True, homeo=True, conductance=Fal
     return net, cfg, drive
 
 
+def izh_rstdp(n=2000, k=50, seed=44, wf=A.WEIGHT_F32, reward_decay=0.5, threshold=3,
+              n_out=200, rstdp_w_max=10.0, consolidation=False, homeo=False):
+    """Izhikevich + pair STDP with R-STDP: the first n_out neurons are outputs,
+    every plastic synapse carries an eligibility trace, and a fast reward
+    decay makes rewarded stretches start and stop often (both reward paths)."""
+    net, cfg, drive = izh_stdp(n=n, k=k, seed=seed, wf=wf)
+    out = np.zeros(n, np.uint8)
+    out[:n_out] = 1
+    net.is_output = out
+    cfg.rstdp_enabled = True
+    cfg.rstdp_lr = 0.5
+    cfg.rstdp_w_max = rstdp_w_max
+    cfg.reward_decay = reward_decay
+    cfg.reward_threshold = threshold
+    cfg.homeostasis_enabled = homeo
+    if consolidation:
+        cfg.consolidation_enabled = True
+    return net, cfg, drive
+
+
+def with_consolidation(cfg, tau=10000.0, target=0.5, drift=0.001):
+    cfg.consolidation_enabled = True
+    cfg.consolidation_tau, cfg.consolidation_target, cfg.consolidation_drift = tau, target, drift
+    return cfg
+
+
+def with_stp(net, frac=0.5, seed=7):
+    """Tsodyks-Markram state on a fraction of the synapses (u_se, tau_rec,
+    tau_facil, u, r), u and r away from their rest values."""
+    rng = np.random.default_rng(seed)
+    m = net.m
+    stp = np.zeros((m, 5))
+    stp[:, 0] = rng.uniform(0.1, 0.6, m)
+    stp[:, 1] = rng.uniform(50.0, 800.0, m)
+    stp[:, 2] = rng.uniform(20.0, 1000.0, m)
+    stp[:, 3] = rng.uniform(0.05, 0.9, m)
+    stp[:, 4] = rng.uniform(0.3, 1.0, m)
+    net.stp = stp
+    net.has_stp = (rng.random(m) < frac).astype(np.uint8)
+    return net
+
+
+def lif_conductance_all_types(n=1500, seed=42):
+    """Reference conductance mode with all four synapse types: excitatory
+    sources split AMPA / NMDA, inhibitory sources GABA / GABA-B."""
+    net, cfg, drive = lif_reference_default(n=n, seed=seed, stdp=False, homeo=False, conductance=True)
+    rng = np.random.default_rng(seed + 1)
+    ty = net.syn_type.copy()
+    flip = rng.random(len(ty)) < 0.4
+    ty[(ty == A.SYN_AMPA) & flip] = A.SYN_NMDA
+    ty[(ty == A.SYN_GABA) & flip] = A.SYN_GABA_B
+    net.syn_type = ty
+    return net, cfg, drive
+
+
 def hh_cond(n=1000, k=50, seed=46, dt=0.01, integrator=A.HH_RUSH_LARSEN):
     net, cfg, drive, _ = configs.hh_c4(n=n, k=k, seed=seed, integrator=integrator, dt_ms=dt)
     cfg.spike_log_capacity = 20_000_000
