@@ -20,6 +20,7 @@ max over ranks of the device time.
 host: rank 0 only, each step one simulation step of the same network.
 """
 import argparse
+import copy
 import json
 import os
 import statistics
@@ -55,7 +56,7 @@ def args_():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-extra", action="store_true", help="skip the LIF and HH configuration lines")
     p.add_argument("--no-surrogate", action="store_true", help="skip the learned HH macro-step line")
-    p.add_argument("--only", choices=["c1c4", "c3", "c5"], default=None,
+    p.add_argument("--only", choices=["c1c4", "c3", "c5", "phase2"], default=None,
                    help="run one secondary configuration alone and print its result (profiling)")
     p.add_argument("--sur-train-steps", type=int, default=12000)
     p.add_argument("--ref-warm-steps", type=int, default=300,
@@ -280,6 +281,7 @@ def run_ours(a):
         elif rank == 0:
             extra = run_extra_configs(local)
             extra["lif_batch_c3"] = batch
+            extra["izh_c2_phase2_rules"] = run_phase2_rules(local)
             if not a.no_surrogate:
                 extra["hh_surrogate_c5"] = run_surrogate_config(local, a.sur_train_steps)
 
@@ -408,6 +410,47 @@ def run_extra_configs(local):
                           "x_realtime": (steps * cfg.dt_ms) / ms,
                           "events_per_s": events / (ms / 1e3),
                           "spikes_per_step": spikes / steps}
+        out[name] = res
+    return out
+
+
+def run_phase2_rules(local, warm=500, steps=500):
+    """The rest of phase 2 on the C2 network (1M Izhikevich, 100M BF16
+    synapses, pair STDP): per-step cost with R-STDP (10% output neurons;
+    reward threshold 5, so every step is rewarded and the reward is applied
+    in the STDP walks), with an R-STDP range narrower than STDP's (every
+    rewarded step takes the full O(M) pass), with consolidation (the O(1)
+    frame) and with both."""
+    import torch
+    from neuralsim_b200 import SimulationEngine
+    net, cfg0, drive, _ = build_network(1_000_000, 100, 44)
+    net.is_output = (np.arange(net.n) < net.n // 10).astype(np.uint8)
+    variants = {
+        "stdp": {},
+        "rstdp_rewarded": {"rstdp_enabled": True},
+        "rstdp_full_pass_each_step": {"rstdp_enabled": True, "rstdp_w_max": 5.0},
+        "consolidation": {"consolidation_enabled": True},
+        "rstdp_and_consolidation": {"rstdp_enabled": True, "consolidation_enabled": True},
+    }
+    out = {"neurons": net.n, "synapses": net.m, "timed_steps": steps, "output_neurons": net.n // 10}
+    base = None
+    for name, kv in variants.items():
+        cfg = copy.deepcopy(cfg0)
+        cfg.device = local
+        for key, val in kv.items():
+            setattr(cfg, key, val)
+        eng = SimulationEngine(net, cfg, drive)
+        stream = torch.cuda.ExternalStream(eng.stream(), device=local)
+        eng.run(warm)
+        ms, spikes, events = timed_run(eng, steps, stream)
+        res = {"ns_per_step": ms * 1e6 / steps, "events_per_s": events / (ms / 1e3),
+               "spikes_per_step": spikes / steps, "schedule": eng.schedule()[0]}
+        if cfg.rstdp_enabled:
+            res["reward"] = eng.reward()[0]
+        eng.close()
+        if base is None:
+            base = res["ns_per_step"]
+        res["cost_vs_stdp"] = res["ns_per_step"] / base
         out[name] = res
     return out
 
@@ -697,6 +740,8 @@ def main():
             print(json.dumps(run_extra_configs(0)), flush=True)
         elif a.only == "c3":
             print(json.dumps(run_batch_config(0, 0, 1, None, a.c3_nets)), flush=True)
+        elif a.only == "phase2":
+            print(json.dumps(run_phase2_rules(0)), flush=True)
         else:
             print(json.dumps(run_surrogate_config(0, a.sur_train_steps, a.sur_only_1m)), flush=True)
         return

@@ -1876,6 +1876,11 @@ static ns_status set_eligibility(ns_handle* h, const uint8_t* eligible, const fl
     d.elig = ev; d.elig_flag = fl;
   }
   uint8_t* fl = const_cast<uint8_t*>(d.elig_flag);
+  // flags equal to the plastic flags: the walks, which only touch plastic
+  // synapses, need not read them
+  const int all = eligible ? 0 : 1;
+  if (d.elig_all != all) drop_graphs(h);   // captured launches carry the flag
+  d.elig_all = all;
   CK(cudaMemsetAsync(fl, 0, mp, h->st));
   CK(cudaMemsetAsync(d.elig, 0, mp * 4, h->st));
   if (h->m) {

@@ -129,7 +129,8 @@ struct NsDev {
   // R-STDP (plasticity.rs:166-221), consolidation (:269-290) and
   // short-term plasticity (:85-116)
   int rstdp, cons, fuse, plast_any;
-  float ce, rw_min, rw_max, pad_f;  // exp(-dt/eligibility_tau), R-STDP clamp
+  int elig_all;                    // every plastic synapse carries a trace (no flag reads in the walks)
+  float ce, rw_min, rw_max;        // exp(-dt/eligibility_tau), R-STDP clamp
   double reward_decay, rstdp_lr, cons_a, cons_T;
   unsigned long long reward_thr;
   float* elig;                     // eligibility values [m_pad]
@@ -876,8 +877,12 @@ __device__ __forceinline__ void row_item(const NsDev& d, const StepCtx& c, uint3
       bool el[4] = {false, false, false, false};
       float evl[4] = {0.f, 0.f, 0.f, 0.f};
       if (EXT && d.rstdp && (pl[0] | pl[1] | pl[2] | pl[3])) {
-        const uchar4 f4 = *reinterpret_cast<const uchar4*>(d.elig_flag + e0);
-        el[0] = pl[0] && f4.x; el[1] = pl[1] && f4.y; el[2] = pl[2] && f4.z; el[3] = pl[3] && f4.w;
+        if (d.elig_all) {
+          el[0] = pl[0]; el[1] = pl[1]; el[2] = pl[2]; el[3] = pl[3];
+        } else {
+          const uchar4 f4 = *reinterpret_cast<const uchar4*>(d.elig_flag + e0);
+          el[0] = pl[0] && f4.x; el[1] = pl[1] && f4.y; el[2] = pl[2] && f4.z; el[3] = pl[3] && f4.w;
+        }
         if (el[0] | el[1] | el[2] | el[3]) {
           const float4 v4 = *reinterpret_cast<const float4*>(d.elig + e0);
           evl[0] = v4.x; evl[1] = v4.y; evl[2] = v4.z; evl[3] = v4.w;
@@ -965,7 +970,7 @@ __device__ __forceinline__ void ltd_item(const NsDev& d, const StepCtx& c, uint3
       float st = w1;
       if (EXT) {
         const uint32_t pos = sp[u].y;
-        const bool el = d.rstdp && d.elig_flag[pos];
+        const bool el = d.rstdp && (d.elig_all || d.elig_flag[pos]);
         float evq = el ? d.elig[pos] : 0.0f;
         if (el) evq = evq * d.ce + dm;   // EligibilityTrace::update, engine.rs:531-533
         st = ext_store<BF16>(d, fr, mode, w1, el, evq);

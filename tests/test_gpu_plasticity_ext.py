@@ -57,6 +57,23 @@ def test_rstdp_schedules_identical(lib, sched):
     assert np.array_equal(eng.eligibility().astype(np.float64), o.eligibility())
 
 
+def test_rstdp_subset_eligible(lib):
+    # half of the plastic synapses carry an eligibility trace (with_rstdp on
+    # some synapses only): the walks read the per-synapse flags
+    net, cfg, drive = nets.izh_rstdp(n=4000, k=60)
+    rng = np.random.default_rng(3)
+    net.eligible = (rng.random(net.m) < 0.5).astype(np.uint8)
+    eng = SimulationEngine(net, cfg, drive)
+    eng.run(300)
+    o = FastOracle(net, cfg, drive, precision=32)
+    o.step(300)
+    assert nets.rasters_equal(eng.read_raster(0, 300), o.raster())
+    assert same_weights(eng, o)
+    e = eng.eligibility()
+    assert np.array_equal(e.astype(np.float64), o.eligibility())
+    assert not np.any(e[net.eligible == 0])
+
+
 def test_rstdp_full_pass_config(lib):
     # R-STDP range narrower than STDP's: every rewarded step takes the full pass
     net, cfg, drive = nets.izh_rstdp(n=4000, k=60, rstdp_w_max=4.0)
