@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <array>
 #include <map>
 #include <string>
 #include <vector>
@@ -67,6 +68,8 @@ struct ns_handle {
   std::vector<void*> ext_allocs;    // elig + elig_flag (R-STDP)
   std::vector<void*> stp_allocs;    // stp_f
   bool win_ran = false;             // windowed steps ran (reward not maintained)
+  uint8_t* pidx_buf = nullptr;      // parameter dictionary buffers (d.pidx / d.ptab when used)
+  float* ptab_buf = nullptr;
 };
 
 namespace {
@@ -519,8 +522,9 @@ typedef void (*neuron_fn)(NsDev, uint32_t);
 typedef void (*prop_fn)(NsDev, uint32_t);
 typedef void (*ltd_fn)(NsDev, uint32_t);
 
-neuron_fn pick_neuron(uint32_t model, uint32_t mode) {
-#define NSN(MO, MD) if (model == MO && mode == MD) return ns::k_neuron<MO, MD>;
+neuron_fn pick_neuron(uint32_t model, uint32_t mode, bool pt) {
+#define NSN(MO, MD) \
+  if (model == MO && mode == MD) return pt ? ns::k_neuron<MO, MD, true> : ns::k_neuron<MO, MD, false>;
   NSN(0, 0) NSN(0, 1) NSN(0, 2) NSN(0, 3) NSN(0, 4)
   NSN(1, 0) NSN(1, 1) NSN(1, 2) NSN(1, 3) NSN(1, 4)
   NSN(2, 0) NSN(2, 1) NSN(2, 2) NSN(2, 3) NSN(2, 4)
@@ -585,7 +589,7 @@ uint32_t sched_of(const ns_handle* h) { return h->sched == 0 ? 1u : h->sched; }
 // step j runs on the side stream beside the neuron kernel of step j+1 and the
 // row walk of step j+1 waits for it; *ltd_pending tracks the open branch.
 cudaError_t enqueue_step(ns_handle* h, uint32_t j, bool* ltd_pending, uint32_t sched) {
-  neuron_fn nf = pick_neuron(h->cfg.model, h->cfg.input_mode);
+  neuron_fn nf = pick_neuron(h->cfg.model, h->cfg.input_mode, h->d.pidx != nullptr);
   nf<<<h->ntiles, ns::kThreads, 0, h->st>>>(h->d, j);
   if (*ltd_pending) {
     cudaError_t e = cudaStreamWaitEvent(h->st, h->ev_ltd, 0);
@@ -1195,6 +1199,7 @@ ns_status ns_upload_neurons(ns_handle* h, const ns_neuron_soa* s) {
     for (int t = 0; t < 4; ++t) DA(d.G[t], np)
     DA(d.bitmap, np / 32 + 2) DA(d.spk, 2 * np)
     DA(d.tile_cnt, 2 * ((uint64_t)h->ntiles + 1)) DA(d.tile_off, 2 * ((uint64_t)h->ntiles + 1))
+    DA(h->pidx_buf, np) DA(h->ptab_buf, 256 * 8)
 #undef DA
   }
   auto up = [&](void* dst, const void* src, size_t bytes) {
@@ -1207,6 +1212,38 @@ ns_status ns_upload_neurons(ns_handle* h, const ns_neuron_soa* s) {
   CK(up(d.pre, pre.data(), np * 4)); CK(up(d.post, post.data(), np * 4));
   CK(up(d.last, last.data(), np * 8));
   for (int q = 0; q < npar; ++q) CK(up(d.par[q], par[q].data(), np * 4));
+  {
+    // parameter dictionary: at most 256 distinct rows (by bit pattern) give
+    // the neuron kernel a 1-byte index per neuron instead of its rows
+    std::map<std::array<uint32_t, 8>, uint32_t> rows;
+    std::vector<uint8_t> pidx(np);
+    std::vector<float> ptab;
+    bool ok = true;
+    for (uint64_t i = 0; i < np && ok; ++i) {
+      std::array<uint32_t, 8> key{};
+      for (int q = 0; q < npar; ++q) std::memcpy(&key[q], &par[q][i], 4);
+      if (model == NS_MODEL_LIF) std::memcpy(&key[7], &rsteps[i], 4);
+      auto it = rows.find(key);
+      if (it == rows.end()) {
+        if (rows.size() == 256) { ok = false; break; }
+        it = rows.emplace(key, (uint32_t)rows.size()).first;
+        const size_t at = ptab.size();
+        ptab.resize(at + 8);
+        std::memcpy(ptab.data() + at, key.data(), 32);
+      }
+      pidx[i] = (uint8_t)it->second;
+    }
+    const uint8_t* want = ok ? h->pidx_buf : nullptr;
+    if (want != d.pidx) drop_graphs(h);  // the kernel variant changes
+    d.pidx = want;
+    d.ptab = ok ? h->ptab_buf : nullptr;
+    d.ptab_rows = ok ? (uint32_t)rows.size() : 0u;
+    if (ok) {
+      CK(up(h->pidx_buf, pidx.data(), np));
+      CK(up(h->ptab_buf, ptab.data(), ptab.size() * 4));
+      CK(cudaStreamSynchronize(h->st));
+    }
+  }
   if (s->conductance) {
     std::vector<float> g(np, 0.0f);
     for (int t = 0; t < 4; ++t) {
@@ -1626,7 +1663,7 @@ ns_status ns_step_traced(ns_handle* h, uint64_t* pos_out, uint64_t cap, uint64_t
     return st;
   }
   NsDev d = h->d;
-  neuron_fn nf = pick_neuron(h->cfg.model, h->cfg.input_mode);
+  neuron_fn nf = pick_neuron(h->cfg.model, h->cfg.input_mode, h->d.pidx != nullptr);
   const bool ext = ext_on(h);
   prop_fn pf = pick_prop(h->cfg.input_mode, h->cfg.weight_format, ext);
   nf<<<h->ntiles, ns::kThreads, 0, h->st>>>(d, 0);
@@ -2139,7 +2176,7 @@ ns_status ns_profile_steps(ns_handle* h, uint32_t n_steps, double* kernel_ms, ui
   if (r) return r;
   CK(cudaSetDevice(h->dev));
   fill_scalars(h);
-  neuron_fn nf = pick_neuron(h->cfg.model, h->cfg.input_mode);
+  neuron_fn nf = pick_neuron(h->cfg.model, h->cfg.input_mode, h->d.pidx != nullptr);
   const bool ext = ext_on(h);
   prop_fn pf = pick_prop(h->cfg.input_mode, h->cfg.weight_format, ext);
   ltd_fn lf = pick_ltd(h->cfg.weight_format, ext);

@@ -133,6 +133,14 @@ struct NsDev {
   float ce, rw_min, rw_max;        // exp(-dt/eligibility_tau), R-STDP clamp
   double reward_decay, rstdp_lr, cons_a, cons_T;
   unsigned long long reward_thr;
+  // parameter dictionary: when a network has at most 256 distinct
+  // parameter rows, the neuron kernel reads a 1-byte index per neuron and
+  // the row from a table in shared memory (8 floats per row: the model's
+  // parameter arrays in par[] order, the LIF refractory steps as int bits
+  // in column 7)
+  const uint8_t* pidx;
+  const float* ptab;
+  uint32_t ptab_rows;
   float* elig;                     // eligibility values [m_pad]
   const uint8_t* elig_flag;        // synapse carries an eligibility trace [m_pad]
   const float* stp_f;              // STP factor per synapse, or null
@@ -395,8 +403,9 @@ __global__ void k_setup(NsDev d, uint32_t jstep) {
 // own slice of the spike buffer (warp ballots + a 32-entry scan), so no tile
 // waits for another; the last tile to finish does the step's bookkeeping.
 // ---------------------------------------------------------------------------
-template <int MODEL, int MODE>
+template <int MODEL, int MODE, bool PT>
 __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
+  __shared__ float s_tab[PT ? 256 * 8 : 1];
   __shared__ uint32_t s_off[kPairs * kWarps];
   __shared__ uint32_t s_me[kPairs * kWarps], s_mo[kPairs * kWarps];
   __shared__ uint32_t s_total;
@@ -418,6 +427,8 @@ __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
   float2* const rec_k = d.rec + par_k * d.n_pad;
 
   if (tid == 0) s_nk = 0;
+  if (PT)
+    for (uint32_t q = tid; q < d.ptab_rows * 8u; q += kThreads) s_tab[q] = __ldg(d.ptab + q);
   __syncthreads();
   if (d.drive_kind == 1 && warp == 1) {
     // reference-shaped global kicks (engine.rs:280-287): lane j computes kick j
@@ -466,15 +477,24 @@ __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
       st[0].I = c.x; st[1].I = c.y;
     }
     float par[2][7];
-#pragma unroll
-    for (int q = 0; q < NP; ++q) {
-      const float2 pv = *reinterpret_cast<const float2*>(d.par[q] + i0);
-      par[0][q] = pv.x; par[1][q] = pv.y;
-    }
     int rs[2] = {0, 0};
-    if (MODEL == 0) {
-      const int2 r2 = *reinterpret_cast<const int2*>(d.refr_steps + i0);
-      rs[0] = r2.x; rs[1] = r2.y;
+    if (PT) {
+      const uchar2 ix = *reinterpret_cast<const uchar2*>(d.pidx + i0);
+      const float* t0 = s_tab + 8u * ix.x;
+      const float* t1 = s_tab + 8u * ix.y;
+#pragma unroll
+      for (int q = 0; q < NP; ++q) { par[0][q] = t0[q]; par[1][q] = t1[q]; }
+      if (MODEL == 0) { rs[0] = __float_as_int(t0[7]); rs[1] = __float_as_int(t1[7]); }
+    } else {
+#pragma unroll
+      for (int q = 0; q < NP; ++q) {
+        const float2 pv = *reinterpret_cast<const float2*>(d.par[q] + i0);
+        par[0][q] = pv.x; par[1][q] = pv.y;
+      }
+      if (MODEL == 0) {
+        const int2 r2 = *reinterpret_cast<const int2*>(d.refr_steps + i0);
+        rs[0] = r2.x; rs[1] = r2.y;
+      }
     }
     longlong2 accv[NT];
 #pragma unroll

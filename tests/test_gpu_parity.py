@@ -67,6 +67,27 @@ def test_izh_stdp_raster_weights_bit_exact_1s(lib, wf):
     assert np.count_nonzero(st["w"] != net.w) > 1000
 
 
+@pytest.mark.parametrize("distinct_rows", [2, 5000])
+def test_parameter_rows_dictionary_and_per_neuron(lib, distinct_rows):
+    # up to 256 distinct parameter rows: the neuron kernel reads a 1-byte
+    # index and a shared-memory table; more rows: the per-neuron arrays.
+    # Both give the oracle's results bit for bit.
+    net, cfg, drive = nets.izh_stdp(n=20_000, k=60, wf=A.WEIGHT_F32)
+    if distinct_rows > 256:
+        rng = np.random.default_rng(11)
+        p = net.params.copy()
+        p[:, 2] = p[:, 2] + rng.uniform(-2.0, 2.0, net.n).astype(np.float32)   # reset c
+        net.params = p
+    assert len(np.unique(net.params, axis=0)) >= min(distinct_rows, 2)
+    eng = gpu_run(net, cfg, drive, 400)
+    o = FastOracle(net, cfg, drive, precision=32)
+    o.step(400)
+    assert nets.rasters_equal(eng.read_raster(0, 400), o.raster())
+    st = eng.download_state()
+    assert np.array_equal(st["v"].astype(np.float64), o.state()["v"])
+    assert np.array_equal(st["params"], net.params)
+
+
 @pytest.mark.parametrize("sched", [1, 2, 3, 4])
 def test_step_schedules_identical(lib, sched):
     # fused, split (LTD beside the next neuron update) and fused-4 schedules
