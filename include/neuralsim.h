@@ -368,6 +368,35 @@ ns_status ns_get_stream(ns_handle* h, void** stream);
  * homeostasis kernels to kernel_ms[4] / launches[4]. Same numerics as ns_step. */
 ns_status ns_profile_steps(ns_handle* h, uint32_t n_steps, double* kernel_ms, uint64_t* launches);
 
+/* --- single-network sharding (one process per GPU; no counterpart in the
+ *     reference, which runs one network on one device) ------------------
+ * A network's neurons are split over `world` ranks by 2048-neuron tiles:
+ * rank r updates neurons [lo, hi) (ns_shard_range) and holds the synapses
+ * whose target is one of them. Its CSR keeps every source row (row_ptr over
+ * all n neurons) with global target indices, all inside [lo, hi); every
+ * rank uploads the full neuron SoA. Each step the ranks all-gather the
+ * step's spike bitmap (n/8 bytes in all); each rank then rebuilds the other
+ * ranks' spike lists and source traces, walks every spiking row into its
+ * own targets and runs LTD and homeostasis for its own targets. The union
+ * of the ranks' rasters, owned states and weights equals the one-GPU run
+ * bit for bit. Windowed stepping, batches, traced and profiled steps are
+ * single-GPU only; the schedule is fixed (fused, 4 blocks/SM, unless
+ * step_schedule names one). State outside [lo, hi) is not the rank's. */
+ns_status ns_shard_range(uint64_t n, uint32_t rank, uint32_t world, uint64_t* lo, uint64_t* hi);
+/* Before the uploads. */
+ns_status ns_shard_configure(ns_handle* h, uint32_t rank, uint32_t world);
+/* NCCL all-gather inside the step graphs: rank 0 makes the id, every rank
+ * receives it (e.g. over the job's process group) and initialises; ns_step
+ * then steps all ranks in lockstep. NCCL is loaded at run time. */
+ns_status ns_shard_nccl_unique_id(char id_out[128]);
+ns_status ns_shard_nccl_init(ns_handle* h, const char id[128]);
+/* Without NCCL (ranks on one GPU or driven by one process): per step,
+ * ns_shard_step_begin on every rank, ns_shard_copy_bitmap(dst, src) for
+ * every ordered pair of ranks, then ns_shard_step_end on every rank. */
+ns_status ns_shard_step_begin(ns_handle* h);
+ns_status ns_shard_copy_bitmap(ns_handle* dst, ns_handle* src);
+ns_status ns_shard_step_end(ns_handle* h);
+
 /* --- allocation-free step (no counterpart in the reference) -------------
  * For callers that cannot allocate device memory where they step neurons:
  * one recorded into their own CUDA stream capture (cudaMalloc cannot be

@@ -133,6 +133,14 @@ SIGNATURES = {
     "ns_get_reward": (C.c_int32, [_P, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "ns_set_reward": (C.c_int32, [_P, C.c_double]),
     "ns_upload_stp": (C.c_int32, [_P, C.c_void_p, C.c_void_p]),
+    "ns_shard_range": (C.c_int32, [C.c_uint64, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint64),
+                                   C.POINTER(C.c_uint64)]),
+    "ns_shard_configure": (C.c_int32, [_P, C.c_uint32, C.c_uint32]),
+    "ns_shard_nccl_unique_id": (C.c_int32, [C.c_void_p]),
+    "ns_shard_nccl_init": (C.c_int32, [_P, C.c_void_p]),
+    "ns_shard_step_begin": (C.c_int32, [_P]),
+    "ns_shard_copy_bitmap": (C.c_int32, [_P, _P]),
+    "ns_shard_step_end": (C.c_int32, [_P]),
     "ns_step_traced": (C.c_int32, [_P, _P, C.c_uint64, _U64P]),
     "ns_launch_count": (C.c_int32, [_P, _U64P]),
     "ns_get_schedule": (C.c_int32, [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_double)]),

@@ -3,6 +3,8 @@
 // CUDA-graph step loop. Replaces GpuBackend (src/simulation/gpu_backend.rs).
 #include <cuda_runtime.h>
 #include <cub/cub.cuh>
+#include <dlfcn.h>
+#include <nccl.h>
 
 #include <algorithm>
 #include <cmath>
@@ -70,11 +72,53 @@ struct ns_handle {
   bool win_ran = false;             // windowed steps ran (reward not maintained)
   uint8_t* pidx_buf = nullptr;      // parameter dictionary buffers (d.pidx / d.ptab when used)
   float* ptab_buf = nullptr;
+  // single-network sharding: rank / world (world 0 or 1 = one GPU); the
+  // spike bitmap exchange is an NCCL all-gather inside the step graph, or
+  // done by the caller between ns_shard_step_begin and ns_shard_step_end
+  uint32_t shard_rank = 0, shard_world = 0;
+  ncclComm_t nccl = nullptr;
 };
 
 namespace {
 
 thread_local std::string g_err;
+
+// NCCL is loaded when a sharded handle first needs it (the process may
+// already hold the NCCL that its framework loaded; the same library is
+// then shared), so the library has no link-time dependency on it.
+struct NcclApi {
+  bool tried = false, ok = false;
+  ncclResult_t (*get_unique_id)(ncclUniqueId*) = nullptr;
+  ncclResult_t (*comm_init_rank)(ncclComm_t*, int, ncclUniqueId, int) = nullptr;
+  ncclResult_t (*all_gather)(const void*, void*, size_t, ncclDataType_t, ncclComm_t, cudaStream_t) = nullptr;
+  ncclResult_t (*comm_destroy)(ncclComm_t) = nullptr;
+  const char* (*error_string)(ncclResult_t) = nullptr;
+};
+NcclApi g_nccl;
+
+bool nccl_load() {
+  if (g_nccl.tried) return g_nccl.ok;
+  g_nccl.tried = true;
+  void* lib = dlopen("libnccl.so.2", RTLD_NOW | RTLD_GLOBAL);
+  if (!lib) lib = dlopen("libnccl.so", RTLD_NOW | RTLD_GLOBAL);
+  if (!lib) return false;
+  g_nccl.get_unique_id = (decltype(g_nccl.get_unique_id))dlsym(lib, "ncclGetUniqueId");
+  g_nccl.comm_init_rank = (decltype(g_nccl.comm_init_rank))dlsym(lib, "ncclCommInitRank");
+  g_nccl.all_gather = (decltype(g_nccl.all_gather))dlsym(lib, "ncclAllGather");
+  g_nccl.comm_destroy = (decltype(g_nccl.comm_destroy))dlsym(lib, "ncclCommDestroy");
+  g_nccl.error_string = (decltype(g_nccl.error_string))dlsym(lib, "ncclGetErrorString");
+  g_nccl.ok = g_nccl.get_unique_id && g_nccl.comm_init_rank && g_nccl.all_gather &&
+              g_nccl.comm_destroy && g_nccl.error_string;
+  return g_nccl.ok;
+}
+
+// tiles of a network of n neurons split over `world` ranks: a whole number
+// of 2048-neuron tiles per rank
+uint32_t tiles_for(uint64_t n, uint32_t world) {
+  uint64_t t = (n + ns::kTile - 1) / ns::kTile;
+  if (world > 1) t = (t + world - 1) / world * world;
+  return (uint32_t)t;
+}
 
 ns_status fail(ns_handle* h, ns_status s, const std::string& msg) {
   if (h) h->err = msg; else g_err = msg;
@@ -431,6 +475,9 @@ void fill_scalars(ns_handle* h) {
   const ns_config& c = h->cfg;
   d.n = h->n; d.n_pad = h->n_pad; d.m = h->m;
   d.D = c.delay_steps; d.ntiles = h->ntiles;
+  const uint32_t world = h->shard_world > 1 ? h->shard_world : 1u;
+  d.tiles_own = h->ntiles / world;
+  d.tile0 = h->shard_rank * d.tiles_own;
   d.dt = c.dt_ms; d.dt_f = (float)c.dt_ms;
   d.decay_I = (float)c.current_decay;
   d.stdp = c.stdp_enabled ? 1 : 0;
@@ -585,12 +632,29 @@ bool overlap_ltd(const ns_handle* h) {
 // schedule a step uses (fused at 6 blocks/SM until the autotuner decides)
 uint32_t sched_of(const ns_handle* h) { return h->sched == 0 ? 1u : h->sched; }
 
+// In-place all-gather of the step's spike bitmap: rank r owns words
+// [r*W, (r+1)*W), W = 64 words per tile times the tiles of a rank.
+cudaError_t shard_exchange(ns_handle* h) {
+  if (!h->nccl) return cudaErrorNotReady;
+  const size_t words = (size_t)h->d.tiles_own * (ns::kTile / 32);
+  uint32_t* bm = h->d.bitmap;
+  ncclResult_t r = g_nccl.all_gather(bm + (size_t)h->shard_rank * words, bm, words, ncclUint32,
+                                     h->nccl, h->st);
+  return r == ncclSuccess ? cudaSuccess : cudaErrorUnknown;
+}
+
 // Enqueues one step (graph-node index j). With overlap, the LTD kernel of
 // step j runs on the side stream beside the neuron kernel of step j+1 and the
 // row walk of step j+1 waits for it; *ltd_pending tracks the open branch.
 cudaError_t enqueue_step(ns_handle* h, uint32_t j, bool* ltd_pending, uint32_t sched) {
   neuron_fn nf = pick_neuron(h->cfg.model, h->cfg.input_mode, h->d.pidx != nullptr);
-  nf<<<h->ntiles, ns::kThreads, 0, h->st>>>(h->d, j);
+  nf<<<h->d.tiles_own, ns::kThreads, 0, h->st>>>(h->d, j);
+  if (h->shard_world > 1) {
+    // every rank's spike bitmap words, then the other ranks' tiles rebuilt
+    cudaError_t e = shard_exchange(h);
+    if (e != cudaSuccess) return e;
+    ns::k_shard_merge<<<h->ntiles - h->d.tiles_own, ns::kThreads, 0, h->st>>>(h->d, j);
+  }
   if (*ltd_pending) {
     cudaError_t e = cudaStreamWaitEvent(h->st, h->ev_ltd, 0);
     if (e != cudaSuccess) return e;
@@ -632,7 +696,7 @@ cudaError_t join_ltd(ns_handle* h, bool* ltd_pending) {
 uint64_t launches_per_step(const ns_handle* h, uint32_t sched) {
   const bool split = sched == 2 || sched == 4;
   return 2u + ((split && h->cfg.stdp_enabled) ? 1u : 0u) + (h->cfg.homeostasis_enabled ? 1u : 0u) +
-         (tail_on(h) ? 2u : 0u);
+         (tail_on(h) ? 2u : 0u) + (h->shard_world > 1 ? 1u : 0u);
 }
 
 typedef void (*window_fn)(NsDev, uint32_t, uint32_t);
@@ -759,6 +823,11 @@ uint32_t kTuneWindow = 100;
 ns_status autotune_window(ns_handle* h, uint32_t budget, uint32_t* used);
 ns_status autotune(ns_handle* h, uint32_t budget, uint32_t* used) {
   *used = 0;
+  if (h->shard_world > 1) {
+    // ranks step in lockstep through their collectives: no timed candidates
+    if (h->sched == 0) h->sched = 3;
+    return NS_OK;
+  }
   if (h->win) {
     h->sched = 1;
     if (h->cfg.window_steps != 0) return NS_OK;
@@ -909,6 +978,8 @@ ns_status ready(ns_handle* h) {
   if (h->n == 0) return fail(h, NS_ERR_STATE, "empty network");
   if (h->sur_on && h->drive.kind != NS_DRIVE_NONE && h->drive.kind != NS_DRIVE_POISSON_CONDUCTANCE)
     return fail(h, NS_ERR_UNSUPPORTED, "the surrogate macro-step takes no drive or the Poisson conductance drive");
+  if (h->shard_world > 1 && h->n_nets)
+    return fail(h, NS_ERR_UNSUPPORTED, "a sharded handle holds one network");
   if (h->n_nets && h->cfg.rstdp_enabled)
     return fail(h, NS_ERR_UNSUPPORTED, "R-STDP's reward is global to one network; batches do not take it");
   if (h->n_nets && h->drive.kind == NS_DRIVE_REF_UNIFORM)
@@ -1077,6 +1148,7 @@ ns_status ns_destroy(ns_handle* h) {
   free_bag(h->sur_allocs);
   free_bag(h->ext_allocs);
   free_bag(h->stp_allocs);
+  if (h->nccl) g_nccl.comm_destroy(h->nccl);
   if (h->ctl) cudaFree(h->ctl);
   if (h->st2) cudaStreamSynchronize(h->st2);
   if (h->ev_rows) cudaEventDestroy(h->ev_rows);
@@ -1136,7 +1208,7 @@ ns_status ns_upload_neurons(ns_handle* h, const ns_neuron_soa* s) {
   }
   const uint64_t n = s->n;
   h->n = n;
-  h->ntiles = (uint32_t)((n + ns::kTile - 1) / ns::kTile);
+  h->ntiles = tiles_for(n, h->shard_world);
   h->n_pad = (uint64_t)h->ntiles * ns::kTile;
   const uint64_t np = h->n_pad;
   const uint32_t model = h->cfg.model;
@@ -1309,7 +1381,7 @@ static ns_status alloc_dynamic(ns_handle* h) {
   }
   d.trace_pos = nullptr; d.trace_off = nullptr; d.trace_cap = 0;
   // windowed stepping buffers
-  h->win = window_len(c);
+  h->win = h->shard_world > 1 ? 0u : window_len(c);
   h->wcur = h->win;
   h->next_tune_step = 0;
   d.inbits = nullptr; d.seg_cnt = nullptr; d.seg_lst = nullptr; d.seg_off = nullptr;
@@ -1350,6 +1422,13 @@ ns_status ns_upload_csr(ns_handle* h, uint64_t n, uint64_t m, const uint64_t* ro
   if (h->have_neurons && n != h->n) return fail(h, NS_ERR_INVALID_ARG, "n differs from the neuron upload");
   if (m >= 0xFFFFFFFFull) return fail(h, NS_ERR_UNSUPPORTED, "m must be < 2^32");
   if (row_ptr[0] != 0 || row_ptr[n] != m) return fail(h, NS_ERR_CSR, "row_ptr[0] must be 0 and row_ptr[n] == m");
+  if (h->shard_world > 1) {
+    // a rank holds only synapses onto its own neurons
+    uint64_t lo = 0, hi = 0;
+    ns_shard_range(n, h->shard_rank, h->shard_world, &lo, &hi);
+    for (uint64_t e = 0; e < m; ++e)
+      if (col[e] < lo || col[e] >= hi) return fail(h, NS_ERR_CSR, "a sharded rank's synapse targets a neuron it does not own");
+  }
   CK(cudaSetDevice(h->dev));
   CK(cudaStreamSynchronize(h->st));
   CK(cudaStreamSynchronize(h->st2));
@@ -1364,7 +1443,7 @@ ns_status ns_upload_csr(ns_handle* h, uint64_t n, uint64_t m, const uint64_t* ro
   h->m_pad = round_up(std::max<uint64_t>(m, 4), 4) + 4;
   if (!h->have_neurons) {
     h->n = n;
-    h->ntiles = (uint32_t)((n + ns::kTile - 1) / ns::kTile);
+    h->ntiles = tiles_for(n, h->shard_world);
     h->n_pad = (uint64_t)h->ntiles * ns::kTile;
   }
   ns_status st;
@@ -1625,6 +1704,8 @@ ns_status ns_step(ns_handle* h, uint32_t n_steps, ns_step_stats* out) {
   if (!h) return NS_ERR_NULL_HANDLE;
   ns_status r = ready(h);
   if (r) return r;
+  if (h->shard_world > 1 && !h->nccl)
+    return fail(h, NS_ERR_STATE, "sharded handle without NCCL: step with ns_shard_step_begin / ns_shard_step_end");
   CK(cudaSetDevice(h->dev));
   fill_scalars(h);
   ns::Ctl before{};
@@ -1652,6 +1733,7 @@ ns_status ns_step_traced(ns_handle* h, uint64_t* pos_out, uint64_t cap, uint64_t
   if (!h) return NS_ERR_NULL_HANDLE;
   ns_status r = ready(h);
   if (r) return r;
+  if (h->shard_world > 1) return fail(h, NS_ERR_UNSUPPORTED, "traced steps run on one GPU");
   if (!n_events || (cap && !pos_out)) return fail(h, NS_ERR_INVALID_ARG, "null output");
   CK(cudaSetDevice(h->dev));
   fill_scalars(h);
@@ -1666,7 +1748,7 @@ ns_status ns_step_traced(ns_handle* h, uint64_t* pos_out, uint64_t cap, uint64_t
   neuron_fn nf = pick_neuron(h->cfg.model, h->cfg.input_mode, h->d.pidx != nullptr);
   const bool ext = ext_on(h);
   prop_fn pf = pick_prop(h->cfg.input_mode, h->cfg.weight_format, ext);
-  nf<<<h->ntiles, ns::kThreads, 0, h->st>>>(d, 0);
+  nf<<<h->d.tiles_own, ns::kThreads, 0, h->st>>>(d, 0);
   if (tail_on(h)) ns::k_setup<<<1, 32, 0, h->st>>>(d, 0);
   ns::k_trace_offsets<<<1, 32, 0, h->st>>>(d, off);
   d.trace_pos = pos; d.trace_off = off; d.trace_cap = cap;
@@ -2174,6 +2256,7 @@ ns_status ns_profile_steps(ns_handle* h, uint32_t n_steps, double* kernel_ms, ui
   if (!kernel_ms || !launches) return fail(h, NS_ERR_INVALID_ARG, "null output");
   ns_status r = ready(h);
   if (r) return r;
+  if (h->shard_world > 1) return fail(h, NS_ERR_UNSUPPORTED, "kernel profiles run on one GPU");
   CK(cudaSetDevice(h->dev));
   fill_scalars(h);
   neuron_fn nf = pick_neuron(h->cfg.model, h->cfg.input_mode, h->d.pidx != nullptr);
@@ -2188,7 +2271,7 @@ ns_status ns_profile_steps(ns_handle* h, uint32_t n_steps, double* kernel_ms, ui
   for (uint32_t j = 0; j < n_steps; ++j) {
     cudaEvent_t* e = &ev[(size_t)j * 8];
     CK(cudaEventRecord(e[0], h->st));
-    nf<<<h->ntiles, ns::kThreads, 0, h->st>>>(h->d, j);
+    nf<<<h->d.tiles_own, ns::kThreads, 0, h->st>>>(h->d, j);
     if (tail_on(h)) ns::k_setup<<<1, 32, 0, h->st>>>(h->d, j);
     CK(cudaEventRecord(e[1], h->st));
     CK(cudaEventRecord(e[2], h->st));
@@ -2217,6 +2300,108 @@ ns_status ns_profile_steps(ns_handle* h, uint32_t n_steps, double* kernel_ms, ui
     }
   for (auto& e : ev) cudaEventDestroy(e);
   h->launches += nl + 1 + (tail_on(h) ? (h->cfg.stdp_enabled ? 2u : 1u) * (uint64_t)n_steps : 0);
+  return check_device_status(h);
+}
+
+// --- single-network sharding ------------------------------------------
+ns_status ns_shard_range(uint64_t n, uint32_t rank, uint32_t world, uint64_t* lo, uint64_t* hi) {
+  if (!lo || !hi || world == 0 || rank >= world || n == 0) return NS_ERR_INVALID_ARG;
+  const uint64_t per = (uint64_t)(tiles_for(n, world) / world) * ns::kTile;
+  *lo = std::min<uint64_t>(n, (uint64_t)rank * per);
+  *hi = std::min<uint64_t>(n, (uint64_t)(rank + 1) * per);
+  return NS_OK;
+}
+
+ns_status ns_shard_configure(ns_handle* h, uint32_t rank, uint32_t world) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  if (world == 0 || rank >= world) return fail(h, NS_ERR_INVALID_ARG, "rank must be < world");
+  if (h->have_neurons || h->have_csr) return fail(h, NS_ERR_STATE, "configure the shard before the uploads");
+  h->shard_rank = rank;
+  h->shard_world = world;
+  if (world > 1 && h->sched == 0) h->sched = 3;
+  return NS_OK;
+}
+
+ns_status ns_shard_nccl_unique_id(char id_out[128]) {
+  if (!id_out) return NS_ERR_INVALID_ARG;
+  if (!nccl_load()) return fail(nullptr, NS_ERR_UNSUPPORTED, "NCCL (libnccl.so.2) could not be loaded");
+  ncclUniqueId id;
+  ncclResult_t r = g_nccl.get_unique_id(&id);
+  if (r != ncclSuccess) return fail(nullptr, NS_ERR_CUDA, g_nccl.error_string(r));
+  static_assert(sizeof(id) == 128, "ncclUniqueId is 128 bytes");
+  std::memcpy(id_out, &id, 128);
+  return NS_OK;
+}
+
+ns_status ns_shard_nccl_init(ns_handle* h, const char id[128]) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  if (!id) return fail(h, NS_ERR_INVALID_ARG, "null id");
+  if (h->shard_world == 0) return fail(h, NS_ERR_STATE, "ns_shard_configure first");
+  if (h->nccl) return fail(h, NS_ERR_STATE, "NCCL already initialised");
+  if (!nccl_load()) return fail(h, NS_ERR_UNSUPPORTED, "NCCL (libnccl.so.2) could not be loaded");
+  CK(cudaSetDevice(h->dev));
+  ncclUniqueId uid;
+  std::memcpy(&uid, id, 128);
+  ncclComm_t comm = nullptr;
+  ncclResult_t r = g_nccl.comm_init_rank(&comm, (int)h->shard_world, uid, (int)h->shard_rank);
+  if (r != ncclSuccess) return fail(h, NS_ERR_CUDA, std::string("ncclCommInitRank: ") + g_nccl.error_string(r));
+  h->nccl = comm;
+  drop_graphs(h);
+  return NS_OK;
+}
+
+ns_status ns_shard_step_begin(ns_handle* h) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  ns_status r = ready(h);
+  if (r) return r;
+  if (h->shard_world == 0) return fail(h, NS_ERR_STATE, "not a sharded handle");
+  CK(cudaSetDevice(h->dev));
+  fill_scalars(h);
+  if (h->sched == 0) h->sched = 3;
+  neuron_fn nf = pick_neuron(h->cfg.model, h->cfg.input_mode, h->d.pidx != nullptr);
+  nf<<<h->d.tiles_own, ns::kThreads, 0, h->st>>>(h->d, 0);
+  h->launches += 1;
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(h->st));
+  return NS_OK;
+}
+
+ns_status ns_shard_copy_bitmap(ns_handle* dst, ns_handle* src) {
+  if (!dst || !src) return NS_ERR_NULL_HANDLE;
+  ns_handle* h = dst;
+  if (dst->shard_world != src->shard_world || dst->n_pad != src->n_pad || dst->shard_world < 2)
+    return fail(dst, NS_ERR_INVALID_ARG, "handles of different shardings");
+  const size_t words = (size_t)(src->ntiles / src->shard_world) * (ns::kTile / 32);
+  const size_t off = (size_t)src->shard_rank * words;
+  CK(cudaSetDevice(dst->dev));
+  CK(cudaMemcpyPeerAsync(dst->d.bitmap + off, dst->dev, src->d.bitmap + off, src->dev, words * 4, dst->st));
+  CK(cudaStreamSynchronize(dst->st));
+  return NS_OK;
+}
+
+ns_status ns_shard_step_end(ns_handle* h) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  if (h->shard_world == 0) return fail(h, NS_ERR_STATE, "not a sharded handle");
+  CK(cudaSetDevice(h->dev));
+  // the rest of enqueue_step after the neuron kernel, eagerly, one step
+  if (h->shard_world > 1)
+    ns::k_shard_merge<<<h->ntiles - h->d.tiles_own, ns::kThreads, 0, h->st>>>(h->d, 0);
+  const bool ext = ext_on(h);
+  const uint32_t sched = sched_of(h);
+  if (tail_on(h)) ns::k_setup<<<1, 32, 0, h->st>>>(h->d, 0);
+  if (sched == 1 || sched == 3) {
+    pick_fused(h->cfg.input_mode, h->cfg.weight_format, sched, ext)
+        <<<h->fused_blocks[sched == 3 ? 1 : 0], 256, 0, h->st>>>(h->d, 0);
+  } else {
+    pick_prop(h->cfg.input_mode, h->cfg.weight_format, ext)<<<h->prop_blocks, 256, 0, h->st>>>(h->d, 0);
+    if (h->cfg.stdp_enabled) pick_ltd(h->cfg.weight_format, ext)<<<h->ltd_blocks, 256, 0, h->st>>>(h->d, 0);
+  }
+  if (tail_on(h)) launch_tail(h, h->d, 0, h->st);
+  if (h->cfg.homeostasis_enabled) launch_homeo(h, h->d, 0, h->st);
+  ns::k_advance<<<1, 1, 0, h->st>>>(h->ctl, 1);
+  h->launches += launches_per_step(h, sched);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(h->st));
   return check_device_status(h);
 }
 

@@ -141,6 +141,10 @@ struct NsDev {
   const uint8_t* pidx;
   const float* ptab;
   uint32_t ptab_rows;
+  // single-network sharding: this rank updates tiles [tile0, tile0 +
+  // tiles_own); the other tiles' spikes arrive as bitmap words (0 and all
+  // tiles on one GPU)
+  uint32_t tile0, tiles_own;
   float* elig;                     // eligibility values [m_pad]
   const uint8_t* elig_flag;        // synapse carries an eligibility trace [m_pad]
   const float* stp_f;              // STP factor per synapse, or null
@@ -447,7 +451,7 @@ __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
     if (lane == 0) s_nk = cnt;
   }
   __syncthreads();
-  const uint32_t tile = blockIdx.x;
+  const uint32_t tile = blockIdx.x + d.tile0;
   const uint64_t base = (uint64_t)tile * kTile;
   const int nk = s_nk;
 
@@ -1177,6 +1181,102 @@ __global__ void __launch_bounds__(256) k_homeostasis(NsDev d, uint32_t jstep) {
     }
     const double inst = bit_of(d.bitmap, (uint32_t)i) ? 1000.0 / d.dt : 0.0;
     d.rate[i] = rate + (inst - rate) * d.dt / 100.0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Single-network sharding (one rank per GPU, neurons split by tiles): after
+// the step's spike bitmap words of every rank have been gathered, one block
+// per tile of the other ranks ("ghost" tiles) rebuilds what the owner's
+// neuron kernel produced for it: the tile's ascending spike list and count,
+// and its neurons' decayed traces with the spike sign (the same float
+// operations as the owner). The tiles count on with the neuron kernel's
+// counter, so the last block to finish does the step's bookkeeping exactly
+// as the neuron kernel's last tile does without sharding.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) k_shard_merge(NsDev d, uint32_t jstep) {
+  __shared__ uint32_t s_wsum[kThreads / 32];
+  __shared__ uint32_t s_total;
+  __shared__ int s_last;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint64_t k = d.ctl->step_base + jstep;
+  const uint32_t par_k = (uint32_t)(k & 1);
+  uint32_t* const spk_k = d.spk + par_k * d.n_pad;
+  uint32_t* const tcnt_k = d.tile_cnt + par_k * (d.ntiles + 1);
+  float2* const rec_k = d.rec + par_k * d.n_pad;
+  // ghost tile of this block: the tiles outside [tile0, tile0 + tiles_own)
+  const uint32_t tile = blockIdx.x < d.tile0 ? blockIdx.x : blockIdx.x + d.tiles_own;
+  const uint64_t base = (uint64_t)tile * kTile;
+  constexpr int kWords = kTile / 32;                 // bitmap words of a tile
+  static_assert(kWords <= kThreads, "one word per thread");
+  const uint32_t wbits = tid < kWords ? d.bitmap[(base >> 5) + tid] : 0u;
+  // ascending list: exclusive scan of the words' popcounts
+  const uint32_t c = __popc(wbits);
+  uint32_t incl = c;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) s_wsum[warp] = incl;
+  __syncthreads();
+  uint32_t woff = 0, tot = 0;
+#pragma unroll
+  for (int q = 0; q < kThreads / 32; ++q) {
+    const uint32_t v = s_wsum[q];
+    woff += q < warp ? v : 0u;
+    tot += v;
+  }
+  uint32_t o = woff + incl - c;
+  for (uint32_t m = wbits; m; m &= m - 1u) spk_k[base + o++] = (uint32_t)(base + 32u * tid + __ffs(m) - 1);
+  if (tid == 0) {
+    tcnt_k[tile] = tot;
+    s_total = tot;
+  }
+  // traces of the ghost neurons: per-step decay, sign bit = spiked
+  if (d.stdp) {
+    for (uint32_t q = tid; q < (uint32_t)kTile; q += kThreads) {
+      const uint64_t i = base + q;
+      const float pv = d.pre[i] * d.ep, qv = d.post[i] * d.em;
+      d.pre[i] = pv;
+      d.post[i] = qv;
+      const bool sp = (d.bitmap[i >> 5] >> (i & 31)) & 1u;
+      rec_k[i] = make_float2(sp ? -pv : pv, sp ? -qv : qv);
+    }
+  }
+  __syncthreads();
+  if (tid == 0) {
+    if (s_total) atomicAdd(&d.ctl->spk_acc[k & 3], (unsigned long long)s_total);
+    __threadfence();
+    const unsigned done = atomicAdd(&d.ctl->tiles_done, 1u);
+    s_last = (done == d.ntiles - 1) ? 1 : 0;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  if (d.ntiles > kSmemTiles) block_scan_u32(tcnt_k, d.tile_off + par_k * (d.ntiles + 1), d.ntiles);
+  if (tid == 0) {
+    Ctl* cc = d.ctl;
+    const unsigned long long total = atomicAdd(&cc->spk_acc[k & 3], 0ull);
+    cc->spk_acc[(k + 2) & 3] = 0ull;
+    cc->tiles_done = 0u;
+    cc->step_spikes[k & 3] = total;
+    cc->spikes_total += total;
+    cc->sim_time += d.dt;
+    unsigned ok = 0u;
+    if (d.log_idx != nullptr && cc->log_steps < d.log_steps_cap && !(cc->status & kErrLogFull)) {
+      if (cc->log_size + total <= d.log_cap) {
+        const unsigned long long sl = cc->log_steps;
+        if (sl == 0) cc->log_first = k;
+        d.log_off[sl + 1] = cc->log_size + total;
+        cc->log_size += total;
+        cc->log_steps = sl + 1;
+        ok = 1u;
+      } else {
+        atomicOr(&cc->status, kErrLogFull);
+      }
+    }
+    cc->log_ok[k & 3] = ok;
   }
 }
 

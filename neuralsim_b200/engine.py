@@ -156,7 +156,10 @@ class SimulationEngine:
     """Device-backed engine. One instance owns one ns_handle (not thread-safe,
     like the Mutex-guarded reference engine, src/simulation/scheduler.rs:23)."""
 
-    def __init__(self, network: Network, config: SimConfig = None, drive: Drive = None):
+    def __init__(self, network: Network, config: SimConfig = None, drive: Drive = None,
+                 shard=None):
+        """shard: (rank, world) for one rank of a sharded network (see
+        neuralsim_b200.shard.partition_network); None for a whole network."""
         self.lib = A.load()
         self.config = config or SimConfig(model=network.model)
         if self.config.model != network.model:
@@ -168,6 +171,8 @@ class SimulationEngine:
         if st != A.NS_OK:
             raise A.NsError(st, (self.lib.ns_last_error(None) or b"").decode())
         try:
+            if shard is not None:
+                self._check(self.lib.ns_shard_configure(self._h, int(shard[0]), int(shard[1])))
             self._upload(network)
             self.set_drive(drive or Drive())
         except Exception:

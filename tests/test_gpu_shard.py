@@ -1,0 +1,62 @@
+"""GPU: one network split over ranks (the ranks driven by one process on one
+GPU, their spike bitmaps copied between them every step) equals the one-GPU
+run bit for bit: rasters, every rank's own neuron state, weights (scattered
+back to CSR positions) and the summed synaptic events."""
+import numpy as np
+import pytest
+
+from neuralsim_b200 import _abi as A
+from neuralsim_b200 import SimulationEngine, NsError
+from neuralsim_b200.shard import VirtualShards, partition_network
+import nets
+
+pytestmark = pytest.mark.gpu
+
+
+def compare(net, cfg, drive, steps, world):
+    one = SimulationEngine(net, cfg, drive)
+    one.run(steps)
+    vs = VirtualShards(net, cfg, drive, world)
+    vs.run(steps)
+    ra, rb = one.read_raster(0, steps), vs.read_raster(0, steps)
+    assert len(ra[0]) > 100
+    assert nets.rasters_equal(ra, rb)
+    sa, sb = one.download_state(), vs.download_state()
+    for key in ("v", "u", "pre_trace", "post_trace", "last_spike_step", "w"):
+        assert np.array_equal(sa[key], sb[key]), key
+    assert vs.events() == int(one.counters()[3])
+    return one, vs
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_sharded_izhikevich_stdp_equals_one_gpu(lib, world):
+    net, cfg, drive = nets.izh_stdp(n=12_000, k=60)
+    compare(net, cfg, drive, 300, world)
+
+
+def test_sharded_reference_engine_with_phase2_rules(lib):
+    # direct current mode, reference drive, STDP, homeostasis, R-STDP and
+    # consolidation: each rank's rules act on its own synapses; the reward
+    # counts every output spike on every rank
+    net, cfg, drive = nets.lif_reference_default(n=5000)
+    net.is_output = (np.arange(net.n) < 1000).astype(np.uint8)
+    cfg.rstdp_enabled = True
+    cfg.reward_threshold = 2
+    nets.with_consolidation(cfg, tau=200.0, drift=0.05)
+    one, vs = compare(net, cfg, drive, 150, 2)
+    assert one.reward() == vs.ranks[0].reward() == vs.ranks[1].reward()
+    e = np.zeros(net.m, np.float32)
+    for r, pos in zip(vs.ranks, vs.pos):
+        e[pos] = r.eligibility()
+    assert np.array_equal(e, one.eligibility())
+
+
+def test_sharded_rank_rejects_foreign_synapses(lib):
+    net, cfg, drive = nets.izh_stdp(n=6000, k=20)
+    part, _ = partition_network(net, 0, 2)
+    with pytest.raises(NsError):
+        SimulationEngine(net, cfg, drive, shard=(0, 2))   # the whole CSR: targets it does not own
+    eng = SimulationEngine(part, cfg, drive, shard=(0, 2))
+    with pytest.raises(NsError):
+        eng.run(1)                                        # no NCCL: the caller exchanges
+    eng.close()
