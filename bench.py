@@ -64,6 +64,8 @@ def args_():
     p.add_argument("--c3-nets", type=int, default=256, help="networks of the batched sweep (profiling: fewer)")
     p.add_argument("--sur-only-1m", action="store_true",
                    help="surrogate line: evaluate only the 1M-neuron network (profiling)")
+    p.add_argument("--shard", action="store_true",
+                   help="under torchrun: one network split over the GPUs (strong scaling) instead of replicas")
     p.add_argument("--schedule", type=int, default=0, choices=[0, 1, 2, 3, 4],
                    help="step schedule: 0 autotune, 1 fused, 2 split, 3 fused 4 blocks/SM, 4 split narrow LTD")
     return p.parse_args()
@@ -370,6 +372,66 @@ def run_ours(a):
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def run_sharded_c2(a):
+    """--shard under torchrun: the C2 network split over the ranks (strong
+    scaling: the same 1M-neuron network whatever N), a spike-bitmap NCCL
+    all-gather per simulation step inside the step graphs. `value` counts
+    every rank's synaptic events over the slowest rank's device time."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    from neuralsim_b200.shard import ShardedEngine
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    net, cfg, drive, _ = build_network(a.neurons, a.in_degree, 44)
+    cfg.device = local
+    cfg.step_schedule = a.schedule or 3
+    se = ShardedEngine(net, cfg, drive, rank, world)
+    eng = se.engine
+    stream = torch.cuda.ExternalStream(eng.stream(), device=local)
+    S = a.sim_steps
+    for _ in range(a.warmup):
+        se.run(S)
+    c0 = eng.counters()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(a.steps):
+            se.run(S)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    c1 = eng.counters()
+    t = torch.tensor([ms, float(c1[3] - c0[3])], dtype=torch.float64, device=f"cuda:{local}")
+    tm = t.clone()
+    dist.all_reduce(tm[0:1], op=dist.ReduceOp.MAX)
+    dist.all_reduce(tm[1:2], op=dist.ReduceOp.SUM)
+    ms_max, events_all = float(tm[0]), float(tm[1])
+    if rank == 0:
+        sim_steps = c1[0] - c0[0]
+        print(json.dumps({
+            "metric": METRIC, "value": events_all / (ms_max / 1e3), "unit": UNIT, "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_max / a.steps,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded generator, configuration shapes)",
+            "config": {"workload": WORKLOAD, "neurons": net.n, "synapses": net.m,
+                       "sim_steps_per_step": S, "parallelism": f"one network sharded over {world} GPUs",
+                       "exchange": "NCCL all-gather of the spike bitmap per simulation step",
+                       "spikes_per_sim_step": (c1[1] - c0[1]) / max(sim_steps, 1),
+                       "events_per_sim_step": events_all / max(sim_steps, 1)},
+            "roofline": None, "cpu_baseline": None, "e2e": None, "clocks": clk.summary(),
+            "gpu_launches": int(eng.launch_count())}), flush=True)
+    se.close()
+    dist.barrier()
+    dist.destroy_process_group()
 
 
 def timed_run(eng, steps, stream):
@@ -747,6 +809,8 @@ def main():
         return
     if a.impl == "reference":
         run_reference(a)
+    elif a.shard and int(os.environ.get("WORLD_SIZE", "1")) > 1:
+        run_sharded_c2(a)
     else:
         run_ours(a)
 
