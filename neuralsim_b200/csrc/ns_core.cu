@@ -77,6 +77,7 @@ struct ns_handle {
   // done by the caller between ns_shard_step_begin and ns_shard_step_end
   uint32_t shard_rank = 0, shard_world = 0;
   ncclComm_t nccl = nullptr;
+  uint32_t type_mask = 1u;          // synapse types present in the CSR (bit per type)
 };
 
 namespace {
@@ -478,6 +479,7 @@ void fill_scalars(ns_handle* h) {
   const uint32_t world = h->shard_world > 1 ? h->shard_world : 1u;
   d.tiles_own = h->ntiles / world;
   d.tile0 = h->shard_rank * d.tiles_own;
+  d.type_mask = h->type_mask;
   d.dt = c.dt_ms; d.dt_f = (float)c.dt_ms;
   d.decay_I = (float)c.current_decay;
   d.stdp = c.stdp_enabled ? 1 : 0;
@@ -1483,6 +1485,14 @@ ns_status ns_upload_csr(ns_handle* h, uint64_t n, uint64_t m, const uint64_t* ro
     if (badh & 2u) return fail(h, NS_ERR_CSR, "column index >= n");
     if (badh & 4u) return fail(h, NS_ERR_NONFINITE, "weight is not finite or |w| >= 2^22");
     return fail(h, NS_ERR_CSR, "synapse type > 3");
+  }
+  // synapse types present: the conductance kernels skip the rows of the others
+  {
+    uint32_t mask = 0u;
+    if (syn_type) for (uint64_t e = 0; e < m && mask != 15u; ++e) mask |= 1u << (syn_type[e] & 3u);
+    else mask = m ? 1u : 0u;
+    if (mask != h->type_mask) drop_graphs(h);  // captured launches carry the mask
+    h->type_mask = mask;
   }
   // weights in storage format
   d.w32 = nullptr; d.w16 = nullptr;

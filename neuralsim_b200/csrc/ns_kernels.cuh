@@ -145,6 +145,9 @@ struct NsDev {
   // tiles_own); the other tiles' spikes arrive as bitmap words (0 and all
   // tiles on one GPU)
   uint32_t tile0, tiles_own;
+  // synapse types present (bit t): accumulator rows of absent types stay
+  // zero and are neither read nor cleared (conductance modes)
+  uint32_t type_mask;
   float* elig;                     // eligibility values [m_pad]
   const uint8_t* elig_flag;        // synapse carries an eligibility trace [m_pad]
   const float* stp_f;              // STP factor per synapse, or null
@@ -503,7 +506,9 @@ __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
     longlong2 accv[NT];
 #pragma unroll
     for (int t = 0; t < NT; ++t)
-      accv[t] = *reinterpret_cast<const longlong2*>(d.acc + ((uint64_t)t * d.D + slot) * d.n_pad + i0);
+      accv[t] = (!COND || ((d.type_mask >> t) & 1u))
+                    ? *reinterpret_cast<const longlong2*>(d.acc + ((uint64_t)t * d.D + slot) * d.n_pad + i0)
+                    : make_longlong2(0, 0);
     float G[4][2];
     if (COND) {
 #pragma unroll
@@ -529,8 +534,9 @@ __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
     for (int t = 0; t < NT; ++t) {
       S[t][0] = from_fix(accv[t].x);
       S[t][1] = from_fix(accv[t].y);
-      *reinterpret_cast<longlong2*>(d.acc + ((uint64_t)t * d.D + slot) * d.n_pad + i0) =
-          make_longlong2(0, 0);
+      if (!COND || ((d.type_mask >> t) & 1u))
+        *reinterpret_cast<longlong2*>(d.acc + ((uint64_t)t * d.D + slot) * d.n_pad + i0) =
+            make_longlong2(0, 0);
     }
     // ---- drive draws: one Philox per pair ----
     U4 y2[2];

@@ -108,6 +108,7 @@ __global__ void __launch_bounds__(kWinThreads, window_min_blocks<MODEL>()) k_win
     if ((word >> lane) & 1u) {
 #pragma unroll
       for (int t = 0; t < NT; ++t) {
+        if (COND && !((d.type_mask >> t) & 1u)) continue;   // absent type: row stays 0
         unsigned long long* ap = d.acc + ((uint64_t)t * d.D + slot) * d.n_pad + i;
         S[t] = from_fix((long long)*ap);
         *ap = 0ull;

@@ -266,6 +266,7 @@ __global__ void __launch_bounds__(256, 2) k_window_sur(NsDev d, SurDev sd, uint3
           inmask |= 1u << s;
 #pragma unroll
           for (int t = 0; t < 4; ++t) {
+            if (!((d.type_mask >> t) & 1u)) continue;   // absent type: no input
             float inc = from_fix((long long)d.acc[((uint64_t)t * d.D + slot) * d.n_pad + i]) * kSyn[t].gmax;
             if (kSyn[t].mg) inc = inc * mgf;
             gmean[t] += inc * sd.wmean[s][t];
@@ -387,6 +388,7 @@ __global__ void __launch_bounds__(256) k_window_fb(NsDev d, SurDev sd, uint32_t 
       if ((word >> (j & 31u)) & 1u) {
 #pragma unroll
         for (int t = 0; t < 4; ++t) {
+          if (!((d.type_mask >> t) & 1u)) continue;   // absent type: row stays 0
           unsigned long long* ap = d.acc + ((uint64_t)t * d.D + slot) * d.n_pad + j;
           S[t] = from_fix((long long)*ap);
           *ap = 0ull;
