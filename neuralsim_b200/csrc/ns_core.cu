@@ -63,8 +63,6 @@ struct ns_handle {
   bool sur_on = false;
   ns::SurDev sd{};
   uint32_t* hstep = nullptr;        // [n_pad] hand-over steps of the surrogate window
-  uint32_t* fb_list = nullptr;      // [n_pad] neurons handed over in a window
-  uint32_t* fb_count = nullptr;     // their number
   std::vector<void*> sur_allocs;
   // R-STDP eligibility and short-term plasticity arrays
   std::vector<void*> ext_allocs;    // elig + elig_flag (R-STDP)
@@ -733,8 +731,6 @@ cudaError_t enqueue_window(ns_handle* h, uint32_t j0, uint32_t Wc) {
   const uint32_t nseg = h->d.nseg;
   if (h->sur_on) {
     h->sd.hstep = h->hstep;
-    h->sd.fb_list = h->fb_list;
-    h->sd.fb_count = h->fb_count;
     ns::k_window_sur<<<nseg, ns::kWinThreads, ns::kSurSmem, h->st>>>(h->d, h->sd, j0, Wc);
     ns::k_window_fb<<<nseg, ns::kWinThreads, 0, h->st>>>(h->d, h->sd, j0, Wc);
     const uint64_t pairs = (uint64_t)Wc * nseg;
@@ -1352,7 +1348,6 @@ static ns_status alloc_dynamic(ns_handle* h) {
     CK(cudaMemsetAsync(d.acc, 0, acc_bytes, h->st));
     if (d.inbits) CK(cudaMemsetAsync(d.inbits, 0, h->alloc_bytes[d.inbits], h->st));
     if (d.contrib) CK(cudaMemsetAsync(d.contrib, 0, h->alloc_bytes[d.contrib], h->st));
-    if (h->fb_count) CK(cudaMemsetAsync(h->fb_count, 0, 4, h->st));
     CK(cudaMemsetAsync(h->ctl, 0, sizeof(ns::Ctl), h->st));
     CK(set_ext_ctl(h, 0, h->cfg.reward_signal, 0u, 0.0, 0));
     h->win_ran = false;
@@ -1397,11 +1392,8 @@ static ns_status alloc_dynamic(ns_handle* h) {
     if ((st = dalloc(h, B, &d.seg_off, (uint64_t)h->win * (d.nseg + 1)))) return st;
     if ((st = dalloc(h, B, &d.step_total, h->win))) return st;
     h->hstep = nullptr;
-    h->fb_list = nullptr;
-    h->fb_count = nullptr;
     if (c.model == NS_MODEL_HH &&
-        ((st = dalloc(h, B, &h->hstep, h->n_pad)) || (st = dalloc(h, B, &h->fb_list, h->n_pad)) ||
-         (st = dalloc(h, B, &h->fb_count, 1))))
+        (st = dalloc(h, B, &h->hstep, h->n_pad)))
       return st;
     int nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pick_window_rows(c.input_mode, c.weight_format), 256, 0) != cudaSuccess || nb < 1) nb = 4;

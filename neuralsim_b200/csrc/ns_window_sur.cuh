@@ -24,8 +24,8 @@
 //     to the fallback for the rest of the window (k_window_fb): neurons of a
 //     window are independent (the delay is at least the window), so the
 //     macro-step kernel never waits for a Rush-Larsen chain;
-//  4. k_window_fb runs every handed-over neuron (one thread each, dense)
-//     with the plain Rush-Larsen steps from its hand-over step, with the
+//  4. k_window_fb runs every handed-over neuron (one thread per neuron, in
+//     neuron order) with the plain Rush-Larsen steps from its hand-over step, with the
 //     per-step inputs and drive (the arithmetic of the step kernels); spikes
 //     go into their segment's list by atomic counts, and k_window_sort puts
 //     each (step, segment) list in ascending order for the window row walk.
@@ -66,8 +66,6 @@ struct SurDev {
   unsigned long long* counts;   // [0] macro-steps by the MLP, [1] by the fallback
   uint32_t* err;
   uint32_t* hstep;         // [n_pad] step of the window a neuron was handed to the fallback (W: none)
-  uint32_t* fb_list;       // [n_pad] neurons handed over in this window (any order)
-  uint32_t* fb_count;      // their number (reset by k_window_sort)
 };
 
 __device__ __forceinline__ float hh_iion(float v, float m, float h, float n, const float* p) {
@@ -324,7 +322,8 @@ __global__ void __launch_bounds__(256, 2) k_window_sur(NsDev d, SurDev sd, uint3
         if (!((inmask >> s) & 1u)) continue;
         const uint32_t slot = (slotf + s) % d.D;
 #pragma unroll
-        for (int t = 0; t < 4; ++t) d.acc[((uint64_t)t * d.D + slot) * d.n_pad + i] = 0ull;
+        for (int t = 0; t < 4; ++t)
+          if ((d.type_mask >> t) & 1u) d.acc[((uint64_t)t * d.D + slot) * d.n_pad + i] = 0ull;
       }
       ++n_mlp;
     } else {
@@ -338,7 +337,6 @@ __global__ void __launch_bounds__(256, 2) k_window_sur(NsDev d, SurDev sd, uint3
   for (int t = 0; t < 4; ++t) d.G[t][i] = G[t];
   d.I[i] = st.I;
   sd.hstep[i] = hand;
-  if (hand < W) sd.fb_list[atomicAdd(sd.fb_count, 1u)] = (uint32_t)i;
   for (int o2 = 16; o2 > 0; o2 >>= 1) n_mlp += __shfl_down_sync(0xffffffffu, n_mlp, o2);
   if (lane == 0 && n_mlp) atomicAdd(&sd.counts[0], n_mlp);
   if (!ok && lane == 0) atomicOr(sd.err, gemm::kErrWait);
@@ -349,63 +347,71 @@ __global__ void __launch_bounds__(256, 2) k_window_sur(NsDev d, SurDev sd, uint3
 }
 
 // The fallback of a window: every neuron the macro-step kernel handed over
-// (one thread each, dense over the hand-over list) continues from its
-// hand-over step to the window's end with the plain Rush-Larsen steps
-// (per-step input and drive, the arithmetic of the step kernels). Chains
-// are independent: no barrier; a spike takes its place in its segment's
-// list of that step by an atomic count, and k_window_sort restores the
-// ascending order.
+// continues from its hand-over step to the window's end with the plain
+// Rush-Larsen steps (per-step input and drive, the arithmetic of the step
+// kernels). One thread per neuron in neuron order: a warp none of whose
+// neurons was handed over returns at once; otherwise its lanes step
+// together from the warp's earliest hand-over step, each lane from its own,
+// so the input words and accumulator rows a step reads are shared or
+// coalesced across the warp. Chains are independent: no barrier; a spike
+// takes its place in its segment's list of that step by an atomic count, and
+// k_window_sort restores the ascending order.
 __global__ void __launch_bounds__(256) k_window_fb(NsDev d, SurDev sd, uint32_t j0, uint32_t W) {
   const uint32_t lane = threadIdx.x & 31u;
-  const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t cnt = *sd.fb_count;
+  const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t hj = j < d.n ? sd.hstep[j] : W;
+  const bool mine = hj < W;
+  if (__ballot_sync(0xffffffffu, mine) == 0u) return;   // whole warp: nothing handed over
+  const uint32_t s0 = __reduce_min_sync(0xffffffffu, mine ? hj : W);
   unsigned long long my_spk = 0, my_out = 0, nfb = 0;
-  if (idx < cnt) {
-    const uint64_t j = sd.fb_list[idx];
-    const uint32_t hj = sd.hstep[j];
-    const uint32_t seg = (uint32_t)(j / kWinThreads);
-    const uint64_t k0 = d.ctl->step_base + j0;
-    const uint64_t words = d.n_pad >> 5;
-    const uint32_t slot0 = (uint32_t)(k0 % d.D);
-    NState ws;
-    ws.v = d.v[j]; ws.m = d.gm[j]; ws.h = d.gh[j]; ws.n = d.gn[j];
-    ws.u = 0.f; ws.refr = 0; ws.I = d.I[j];
-    float wg[4], wp[7];
+  const uint32_t seg = (uint32_t)(j / kWinThreads);
+  const uint64_t k0 = d.ctl->step_base + j0;
+  const uint64_t words = d.n_pad >> 5;
+  const uint32_t slot0 = (uint32_t)(k0 % d.D);
+  NState ws;
+  ws.v = 0.f; ws.m = 0.f; ws.h = 0.f; ws.n = 0.f; ws.u = 0.f; ws.refr = 0; ws.I = 0.f;
+  float wg[4] = {0.f, 0.f, 0.f, 0.f}, wp[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  uint64_t js = 0;
+  uint32_t jl = 0;
+  if (mine) {
+    ws.v = d.v[j]; ws.m = d.gm[j]; ws.h = d.gh[j]; ws.n = d.gn[j]; ws.I = d.I[j];
 #pragma unroll
     for (int t = 0; t < 4; ++t) wg[t] = d.G[t][j];
 #pragma unroll
     for (int q = 0; q < 7; ++q) wp[q] = d.par[q][j];
-    uint64_t js;
-    uint32_t jl;
     drive_key(d, j, js, jl);
-    PoissonWords wpw;
+  }
+  PoissonWords wpw;
 #pragma unroll 1
-    for (uint32_t s = hj; s < W; ++s) {
-      const uint64_t k = k0 + s;
-      const uint32_t slot = (slot0 + s) % d.D;
-      float S[4] = {0.f, 0.f, 0.f, 0.f};
-      const uint32_t word = d.inbits[(uint64_t)slot * words + (j >> 5)];
-      if ((word >> (j & 31u)) & 1u) {
+  for (uint32_t s = s0; s < W; ++s) {
+    const bool on = mine && s >= hj;
+    const uint64_t k = k0 + s;
+    const uint32_t slot = (slot0 + s) % d.D;
+    float S[4] = {0.f, 0.f, 0.f, 0.f};
+    const uint32_t word = d.inbits[(uint64_t)slot * words + (j >> 5)];
+    if (on && ((word >> (j & 31u)) & 1u)) {
 #pragma unroll
-        for (int t = 0; t < 4; ++t) {
-          if (!((d.type_mask >> t) & 1u)) continue;   // absent type: row stays 0
-          unsigned long long* ap = d.acc + ((uint64_t)t * d.D + slot) * d.n_pad + j;
-          S[t] = from_fix((long long)*ap);
-          *ap = 0ull;
-        }
-      }
-      U4 y{0u, 0u, 0u, 0u};
-      if (d.drive_kind != 0) y.x = wpw.at(js, jl, k);
-      float addI, kick, addg;
-      drive_of(d, y, 0.f, 0, addI, kick, addg);
-      if (update_one<2, 4>(d, k, j, ws, wp, 0, S, wg, addI, kick, addg, nullptr, 0)) {
-        d.last[j] = (long long)k;
-        const uint32_t p = atomicAdd(&d.seg_cnt[(uint64_t)s * d.nseg + seg], 1u);
-        d.seg_lst[(uint64_t)s * d.n_pad + (uint64_t)seg * kWinThreads + p] = (uint32_t)j;
-        ++my_spk;
-        if (d.outp[j]) ++my_out;
+      for (int t = 0; t < 4; ++t) {
+        if (!((d.type_mask >> t) & 1u)) continue;   // absent type: row stays 0
+        unsigned long long* ap = d.acc + ((uint64_t)t * d.D + slot) * d.n_pad + j;
+        S[t] = from_fix((long long)*ap);
+        *ap = 0ull;
       }
     }
+    if (!on) continue;
+    U4 y{0u, 0u, 0u, 0u};
+    if (d.drive_kind != 0) y.x = wpw.at(js, jl, k);
+    float addI, kick, addg;
+    drive_of(d, y, 0.f, 0, addI, kick, addg);
+    if (update_one<2, 4>(d, k, j, ws, wp, 0, S, wg, addI, kick, addg, nullptr, 0)) {
+      d.last[j] = (long long)k;
+      const uint32_t p = atomicAdd(&d.seg_cnt[(uint64_t)s * d.nseg + seg], 1u);
+      d.seg_lst[(uint64_t)s * d.n_pad + (uint64_t)seg * kWinThreads + p] = (uint32_t)j;
+      ++my_spk;
+      if (d.outp[j]) ++my_out;
+    }
+  }
+  if (mine) {
     d.v[j] = ws.v; d.gm[j] = ws.m; d.gh[j] = ws.h; d.gn[j] = ws.n;
 #pragma unroll
     for (int t = 0; t < 4; ++t) d.G[t][j] = wg[t];
@@ -423,11 +429,10 @@ __global__ void __launch_bounds__(256) k_window_fb(NsDev d, SurDev sd, uint32_t 
 }
 
 // One thread per (step, segment) of the window: sorts the segment's spike
-// list of that step ascending (lists hold a few entries), clears the
-// segment's input bits of that step's slot, and resets the hand-over count.
+// list of that step ascending (lists hold a few entries) and clears the
+// segment's input bits of that step's slot.
 __global__ void __launch_bounds__(256) k_window_sort(NsDev d, SurDev sd, uint32_t j0, uint32_t W) {
   const uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q == 0) *sd.fb_count = 0u;
   if (q >= (uint64_t)W * d.nseg) return;
   const uint32_t s = (uint32_t)(q / d.nseg), seg = (uint32_t)(q % d.nseg);
   const uint32_t cnt = d.seg_cnt[q];
