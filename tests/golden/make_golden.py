@@ -30,7 +30,23 @@ def net_digest(net):
     for a in (net.row_ptr, net.col, net.w, net.params, net.syn_type, net.plastic):
         if a is not None:
             h.update(np.ascontiguousarray(a).tobytes())
+    # arrays of the later rules enter the digest only where a network has them
+    for a in (net.is_output, net.eligible, net.stp, net.has_stp):
+        if a is not None:
+            h.update(np.ascontiguousarray(a).tobytes())
     return h.hexdigest()
+
+
+def _consolidating(seed):
+    net, cfg, drive = nets.izh_stdp(n=800, k=40, seed=seed, wf=A.WEIGHT_F32)
+    nets.with_consolidation(cfg, tau=10.0, drift=1.0)   # the frame renormalises every ~105 steps
+    return net, cfg, drive
+
+
+def _with_stp(seed):
+    net, cfg, drive = nets.lif_reference_default(n=300, seed=seed, stdp=False, homeo=False)
+    nets.with_stp(net)
+    return net, cfg, drive
 
 
 # name -> (builder, steps, oracle precision)
@@ -40,6 +56,10 @@ CASES = {
     "izh_stdp_f32_n800": (lambda: nets.izh_stdp(n=800, k=40, seed=145, wf=A.WEIGHT_F32), 300, 32),
     "lif_reference_default_n200": (lambda: nets.lif_reference_default(n=200, seed=142), 300, 32),
     "hh_rush_larsen_n400": (lambda: nets.hh_cond(n=400, k=40, seed=146), 2000, 64),
+    "izh_rstdp_f32_n800": (lambda: nets.izh_rstdp(n=800, k=40, seed=147, wf=A.WEIGHT_F32, n_out=80,
+                                                  threshold=4), 300, 32),
+    "izh_consolidation_f32_n800": (lambda: _consolidating(148), 300, 32),
+    "lif_stp_n300": (lambda: _with_stp(149), 200, 32),
 }
 
 
@@ -58,6 +78,9 @@ def run_case(name):
     for k in ("u", "m", "h", "n", "pre", "post", "refr"):
         if k in st and st[k] is not None:
             out[k] = np.asarray(st[k])
+    if getattr(cfg, "rstdp_enabled", False):
+        out["elig"] = np.asarray(o.eligibility(), np.float32 if prec == 32 else np.float64)
+        out["reward"] = np.asarray(o.reward(), np.float64)
     o.close()
     return out
 

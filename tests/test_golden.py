@@ -3,7 +3,8 @@
 CPU: the network generator still produces the fixture's network (digest) and
 the oracle still produces the fixture's raster and state, bit for bit.
 GPU: the CUDA path reproduces the fixtures: bit-exact for LIF and
-Izhikevich (rasters, state, weights); the reference-default engine with
+Izhikevich (rasters, state, weights; eligibility and reward for R-STDP,
+weights through the consolidation frame, STP-scaled input); the reference-default engine with
 homeostasis has equal rasters and weights within 1e-5; for Hodgkin-Huxley (FP64 fixture,
 float device) every spike matched within 0.05 ms and the final V within
 1e-2 of max(|V|, 10 mV).
@@ -61,6 +62,10 @@ def test_gpu_reproduces_fixture(lib, name):
         assert np.array_equal(st["w"].astype(np.float32), f["weights"])
         if "u" in f and name.startswith("izh"):
             assert np.array_equal(st["u"].astype(np.float64), f["u"])
+        if "elig" in f:
+            assert np.array_equal(eng.eligibility(), f["elig"])
+            r, rs = eng.reward()
+            assert r == f["reward"][0] and rs == pytest.approx(f["reward"][1], rel=1e-12)
     else:
         dt_steps = int(round(0.05 / cfg.dt_ms))
         d, ua, ub = nets.match_spikes((f["idx"], f["off"]), raster, dt_steps)
