@@ -666,6 +666,7 @@ def run_e2e(a, net, cfg, drive, local, dist):
     eng = SimulationEngine(pnet, cfg, drive)   # allocations done once
     stream = torch.cuda.ExternalStream(eng.stream(), device=local)
     times, events, d2h = [], [], []
+    raster_buf = None   # pinned, sized after the warm-up job
     for job in range(a.e2e_jobs + 1):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         if dist:
@@ -676,12 +677,14 @@ def run_e2e(a, net, cfg, drive, local, dist):
         c0 = eng.counters()
         eng.run(job_steps)
         c1 = eng.counters()
-        idx, off = eng.read_raster(c0[0], job_steps)
+        idx, off = eng.read_raster(c0[0], job_steps, out=raster_buf)
         st = eng.download_state(with_weights=False)
         e1.record(stream)
         torch.cuda.synchronize()
         if job == 0:
-            continue  # warm-up job
+            # warm-up job: the raster buffer of the timed jobs, pinned once
+            raster_buf = pin(np.zeros(2 * max(int(idx.size), 1), np.uint32))
+            continue
         times.append(e0.elapsed_time(e1))
         events.append(c1[3] - c0[3])
         d2h.append(idx.nbytes + off.nbytes + st["v"].nbytes)

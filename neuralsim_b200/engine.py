@@ -261,15 +261,20 @@ class SimulationEngine:
         idx, off = self.read_raster(first_step, n_steps)
         return [idx[int(off[q]):int(off[q + 1])] for q in range(n_steps)]
 
-    def read_raster(self, first_step: int, n_steps: int):
-        """(idx, offsets) flat form of the spike log."""
+    def read_raster(self, first_step: int, n_steps: int, out=None):
+        """(idx, offsets) flat form of the spike log. out: an optional uint32
+        array (e.g. in pinned host memory) that receives the indices when it
+        is large enough; the returned idx is then a view of it."""
         off = np.zeros(n_steps + 1, np.uint64)
         nw = C.c_uint64()
         st = self.lib.ns_read_spikes(self._h, first_step, n_steps, None, _ptr(off), 0, C.byref(nw))
         total = int(nw.value)
         if st != A.NS_OK and total == 0:
             self._check(st)
-        idx = np.zeros(max(total, 1), np.uint32)
+        if out is not None and out.dtype == np.uint32 and out.flags.c_contiguous and out.size >= max(total, 1):
+            idx = out
+        else:
+            idx = np.empty(max(total, 1), np.uint32)
         self._check(self.lib.ns_read_spikes(self._h, first_step, n_steps, _ptr(idx), _ptr(off),
                                             total, C.byref(nw)))
         return idx[:total], off
