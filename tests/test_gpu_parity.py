@@ -327,6 +327,25 @@ def test_reference_default_engine_matches_oracle(lib):
     assert np.allclose(eng.rates(), o.rates(), rtol=1e-12, atol=1e-9)
 
 
+def test_reference_conductance_all_types_stdp_homeostasis(lib):
+    # reference conductance mode with AMPA, GABA, GABA-B and NMDA synapses,
+    # STDP and homeostasis (contributions carry the NMDA Mg block): rasters
+    # equal the float oracle; weights and V within 1e-5 (per-synapse exp)
+    net, cfg, drive = nets.lif_conductance_all_types(n=3000)
+    cfg.stdp_enabled = True
+    cfg.homeostasis_enabled = True
+    eng = gpu_run(net, cfg, drive, 100)
+    o = FastOracle(net, cfg, drive, precision=32)
+    o.step(100)
+    ra, rb = eng.read_raster(0, 100), o.raster()
+    assert len(rb[0]) > 100
+    assert nets.rasters_equal(ra, rb)
+    st = eng.download_state()
+    assert np.allclose(st["w"].astype(np.float64), o.weights(), rtol=1e-5, atol=1e-6)
+    assert np.allclose(st["v"].astype(np.float64), o.state()["v"], rtol=1e-5, atol=1e-4)
+    assert np.count_nonzero(st["w"] != net.w) > 100
+
+
 def test_reference_conductance_mode_matches_oracle(lib):
     net, cfg, drive = nets.lif_reference_default(n=2000, stdp=False, homeo=False, conductance=True)
     eng = gpu_run(net, cfg, drive, 100)

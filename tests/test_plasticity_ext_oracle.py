@@ -154,6 +154,19 @@ def test_conductance_ref_all_types_fast_vs_literal(oracle_lib):
     assert np.allclose(f.state()["v"], l.state()["v"], rtol=1e-7, atol=1e-6)
 
 
+def test_conductance_ref_all_types_stdp_homeostasis_fast_vs_literal(oracle_lib):
+    # the same mode with STDP and homeostasis: contributions use w*gmax*mg(V)
+    net, cfg, drive = nets.lif_conductance_all_types(n=300)
+    cfg.stdp_enabled = True
+    cfg.homeostasis_enabled = True
+    f, l, _ = run_pair(net, cfg, drive, 120)
+    ra, rb = f.raster(), l.raster()
+    assert len(ra[0]) > 20
+    assert nets.rasters_equal(ra, rb)
+    assert np.allclose(f.weights(), l.weights(), rtol=1e-9, atol=1e-9)
+    assert np.count_nonzero(f.weights() != net.w.astype(np.float64)) > 50
+
+
 def test_reward_sum_is_sum_of_rewards(oracle_lib):
     net, cfg, drive = nets.izh_rstdp(n=1500, k=40)
     f = FastOracle(net, cfg, drive, precision=64)
