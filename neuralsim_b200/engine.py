@@ -197,6 +197,10 @@ class SimulationEngine:
         self._check(self.lib.ns_upload_csr(
             self._h, net.n, net.m, _ptr(net.row_ptr), _ptr(net.col), _ptr(net.w),
             _ptr(net.syn_type), _ptr(net.plastic)))
+        for name, want in (("eligible", (net.m,)), ("has_stp", (net.m,)), ("stp", (net.m, 5))):
+            a = getattr(net, name)
+            if a is not None and a.shape != want:
+                raise ValueError(f"Network.{name} must have shape {want}")
         if self.config.rstdp_enabled and net.eligible is not None:
             self._check(self.lib.ns_upload_eligibility(self._h, _ptr(net.eligible), None))
         if net.stp is not None:
@@ -329,6 +333,9 @@ class SimulationEngine:
     def upload_eligibility(self, eligible=None, values=None):
         el = None if eligible is None else np.ascontiguousarray(eligible, np.uint8)
         va = None if values is None else np.ascontiguousarray(values, np.float32)
+        for a in (el, va):
+            if a is not None and a.size != self.network.m:
+                raise ValueError("eligibility arrays need one entry per synapse (m)")
         self._check(self.lib.ns_upload_eligibility(self._h, _ptr(el), _ptr(va)))
 
     def apply_reward(self, reward: float):

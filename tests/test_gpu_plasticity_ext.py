@@ -227,3 +227,32 @@ def test_conductance_ref_all_types(lib):
     assert nets.rasters_equal(ra, rb)
     v = eng.download_state()["v"].astype(np.float64)
     assert np.allclose(v, o.state()["v"], rtol=1e-5, atol=1e-4)
+
+
+def test_stp_ignored_in_conductance_mode(lib):
+    # the reference applies STP only to direct current injection
+    # (engine.rs:457-463): a conductance network steps as without it
+    net, cfg, drive = nets.lif_reference_default(n=2000, stdp=False, homeo=False, conductance=True)
+    plain = SimulationEngine(net, cfg, drive)
+    plain.run(100)
+    nets.with_stp(net)
+    eng = SimulationEngine(net, cfg, drive)
+    eng.run(100)
+    assert nets.rasters_equal(eng.read_raster(0, 100), plain.read_raster(0, 100))
+
+
+def test_rstdp_entry_points_before_stepping_and_without_rstdp(lib):
+    net, cfg, drive = nets.izh_rstdp(n=2000, k=20)
+    eng = SimulationEngine(net, cfg, drive)
+    eng.apply_reward(1.0)                    # before any step: e = 0 everywhere, no change
+    assert np.array_equal(eng.download_state()["w"], net.w)
+    assert eng.reward() == (cfg.reward_signal, 0.0)
+    with pytest.raises(ValueError):
+        eng.upload_eligibility(values=np.zeros(net.m - 1, np.float32))   # one entry short
+    eng.close()
+    net2, cfg2, drive2 = nets.izh_stdp(n=2000, k=20)
+    e2 = SimulationEngine(net2, cfg2, drive2)
+    with pytest.raises(NsError):
+        e2.upload_eligibility(values=np.zeros(net2.m, np.float32))   # R-STDP is off
+    e2.close()
+

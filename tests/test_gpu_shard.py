@@ -60,3 +60,21 @@ def test_sharded_rank_rejects_foreign_synapses(lib):
     with pytest.raises(NsError):
         eng.run(1)                                        # no NCCL: the caller exchanges
     eng.close()
+
+
+def test_sharded_ranks_without_neurons(lib):
+    # 3 ranks over a network of one tile: ranks 1 and 2 own no neurons and
+    # hold no synapses, but take part in every step's exchange
+    from neuralsim_b200.shard import shard_range
+    net, cfg, drive = nets.izh_stdp(n=1500, k=30)
+    assert shard_range(net.n, 1, 3) == (net.n, net.n)
+    compare(net, cfg, drive, 200, 3)
+
+
+def test_shard_configure_after_upload_is_refused(lib):
+    net, cfg, drive = nets.izh_stdp(n=2000, k=20)
+    eng = SimulationEngine(net, cfg, drive)
+    with pytest.raises(NsError):
+        eng._check(eng.lib.ns_shard_configure(eng._h, 0, 2))
+    eng.close()
+
