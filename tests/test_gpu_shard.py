@@ -5,7 +5,6 @@ back to CSR positions) and the summed synaptic events."""
 import numpy as np
 import pytest
 
-from neuralsim_b200 import _abi as A
 from neuralsim_b200 import SimulationEngine, NsError
 from neuralsim_b200.shard import VirtualShards, partition_network
 import nets
