@@ -742,9 +742,8 @@ cudaError_t enqueue_window(ns_handle* h, uint32_t j0, uint32_t Wc) {
   pick_window_rows(h->cfg.input_mode, h->cfg.weight_format)
       <<<h->win_rows_blocks, 256, 0, h->st>>>(h->d, j0, Wc);
   ns::k_window_scan<<<Wc, 256, 0, h->st>>>(h->d, Wc);
-  if (h->d.log_idx) ns::k_window_log<<<Wc, 256, 0, h->st>>>(h->d, Wc);
-  ns::k_window_commit<<<1, 32, 0, h->st>>>(h->d, j0, Wc);
-  h->launches += h->d.log_idx ? 5 : 4;
+  ns::k_window_finish<<<Wc, 256, 0, h->st>>>(h->d, j0, Wc);
+  h->launches += 4;
   return cudaGetLastError();
 }
 
@@ -789,7 +788,7 @@ ns_status run_steps(ns_handle* h, uint32_t n, uint32_t sched) {
     if (r) return r;
     while (left >= S) {
       CK(cudaGraphLaunch(ex, h->st));
-      if (h->win) h->launches += ((S + h->wcur - 1) / h->wcur) * ((h->d.log_idx ? 5 : 4) + (h->sur_on ? 2 : 0)) + 1;
+      if (h->win) h->launches += ((S + h->wcur - 1) / h->wcur) * (4 + (h->sur_on ? 2 : 0)) + 1;
       else h->launches += (uint64_t)S * launches_per_step(h, sched) + 1;
       left -= S;
     }
@@ -924,7 +923,7 @@ ns_status autotune_window(ns_handle* h, uint32_t budget, uint32_t* used) {
     if ((ce = cudaEventSynchronize(e1)) != cudaSuccess) break;
     if ((ce = cudaEventElapsedTime(&ms, e0, e1)) != cudaSuccess) break;
     us[q] = ms * 1e3 / T;
-    h->launches += ((T + cand[q] - 1) / cand[q]) * (h->d.log_idx ? 5 : 4) + 1;
+    h->launches += ((T + cand[q] - 1) / cand[q]) * 4 + 1;
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);

@@ -54,6 +54,7 @@ struct Ctl {
   unsigned long long cons_k0;     // step whose frame is the identity
   unsigned int ezero_init;        // eligibility all 0 and in range at `origin`
   unsigned int tail_done;         // blocks of k_tail finished (renormalisation)
+  unsigned int win_done;          // blocks of k_window_finish finished
 };
 
 struct Kick { uint32_t target; float amt; };

@@ -9,8 +9,8 @@
 //                    segments of 256 neurons (warp ballots, ascending order);
 //  2. k_window_rows — one warp per non-empty segment walks the spikers' CSR
 //                    rows and delivers into slot (k + D) mod D, setting bits;
-//  3. k_window_scan / k_window_log — per-step totals and the ordered spike
-//                    log; k_window_commit — counters and the FP64 clock.
+//  3. k_window_scan — per-step totals; k_window_finish — the ordered spike
+//                    log, then counters and the FP64 clock.
 #pragma once
 #include "ns_kernels.cuh"
 
@@ -231,34 +231,42 @@ __global__ void __launch_bounds__(256) k_window_scan(NsDev d, uint32_t W) {
   if (threadIdx.x == 0) d.step_total[s] = tot;
 }
 
-// Ordered spike log of the window: block s copies step s's segments in order
-// at its place in the log, after the window fitted as a whole.
-__global__ void __launch_bounds__(256) k_window_log(NsDev d, uint32_t W) {
+// Ordered spike log and bookkeeping of the window, one launch: block s
+// copies step s's segments in order at its place in the log (after the
+// window fitted as a whole); the last block to finish then updates the log
+// counters, the last-step spike counts and the FP64 clock (dt added once
+// per step, as the step path does).
+__global__ void __launch_bounds__(256) k_window_finish(NsDev d, uint32_t j0, uint32_t W) {
+  __shared__ int s_last;
   const uint32_t s = blockIdx.x;
-  if (s >= W || d.log_idx == nullptr) return;
   Ctl* c = d.ctl;
-  if (c->status & kErrLogFull) return;
-  unsigned long long all = 0, before = 0;
-  for (uint32_t q = 0; q < W; ++q) {
-    all += d.step_total[q];
-    if (q < s) before += d.step_total[q];
+  if (s < W && d.log_idx != nullptr && !(c->status & kErrLogFull)) {
+    unsigned long long all = 0, before = 0;
+    for (uint32_t q = 0; q < W; ++q) {
+      all += d.step_total[q];
+      if (q < s) before += d.step_total[q];
+    }
+    if (c->log_steps + W <= d.log_steps_cap && c->log_size + all <= d.log_cap) {
+      const unsigned long long base = c->log_size + before;
+      const uint32_t* off = d.seg_off + (uint64_t)s * (d.nseg + 1);
+      for (uint32_t seg = threadIdx.x; seg < d.nseg; seg += blockDim.x) {
+        const uint32_t cnt = d.seg_cnt[(uint64_t)s * d.nseg + seg];
+        const uint32_t* lst = d.seg_lst + (uint64_t)s * d.n_pad + (uint64_t)seg * kWinThreads;
+        for (uint32_t l = 0; l < cnt; ++l) d.log_idx[base + off[seg] + l] = lst[l];
+      }
+      if (threadIdx.x == 0) d.log_off[c->log_steps + s + 1] = base + d.step_total[s];
+    }
   }
-  if (c->log_steps + W > d.log_steps_cap || c->log_size + all > d.log_cap) return;
-  const unsigned long long base = c->log_size + before;
-  const uint32_t* off = d.seg_off + (uint64_t)s * (d.nseg + 1);
-  for (uint32_t seg = threadIdx.x; seg < d.nseg; seg += blockDim.x) {
-    const uint32_t cnt = d.seg_cnt[(uint64_t)s * d.nseg + seg];
-    const uint32_t* lst = d.seg_lst + (uint64_t)s * d.n_pad + (uint64_t)seg * kWinThreads;
-    for (uint32_t l = 0; l < cnt; ++l) d.log_idx[base + off[seg] + l] = lst[l];
+  // every block has read the log counters before the last one moves them
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(&c->win_done, 1u) == gridDim.x - 1 ? 1 : 0;
   }
-  if (threadIdx.x == 0) d.log_off[c->log_steps + s + 1] = base + d.step_total[s];
-}
-
-// Window bookkeeping: log counters (if the window fitted), last-step spike
-// counts, FP64 clock (dt added once per step, as the step path does).
-__global__ void k_window_commit(NsDev d, uint32_t j0, uint32_t W) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  Ctl* c = d.ctl;
+  __syncthreads();
+  if (!s_last || threadIdx.x != 0) return;
+  __threadfence();
+  c->win_done = 0u;
   const uint64_t k0 = c->step_base + j0;
   unsigned long long all = 0;
   for (uint32_t q = 0; q < W; ++q) {
