@@ -305,6 +305,12 @@ ns_status ns_network_rates(ns_handle* h, uint64_t first_step, uint32_t n_steps, 
 
 /* Weight mean / std over all synapses (engine.rs:658-669), on demand. */
 ns_status ns_weight_stats(ns_handle* h, double* mean, double* stddev);
+/* The engine's LFP signal (lfp_signal, engine.rs:64, :492): the sum over
+ * steps and synapses of |g (E_rev - V)| in the reference conductance mode,
+ * since creation or the last state upload (0 in the other modes). Each
+ * neuron's per-type conductance stands for the sum of its synapses'
+ * (conductances are >= 0: GABA types take |w|). */
+ns_status ns_get_lfp(ns_handle* h, double* lfp);
 
 /* --- the rest of phase 2: R-STDP eligibility and reward, short-term
  *     plasticity (engine.rs:457-463, :519-563, :626-631) ---------------- */

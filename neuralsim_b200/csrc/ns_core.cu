@@ -2304,6 +2304,37 @@ ns_status ns_profile_steps(ns_handle* h, uint32_t n_steps, double* kernel_ms, ui
   return check_device_status(h);
 }
 
+ns_status ns_get_lfp(ns_handle* h, double* lfp) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  if (!lfp) return fail(h, NS_ERR_INVALID_ARG, "null output");
+  ns_status r = ready(h);
+  if (r) return r;
+  *lfp = 0.0;
+  if (h->cfg.input_mode != NS_INPUT_CONDUCTANCE_REF) return NS_OK;  // current modes: no LFP
+  CK(cudaSetDevice(h->dev));
+  fill_scalars(h);
+  ns::Ctl c{};
+  CK(copy_sync(h, &c, h->ctl, sizeof(c), cudaMemcpyDeviceToHost));
+  unsigned long long* acc = nullptr;
+  CK(cudaMalloc(&acc, 8));
+  cudaError_t e = cudaMemsetAsync(acc, 0, 8, h->st);
+  if (e == cudaSuccess) {
+    ns::k_lfp_pending<<<h->sms * 4, 256, 0, h->st>>>(h->d, acc);
+    e = cudaGetLastError();
+  }
+  long long pend = 0;
+  if (e == cudaSuccess) e = copy_sync(h, &pend, acc, 8, cudaMemcpyDeviceToHost);
+  cudaFree(acc);
+  CK(e);
+  h->launches += 1;
+  // the folded steps, the last step's sum, then the last step's own term
+  double t = c.lfp_total;
+  if (c.step_base > 0) t += (double)c.lfp_step[(c.step_base - 1) & 3] * 0x1p-24;
+  t += (double)pend * 0x1p-24;
+  *lfp = t;
+  return NS_OK;
+}
+
 // --- single-network sharding ------------------------------------------
 ns_status ns_shard_range(uint64_t n, uint32_t rank, uint32_t world, uint64_t* lo, uint64_t* hi) {
   if (!lo || !hi || world == 0 || rank >= world || n == 0) return NS_ERR_INVALID_ARG;

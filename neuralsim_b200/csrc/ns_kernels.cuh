@@ -55,6 +55,11 @@ struct Ctl {
   unsigned int ezero_init;        // eligibility all 0 and in range at `origin`
   unsigned int tail_done;         // blocks of k_tail finished (renormalisation)
   unsigned int win_done;          // blocks of k_window_finish finished
+  // LFP of the reference conductance mode (engine.rs:492): per-step sums
+  // of |g (E_rev - V)| in fixed point (2^-24) at [k & 3], folded into an
+  // FP64 total one step later
+  long long lfp_step[4];
+  double lfp_total;
 };
 
 struct Kick { uint32_t target; float amt; };
@@ -322,7 +327,7 @@ template <int MODEL, int MODE>
 __device__ __forceinline__ bool update_one(const NsDev& d, uint64_t k, uint64_t i, NState& st,
                                            const float* par, int rs, const float* S, float* G,
                                            float addI, float kick, float addg, const Kick* kicks,
-                                           int nk) {
+                                           int nk, float* lfp = nullptr) {
   float Iv = 0.f, kk = 0.f;
   const float vi = st.v;
   if (MODE == 0) {
@@ -342,7 +347,9 @@ __device__ __forceinline__ bool update_one(const NsDev& d, uint64_t k, uint64_t 
       float g = G[t] * d.Gdec[t] + inc;
       if (t == 0) g = g + addg;
       G[t] = g;
-      isyn = isyn + g * (kSyn[t].erev - vi);
+      const float cur = g * (kSyn[t].erev - vi);
+      isyn = isyn + cur;
+      if (MODE == 3 && lfp != nullptr) *lfp = *lfp + fabsf(cur);   // lfp += |I_syn|, engine.rs:492
     }
     Iv = (MODE == 3) ? st.I + isyn : isyn;
   }
@@ -435,6 +442,14 @@ __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
   float2* const rec_k = d.rec + par_k * d.n_pad;
 
   if (tid == 0) s_nk = 0;
+  if (MODE == 3 && blockIdx.x == 0 && tid == 0) {
+    // the previous step's LFP sum is complete: fold it; clear the next slot
+    Ctl* c = d.ctl;
+    c->lfp_total += (double)c->lfp_step[(k + 3) & 3] * 0x1p-24;
+    c->lfp_step[(k + 3) & 3] = 0ll;
+    c->lfp_step[(k + 1) & 3] = 0ll;
+  }
+  long long lfp_fix = 0;
   if (PT)
     for (uint32_t q = tid; q < d.ptab_rows * 8u; q += kThreads) s_tab[q] = __ldg(d.ptab + q);
   __syncthreads();
@@ -585,8 +600,10 @@ __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
       for (int t = 0; t < NT; ++t) Se[t] = S[t][e];
 #pragma unroll
       for (int t = 0; t < 4; ++t) Ge[t] = COND ? G[t][e] : 0.f;
+      float lf = 0.f;
       const bool sp = update_one<MODEL, MODE>(d, k, i, st[e], par[e], rs[e], Se, Ge, addI, kick,
-                                              addg, s_kick, nk);
+                                              addg, s_kick, nk, MODE == 3 ? &lf : nullptr);
+      if (MODE == 3) lfp_fix += __float2ll_rn(lf * 0x1p24f);
 #pragma unroll
       for (int t = 0; t < 4; ++t) if (COND) G[t][e] = Ge[t];
       spk[e] = sp && (i < d.n);
@@ -665,6 +682,10 @@ __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
     const uint32_t o = s_off[r * kWarps + warp] + pre_cnt;
     if (s0) spk_k[base + o] = i0;
     if (s1) spk_k[base + o + (s0 ? 1u : 0u)] = i0 + 1;
+  }
+  if (MODE == 3) {
+    for (int o = 16; o > 0; o >>= 1) lfp_fix += __shfl_down_sync(0xffffffffu, lfp_fix, o);
+    if (lane == 0 && lfp_fix) atomicAdd((unsigned long long*)&d.ctl->lfp_step[k & 3], (unsigned long long)lfp_fix);
   }
   // last tile of the step: counters, FP64 clock, spike-log bookkeeping
   if (tid == 0) {
@@ -1285,6 +1306,32 @@ __global__ void __launch_bounds__(kThreads) k_shard_merge(NsDev d, uint32_t jste
     }
     cc->log_ok[k & 3] = ok;
   }
+}
+
+// The LFP term of the last completed step (reference conductance mode): the
+// conductances and currents that the next step's neuron kernel will compute
+// (same float operations), summed without consuming the delivered input.
+__global__ void __launch_bounds__(256) k_lfp_pending(NsDev d, unsigned long long* out) {
+  const uint64_t k = d.ctl->step_base;
+  const uint32_t slot = (uint32_t)(k % d.D);
+  long long acc = 0;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < d.n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const float vi = d.v[i];
+    float lf = 0.f;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const float S = ((d.type_mask >> t) & 1u)
+                          ? from_fix((long long)d.acc[((uint64_t)t * d.D + slot) * d.n_pad + i]) : 0.f;
+      float inc = S * kSyn[t].gmax;
+      if (kSyn[t].mg && inc != 0.0f) inc = inc * (1.0f / (1.0f + (1.0f / 3.57f) * expf(-0.062f * vi)));
+      const float g = d.G[t][i] * d.Gdec[t] + inc;
+      lf = lf + fabsf(g * (kSyn[t].erev - vi));
+    }
+    acc += __float2ll_rn(lf * 0x1p24f);
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0 && acc) atomicAdd(out, (unsigned long long)acc);
 }
 
 __global__ void k_advance(Ctl* ctl, uint32_t steps) { ctl->step_base += steps; }

@@ -324,6 +324,12 @@ class SimulationEngine:
         soa.params_per_neuron = PARAMS_PER_NEURON[self.config.model]
         self._check(self.lib.ns_upload_state(self._h, C.byref(soa), _ptr(st.get("w")), int(step)))
 
+    def lfp(self) -> float:
+        """lfp_signal (engine.rs:492) of the reference conductance mode."""
+        x = C.c_double()
+        self._check(self.lib.ns_get_lfp(self._h, C.byref(x)))
+        return x.value
+
     # -- R-STDP reward and eligibility (engine.rs:151-175, :546-563, :626-631) --
     def eligibility(self):
         e = np.zeros(max(self.network.m, 1), np.float32)

@@ -385,6 +385,12 @@ template <class R> struct Fast {
   double cons_a = 1.0, consA_prev = 1.0, consA_cur = 1.0;
   uint64_t cons_k0 = 0;
   R fr[6] = {1, 0, 1, 1, 0, 1};  // weight frame of step k and k+1: A, B, 1/A
+  // LFP of the reference conductance mode (lfp_signal, engine.rs:478-493):
+  // per neuron sum_t |g_t (E_t - V)| at the neuron's update, the float engine
+  // rounding each neuron's term to 2^-24 fixed point; one step's sum joins
+  // the FP64 total at the start of the next step.
+  int64_t lfp_fix_prev = 0, lfp_fix_cur = 0;
+  double lfp_d_prev = 0, lfp_d_cur = 0, lfp_total = 0;
   bool cond() const { return c.input_mode == 3 || c.input_mode == 4; }
 
   R wget(uint64_t s) const { return bf16 ? (R)bf16_to_f32(wb[s]) : w[s]; }
@@ -629,6 +635,12 @@ template <class R> struct Fast {
     const uint64_t slot = k % D;
     global_kicks(c, n, k, kicks);
     spk.clear();
+    if (c.input_mode == 3) {
+      if (sizeof(R) == 4) lfp_total += (double)lfp_fix_prev * 0x1p-24;
+      else lfp_total += lfp_d_prev;
+      lfp_fix_cur = 0;
+      lfp_d_cur = 0;
+    }
     for (uint64_t i = 0; i < n; ++i) {
       R syn = 0;
       R S[4] = {0, 0, 0, 0};
@@ -655,7 +667,7 @@ template <class R> struct Fast {
           Ii = syn;
           break;
         default: {
-          R isyn = 0;
+          R isyn = 0, lf = 0;
           for (int t = 0; t < 4; ++t) {
             R dec = (R)std::exp(-c.dt / kDyn[t].decay);
             R inc = S[t] * (R)kDyn[t].gmax;
@@ -663,7 +675,13 @@ template <class R> struct Fast {
             R g = G[t][i] * dec + inc;
             if (t == 0) g = g + d.add_g;
             G[t][i] = g;
-            isyn = isyn + g * ((R)kDyn[t].erev - vi);
+            const R cur = g * ((R)kDyn[t].erev - vi);
+            isyn = isyn + cur;
+            lf = lf + std::fabs(cur);
+          }
+          if (c.input_mode == 3) {
+            if (sizeof(R) == 4) lfp_fix_cur += (int64_t)std::llrint((float)lf * 0x1p24f);
+            else lfp_d_cur += (double)lf;
           }
           Ii = (c.input_mode == 3) ? Ii + isyn : isyn;
           break;
@@ -735,6 +753,44 @@ template <class R> struct Fast {
       }
       if (s) { last[i] = (int64_t)k; spk.push_back((uint32_t)i); }
     }
+    if (c.input_mode == 3) { lfp_fix_prev = lfp_fix_cur; lfp_d_prev = lfp_d_cur; }
+  }
+
+  // LFP after the last completed step: the folded steps, the last step's
+  // sum, then the last step's own term, which the device's next neuron
+  // update would compute (the delivered input read, not consumed; no drive).
+  double lfp() const {
+    if (c.input_mode != 3) return 0.0;
+    const uint64_t D = (uint64_t)c.delay_steps;
+    const uint64_t slot = step % D;
+    int64_t pf = 0;
+    double pd = 0;
+    for (uint64_t i = 0; i < n; ++i) {
+      const R vi = v[i];
+      R lf = 0;
+      for (int t = 0; t < 4; ++t) {
+        R S = 0;
+        if (t < ntypes_acc) {
+          const uint64_t a = ((uint64_t)t * D + slot) * n + i;
+          S = sizeof(R) == 4 ? (R)from_fix(accf[a]) : (R)accd[a];
+        }
+        R inc = S * (R)kDyn[t].gmax;
+        if (kDyn[t].mg) inc = inc * mg_block<R>(t, vi);
+        const R g = G[t][i] * (R)std::exp(-c.dt / kDyn[t].decay) + inc;
+        lf = lf + std::fabs(g * ((R)kDyn[t].erev - vi));
+      }
+      if (sizeof(R) == 4) pf += (int64_t)std::llrint((float)lf * 0x1p24f);
+      else pd += (double)lf;
+    }
+    double t = lfp_total;
+    if (sizeof(R) == 4) {
+      if (step > 0) t += (double)lfp_fix_prev * 0x1p-24;
+      t += (double)pf * 0x1p-24;
+    } else {
+      if (step > 0) t += lfp_d_prev;
+      t += pd;
+    }
+    return t;
   }
 
   void accumulate(uint64_t slot_base_type, uint64_t i, R val) {
@@ -1352,6 +1408,7 @@ void or_fast_rates(void* s, double* rates) {
   FAST_DISPATCH(s, std::copy(F->rate.begin(), F->rate.end(), rates));
 }
 uint64_t or_fast_events(void* s) { uint64_t r = 0; FAST_DISPATCH(s, r = F->events); return r; }
+double or_fast_lfp(void* s) { double r = 0; FAST_DISPATCH(s, r = F->lfp()); return r; }
 void or_fast_destroy(void* s) {
   auto* pr = (std::pair<int, void*>*)s;
   if (pr->first == 32) delete (Fast<float>*)pr->second; else delete (Fast<double>*)pr->second;

@@ -125,6 +125,9 @@ void or_fast_state(void* s, double* v, double* u, double* m, double* h, double* 
 void or_fast_weights(void* s, double* w);
 void or_fast_rates(void* s, double* rates);
 uint64_t or_fast_events(void* s);
+/* lfp_signal (engine.rs:492) in the reference conductance mode, as the
+ * device sums it (0 in the other modes) */
+double or_fast_lfp(void* s);
 /* eligibility values (m), reward now and the sum of the reward after each
  * step (out2), and SimulationEngine::apply_reward as the device does it */
 void or_fast_eligibility(void* s, double* e);

@@ -89,6 +89,7 @@ def load():
         "or_fast_weights": (None, [vp, vp]),
         "or_fast_rates": (None, [vp, vp]),
         "or_fast_events": (u64, [vp]),
+        "or_fast_lfp": (C.c_double, [vp]),
         "or_fast_eligibility": (None, [vp, vp]),
         "or_fast_reward": (None, [vp, vp]),
         "or_fast_apply_reward": (None, [vp, C.c_double]),
@@ -199,6 +200,10 @@ class _Base:
 
     def events(self):
         return int(getattr(self.L, self.prefix + "events")(self.h))
+
+    def lfp(self):
+        """lfp_signal (engine.rs:492) as the device sums it."""
+        return float(self.L.or_fast_lfp(self.h))
 
     def eligibility(self):
         e = np.zeros(max(self.m, 1), np.float64)

@@ -356,6 +356,45 @@ def test_reference_conductance_mode_matches_oracle(lib):
     assert np.allclose(v, o.state()["v"], rtol=1e-5, atol=1e-4)
 
 
+@pytest.mark.parametrize("which", ["default", "all_types", "all_types_stdp"])
+def test_lfp_matches_oracle(lib, which):
+    # lfp_signal (engine.rs:492) in the reference conductance mode: each
+    # neuron's term rounded to 2^-24, exact int64 step sums, FP64 total in
+    # step order, so the float oracle's value is matched bit for bit. The
+    # NMDA Mg block (device expf) and STDP (per-synapse exp) leave V within
+    # 1e-5 of the oracle's, so with them the LFP agrees to a tolerance.
+    if which == "default":
+        net, cfg, drive = nets.lif_reference_default(n=2000, stdp=False, homeo=False, conductance=True)
+    else:
+        net, cfg, drive = nets.lif_conductance_all_types(n=3000)
+        if which == "all_types_stdp":
+            cfg.stdp_enabled = True
+            cfg.homeostasis_enabled = True
+    eng = SimulationEngine(net, cfg, drive)
+    o = FastOracle(net, cfg, drive, precision=32)
+    assert eng.lfp() == o.lfp() == 0.0
+    done = 0
+    for k in (1, 37, 100):
+        eng.run(k - done)
+        o.step(k - done)
+        done = k
+        if which != "default":
+            assert eng.lfp() == pytest.approx(o.lfp(), rel=1e-7)
+        else:
+            assert eng.lfp() == o.lfp()
+    assert nets.rasters_equal(eng.read_raster(0, 100), o.raster())
+    assert o.lfp() > 1e6
+    a = eng.lfp()
+    assert eng.lfp() == a   # reading it consumes nothing
+    eng.close()
+
+
+def test_lfp_zero_in_current_mode(lib):
+    net, cfg, drive = nets.lif_reference_default(n=500, stdp=False, homeo=False)
+    eng = gpu_run(net, cfg, drive, 20)
+    assert eng.lfp() == 0.0
+
+
 def test_checkpoint_resume_bit_exact(lib):
     net, cfg, drive = nets.izh_stdp(n=10_000, k=50)
     a = gpu_run(net, cfg, drive, 400)

@@ -167,6 +167,38 @@ def test_conductance_ref_all_types_stdp_homeostasis_fast_vs_literal(oracle_lib):
     assert np.count_nonzero(f.weights() != net.w.astype(np.float64)) > 50
 
 
+@pytest.mark.parametrize("which", ["default", "all_types"])
+def test_lfp_fast_vs_literal(oracle_lib, which):
+    # lfp_signal (engine.rs:492): the reference sums |g (E_rev - V)| per
+    # synapse after each step's delivery; the reformulated engine sums per
+    # neuron and type at the next update, then adds the last step's term.
+    # Per-type sums equal per-synapse sums while each type's conductances
+    # share one sign (excitatory weights > 0; GABA types take |w|).
+    if which == "default":
+        net, cfg, drive = nets.lif_reference_default(n=300, stdp=False, homeo=False, conductance=True)
+    else:
+        net, cfg, drive = nets.lif_conductance_all_types(n=300)
+    f = FastOracle(net, cfg, drive, precision=64)
+    l = LiteralOracle(net, cfg, drive, threads=2)
+    done = 0
+    for k in (1, 9, 40, 100):
+        f.step(k - done)
+        l.step(k - done)
+        done = k
+        ref = l.stats()["lfp"]
+        assert f.lfp() == pytest.approx(ref, rel=1e-12, abs=1e-9)
+    assert ref > 1e6
+    # reading it consumes nothing
+    assert f.lfp() == f.lfp()
+
+
+def test_lfp_zero_outside_reference_conductance_mode(oracle_lib):
+    net, cfg, drive = nets.lif_reference_default(n=300, stdp=False, homeo=False)
+    f = FastOracle(net, cfg, drive, precision=32)
+    f.step(50)
+    assert f.lfp() == 0.0
+
+
 def test_reward_sum_is_sum_of_rewards(oracle_lib):
     net, cfg, drive = nets.izh_rstdp(n=1500, k=40)
     f = FastOracle(net, cfg, drive, precision=64)
