@@ -24,6 +24,8 @@
 using ns::NsDev;
 
 struct ns_handle {
+  void* stage = nullptr;            // pinned host staging of neuron uploads
+  size_t stage_bytes = 0;
   ns_config cfg{};
   ns_drive drive{};
   int dev = 0;
@@ -236,15 +238,23 @@ __global__ void k_check_rows(const uint64_t* rp, uint64_t n, uint64_t m, unsigne
   if (rp[j] > rp[j + 1] || rp[j + 1] > m) atomicOr(bad, 1u);
 }
 
+// also ORs the set of synapse types present into *types (one atomic per warp)
 __global__ void k_check_syn(const uint32_t* col, const float* w, const uint8_t* ty, uint64_t m,
-                            uint64_t n, unsigned int* bad) {
+                            uint64_t n, unsigned int* bad, unsigned int* types) {
+  unsigned int tm = 0u;
   for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < m;
        e += (uint64_t)gridDim.x * blockDim.x) {
     if (col[e] >= n) atomicOr(bad, 2u);
     float x = w[e];
     if (!(fabsf(x) < 4194304.0f)) atomicOr(bad, 4u);  // finite and |w| < 2^22
-    if (ty && ty[e] > 3) atomicOr(bad, 8u);
+    if (ty) {
+      const unsigned int t = ty[e];
+      if (t > 3) atomicOr(bad, 8u);
+      tm |= 1u << (t & 3u);
+    }
   }
+  tm = __reduce_or_sync(0xffffffffu, tm);
+  if ((threadIdx.x & 31) == 0 && tm) atomicOr(types, tm);
 }
 
 // per-row classification of plastic flags and synapse types
@@ -282,21 +292,28 @@ __global__ void k_from_bf16(const uint16_t* in, float* out, uint64_t m) {
 }
 
 // keys (target) and values (CSR position) of the synapses to index
-__global__ void k_in_keys(const uint32_t* col, const uint8_t* pl, uint64_t m, uint32_t* keys,
-                          uint32_t* vals, unsigned long long* cnt, int only_plastic) {
+// (target, position) pairs in position order; a synapse left out of the
+// list gets the key n, which a stable sort by target moves past the end
+__global__ void k_in_keys(const uint32_t* col, const uint8_t* pl, uint64_t m, uint32_t n,
+                          uint32_t* keys, uint32_t* vals, int only_plastic) {
   for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < m;
        e += (uint64_t)gridDim.x * blockDim.x) {
-    if (only_plastic && !(pl && pl[e])) continue;
-    unsigned long long q = atomicAdd(cnt, 1ull);
-    keys[q] = col[e];
-    vals[q] = (uint32_t)e;
+    const bool keep = !only_plastic || (pl && pl[e]);
+    keys[e] = keep ? col[e] : n;
+    vals[e] = (uint32_t)e;
   }
 }
 
-__global__ void k_count_keys(const uint32_t* keys, uint64_t cnt, uint64_t* deg) {
-  for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < cnt;
-       q += (uint64_t)gridDim.x * blockDim.x)
-    atomicAdd((unsigned long long*)&deg[keys[q]], 1ull);
+// ptr[j] = first index of sorted keys with key >= j, j = 0..n: each q in
+// [0, m] sets the j in (keys[q-1], keys[q]] (keys[-1] = -1, keys[m] = n + 1)
+__global__ void k_lower_bounds(const uint32_t* keys, uint64_t m, uint32_t n, uint64_t* ptr) {
+  for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q <= m;
+       q += (uint64_t)gridDim.x * blockDim.x) {
+    const int64_t prev = q == 0 ? -1 : (int64_t)keys[q - 1];
+    const int64_t cur = q == m ? (int64_t)n + 1 : (int64_t)keys[q];
+    const int64_t hi = cur < (int64_t)n ? cur : (int64_t)n;
+    for (int64_t j = prev + 1; j <= hi; ++j) ptr[j] = q;
+  }
 }
 
 __global__ void k_in_list(const uint32_t* pos, uint64_t cnt, const uint64_t* rp, uint64_t n,
@@ -374,67 +391,54 @@ ns_status build_incoming(ns_handle* h, std::vector<void*>& bag, const uint64_t* 
                          uint64_t** out_ptr, uint32_t** out_pos, uint2** out_list) {
   const uint64_t n = h->n, m = h->m;
   uint32_t *keys = nullptr, *vals = nullptr, *keys2 = nullptr, *vals2 = nullptr;
-  unsigned long long* cnt_d = nullptr;
   std::vector<void*> tmp;
   ns_status s;
+  uint64_t* ptr = nullptr;
+  if ((s = dalloc(h, bag, &ptr, n + 1))) return s;
+  if (m == 0) {
+    if (out_list) *out_list = nullptr;
+    if (out_pos) *out_pos = nullptr;
+    *out_ptr = ptr;
+    CK(cudaStreamSynchronize(h->st));
+    return NS_OK;
+  }
   if ((s = dalloc(h, tmp, &keys, m)) || (s = dalloc(h, tmp, &vals, m)) ||
-      (s = dalloc(h, tmp, &keys2, m)) || (s = dalloc(h, tmp, &vals2, m)) ||
-      (s = dalloc(h, tmp, &cnt_d, 1))) {
+      (s = dalloc(h, tmp, &keys2, m)) || (s = dalloc(h, tmp, &vals2, m))) {
     free_bag(tmp);
     return s;
   }
   const int grid = h->sms * 8;
-  k_in_keys<<<grid, 256, 0, h->st>>>(colp, d_pl, m, keys, vals, cnt_d, only_plastic);
-  unsigned long long cnt = 0;
-  CK(cudaMemcpyAsync(&cnt, cnt_d, 8, cudaMemcpyDeviceToHost, h->st));
+  k_in_keys<<<grid, 256, 0, h->st>>>(colp, d_pl, m, (uint32_t)n, keys, vals, only_plastic);
+  // one stable radix sort by target over the bits of n: positions stay
+  // ascending within a target, left-out synapses (key n) go last
+  int end_bit = 1;
+  while (end_bit < 32 && (n >> end_bit) != 0) ++end_bit;
+  size_t tb = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, tb, keys, keys2, vals, vals2, (int64_t)m, 0, end_bit, h->st);
+  void* tstore = nullptr;
+  CK(cudaMalloc(&tstore, std::max<size_t>(tb, 16)));
+  tmp.push_back(tstore);
+  cub::DeviceRadixSort::SortPairs(tstore, tb, keys, keys2, vals, vals2, (int64_t)m, 0, end_bit, h->st);
+  // keys2 = targets sorted (n past the list), vals2 = positions
+  k_lower_bounds<<<grid, 256, 0, h->st>>>(keys2, m, (uint32_t)n, ptr);
+  uint64_t cnt = 0;
+  CK(cudaMemcpyAsync(&cnt, ptr + n, 8, cudaMemcpyDeviceToHost, h->st));
   CK(cudaStreamSynchronize(h->st));
-  uint64_t* ptr = nullptr;
-  if ((s = dalloc(h, bag, &ptr, n + 1))) { free_bag(tmp); return s; }
+  if (out_list) *out_list = nullptr;
+  if (out_pos) *out_pos = nullptr;
   if (cnt > 0) {
-    // sort pairs by (target, position): first by position (already grouped
-    // arbitrarily), then a stable sort by target keeps position order
-    size_t tb = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, tb, vals, vals2, keys, keys2, (int64_t)cnt, 0, 32, h->st);
-    void* tstore = nullptr;
-    CK(cudaMalloc(&tstore, tb));
-    tmp.push_back(tstore);
-    cub::DeviceRadixSort::SortPairs(tstore, tb, vals, vals2, keys, keys2, (int64_t)cnt, 0, 32, h->st);
-    // vals2 = sorted positions, keys2 = their targets
-    size_t tb2 = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, tb2, keys2, keys, vals2, vals, (int64_t)cnt, 0, 32, h->st);
-    if (tb2 > tb) {
-      void* t2 = nullptr;
-      CK(cudaMalloc(&t2, tb2));
-      tmp.push_back(t2);
-      tstore = t2;
-      tb = tb2;
-    }
-    cub::DeviceRadixSort::SortPairs(tstore, tb, keys2, keys, vals2, vals, (int64_t)cnt, 0, 32, h->st);
-    // keys = targets sorted, vals = positions (ascending within a target)
-    uint64_t* deg = nullptr;
-    if ((s = dalloc(h, tmp, &deg, n + 1))) { free_bag(tmp); return s; }
-    k_count_keys<<<grid, 256, 0, h->st>>>(keys, cnt, deg + 1);
-    size_t tb3 = 0;
-    cub::DeviceScan::InclusiveSum(nullptr, tb3, deg, ptr, (int64_t)(n + 1), h->st);
-    void* t3 = nullptr;
-    CK(cudaMalloc(&t3, tb3));
-    tmp.push_back(t3);
-    cub::DeviceScan::InclusiveSum(t3, tb3, deg, ptr, (int64_t)(n + 1), h->st);
     if (out_list) {
       uint2* lst = nullptr;
       if ((s = dalloc(h, bag, &lst, cnt))) { free_bag(tmp); return s; }
-      k_in_list<<<grid, 256, 0, h->st>>>(vals, cnt, rowp, n, lst);
+      k_in_list<<<grid, 256, 0, h->st>>>(vals2, cnt, rowp, n, lst);
       *out_list = lst;
     }
     if (out_pos) {
       uint32_t* pos = nullptr;
       if ((s = dalloc(h, bag, &pos, cnt))) { free_bag(tmp); return s; }
-      CK(cudaMemcpyAsync(pos, vals, cnt * 4, cudaMemcpyDeviceToDevice, h->st));
+      CK(cudaMemcpyAsync(pos, vals2, cnt * 4, cudaMemcpyDeviceToDevice, h->st));
       *out_pos = pos;
     }
-  } else {
-    if (out_list) *out_list = nullptr;
-    if (out_pos) *out_pos = nullptr;
   }
   CK(cudaStreamSynchronize(h->st));
   free_bag(tmp);
@@ -1147,6 +1151,7 @@ ns_status ns_destroy(ns_handle* h) {
   free_bag(h->stp_allocs);
   if (h->nccl) g_nccl.comm_destroy(h->nccl);
   if (h->ctl) cudaFree(h->ctl);
+  if (h->stage) cudaFreeHost(h->stage);
   if (h->st2) cudaStreamSynchronize(h->st2);
   if (h->ev_rows) cudaEventDestroy(h->ev_rows);
   if (h->ev_ltd) cudaEventDestroy(h->ev_ltd);
@@ -1209,49 +1214,93 @@ ns_status ns_upload_neurons(ns_handle* h, const ns_neuron_soa* s) {
   h->n_pad = (uint64_t)h->ntiles * ns::kTile;
   const uint64_t np = h->n_pad;
   const uint32_t model = h->cfg.model;
-  // host staging (padded)
-  for (uint64_t q = 0; q < n * (uint64_t)ppn; ++q)
-    if (!is_fin(s->params[q])) return fail(h, NS_ERR_NONFINITE, "non-finite neuron parameter");
+  // host staging (padded) in the handle's pinned buffer, one region per
+  // device array, filled in parallel; checks are gathered as flag bits
   const int npar = model == NS_MODEL_LIF ? 5 : ppn;
-  std::vector<std::vector<float>> par(npar, std::vector<float>(np, 0.0f));
-  std::vector<int32_t> rsteps(np, 0);
-  std::vector<float> v(np), u(np, 0.0f), I(np, 0.0f), gm(np, 0.05f), gh(np, 0.6f), gn(np, 0.32f);
-  for (uint64_t i = 0; i < n; ++i) {
+  size_t off = 0;
+  auto region = [&](size_t bytes) { size_t at = off; off += (bytes + 255) & ~(size_t)255; return at; };
+  const size_t o_v = region(np * 4), o_u = region(np * 4), o_I = region(np * 4);
+  const size_t o_gm = region(np * 4), o_gh = region(np * 4), o_gn = region(np * 4);
+  const size_t o_refr = region(np * 4), o_rs = region(np * 4);
+  const size_t o_inh = region(np), o_out = region(np);
+  const size_t o_pre = region(np * 4), o_post = region(np * 4), o_last = region(np * 8);
+  size_t o_par[7];
+  for (int q = 0; q < npar; ++q) o_par[q] = region(np * 4);
+  if (off > h->stage_bytes) {
+    if (h->stage) cudaFreeHost(h->stage);
+    h->stage = nullptr;
+    h->stage_bytes = 0;
+    cudaError_t e = cudaMallocHost(&h->stage, off);
+    if (e != cudaSuccess) {
+      h->stage = nullptr;
+      return fail(h, NS_ERR_OOM, std::string("cudaMallocHost: ") + cudaGetErrorString(e));
+    }
+    h->stage_bytes = off;
+  }
+  char* const sb = (char*)h->stage;
+  float* const v = (float*)(sb + o_v);
+  float* const u = (float*)(sb + o_u);
+  float* const I = (float*)(sb + o_I);
+  float* const gm = (float*)(sb + o_gm);
+  float* const gh = (float*)(sb + o_gh);
+  float* const gn = (float*)(sb + o_gn);
+  int32_t* const refr = (int32_t*)(sb + o_refr);
+  int32_t* const rsteps = (int32_t*)(sb + o_rs);
+  uint8_t* const inh = (uint8_t*)(sb + o_inh);
+  uint8_t* const outp = (uint8_t*)(sb + o_out);
+  float* const pre = (float*)(sb + o_pre);
+  float* const post = (float*)(sb + o_post);
+  long long* const last = (long long*)(sb + o_last);
+  float* par[7] = {};
+  for (int q = 0; q < npar; ++q) par[q] = (float*)(sb + o_par[q]);
+  const double dt_ms = h->cfg.dt_ms;
+  unsigned int bad = 0u;  // 1 non-finite parameter, 2 tau_m zero, 4 c_m zero, 8 non-finite state
+#pragma omp parallel for schedule(static) reduction(| : bad) if (np >= (1u << 16))
+  for (int64_t ii = 0; ii < (int64_t)np; ++ii) {
+    const uint64_t i = (uint64_t)ii;
+    if (i >= n) {
+      // padded neurons stay quiet: LIF with tau 1, rest 0, huge threshold
+      for (int q = 0; q < npar; ++q) par[q][i] = 0.0f;
+      if (model == NS_MODEL_LIF) { par[1][i] = 1e30f; par[3][i] = 1.0f; }
+      if (model == NS_MODEL_HH) par[6][i] = 1.0f;
+      v[i] = model == NS_MODEL_HH ? -65.0f : 0.0f;
+      u[i] = 0.0f; I[i] = 0.0f; gm[i] = 0.05f; gh[i] = 0.6f; gn[i] = 0.32f;
+      refr[i] = 0; rsteps[i] = 0; inh[i] = 0; outp[i] = 0;
+      pre[i] = 0.0f; post[i] = 0.0f; last[i] = -1;
+      continue;
+    }
     const float* p = s->params + i * ppn;
+    for (int q = 0; q < ppn; ++q)
+      if (!is_fin(p[q])) bad |= 1u;
     if (model == NS_MODEL_LIF) {
       par[0][i] = p[0]; par[1][i] = p[1]; par[2][i] = p[2]; par[3][i] = p[3]; par[4][i] = p[5];
-      rsteps[i] = (int32_t)std::round((double)p[4] / h->cfg.dt_ms);  // lif.rs:50
-      if (!(p[3] != 0.0f)) return fail(h, NS_ERR_INVALID_ARG, "tau_m must be nonzero");
+      rsteps[i] = (int32_t)std::round((double)p[4] / dt_ms);  // lif.rs:50
+      if (!(p[3] != 0.0f)) bad |= 2u;
     } else {
       for (int q = 0; q < ppn; ++q) par[q][i] = p[q];
-      if (model == NS_MODEL_HH && !(p[6] != 0.0f)) return fail(h, NS_ERR_INVALID_ARG, "c_m must be nonzero");
+      rsteps[i] = 0;
+      if (model == NS_MODEL_HH && !(p[6] != 0.0f)) bad |= 4u;
     }
-    float rest = model == NS_MODEL_LIF ? p[0] : (model == NS_MODEL_IZHIKEVICH ? p[2] : p[5]);
+    const float rest = model == NS_MODEL_LIF ? p[0] : (model == NS_MODEL_IZHIKEVICH ? p[2] : p[5]);
     v[i] = s->v ? s->v[i] : rest;
-    if (s->u) u[i] = s->u[i];
-    if (s->current) I[i] = s->current[i];
-    if (s->hh_m) gm[i] = s->hh_m[i];
-    if (s->hh_h) gh[i] = s->hh_h[i];
-    if (s->hh_n) gn[i] = s->hh_n[i];
+    u[i] = s->u ? s->u[i] : 0.0f;
+    I[i] = s->current ? s->current[i] : 0.0f;
+    gm[i] = s->hh_m ? s->hh_m[i] : 0.05f;
+    gh[i] = s->hh_h ? s->hh_h[i] : 0.6f;
+    gn[i] = s->hh_n ? s->hh_n[i] : 0.32f;
     if (!is_fin(v[i]) || !is_fin(u[i]) || !is_fin(I[i]) || !is_fin(gm[i]) || !is_fin(gh[i]) || !is_fin(gn[i]))
-      return fail(h, NS_ERR_NONFINITE, "non-finite initial state");
+      bad |= 8u;
+    refr[i] = s->refractory ? s->refractory[i] : 0;
+    inh[i] = s->inhibitory ? (s->inhibitory[i] ? 1 : 0) : 0;
+    outp[i] = s->is_output ? (s->is_output[i] ? 1 : 0) : 0;
+    pre[i] = s->pre_trace ? s->pre_trace[i] : 0.0f;
+    post[i] = s->post_trace ? s->post_trace[i] : 0.0f;
+    last[i] = s->last_spike_step ? s->last_spike_step[i] : -1;
   }
-  // padded neurons stay quiet: LIF with tau 1, rest 0, huge threshold
-  for (uint64_t i = n; i < np; ++i) {
-    v[i] = 0.0f;
-    if (model == NS_MODEL_LIF) { par[1][i] = 1e30f; par[3][i] = 1.0f; }
-    if (model == NS_MODEL_HH) { par[6][i] = 1.0f; v[i] = -65.0f; }
-  }
-  std::vector<int32_t> refr(np, 0);
-  if (s->refractory) for (uint64_t i = 0; i < n; ++i) refr[i] = s->refractory[i];
-  std::vector<uint8_t> inh(np, 0), outp(np, 0);
-  if (s->inhibitory) for (uint64_t i = 0; i < n; ++i) inh[i] = s->inhibitory[i] ? 1 : 0;
-  if (s->is_output) for (uint64_t i = 0; i < n; ++i) outp[i] = s->is_output[i] ? 1 : 0;
-  std::vector<float> pre(np, 0.0f), post(np, 0.0f);
-  if (s->pre_trace) for (uint64_t i = 0; i < n; ++i) pre[i] = s->pre_trace[i];
-  if (s->post_trace) for (uint64_t i = 0; i < n; ++i) post[i] = s->post_trace[i];
-  std::vector<long long> last(np, -1);
-  if (s->last_spike_step) for (uint64_t i = 0; i < n; ++i) last[i] = s->last_spike_step[i];
+  if (bad & 1u) return fail(h, NS_ERR_NONFINITE, "non-finite neuron parameter");
+  if (bad & 2u) return fail(h, NS_ERR_INVALID_ARG, "tau_m must be nonzero");
+  if (bad & 4u) return fail(h, NS_ERR_INVALID_ARG, "c_m must be nonzero");
+  if (bad & 8u) return fail(h, NS_ERR_NONFINITE, "non-finite initial state");
 
   NsDev& d = h->d;
   ns_status st;
@@ -1274,13 +1323,13 @@ ns_status ns_upload_neurons(ns_handle* h, const ns_neuron_soa* s) {
   auto up = [&](void* dst, const void* src, size_t bytes) {
     return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->st);
   };
-  CK(up(d.v, v.data(), np * 4)); CK(up(d.u, u.data(), np * 4)); CK(up(d.I, I.data(), np * 4));
-  CK(up(d.gm, gm.data(), np * 4)); CK(up(d.gh, gh.data(), np * 4)); CK(up(d.gn, gn.data(), np * 4));
-  CK(up(d.refr, refr.data(), np * 4)); CK(up(d.refr_steps, rsteps.data(), np * 4));
-  CK(up(d.inh, inh.data(), np)); CK(up(d.outp, outp.data(), np));
-  CK(up(d.pre, pre.data(), np * 4)); CK(up(d.post, post.data(), np * 4));
-  CK(up(d.last, last.data(), np * 8));
-  for (int q = 0; q < npar; ++q) CK(up(d.par[q], par[q].data(), np * 4));
+  CK(up(d.v, v, np * 4)); CK(up(d.u, u, np * 4)); CK(up(d.I, I, np * 4));
+  CK(up(d.gm, gm, np * 4)); CK(up(d.gh, gh, np * 4)); CK(up(d.gn, gn, np * 4));
+  CK(up(d.refr, refr, np * 4)); CK(up(d.refr_steps, rsteps, np * 4));
+  CK(up(d.inh, inh, np)); CK(up(d.outp, outp, np));
+  CK(up(d.pre, pre, np * 4)); CK(up(d.post, post, np * 4));
+  CK(up(d.last, last, np * 8));
+  for (int q = 0; q < npar; ++q) CK(up(d.par[q], par[q], np * 4));
   {
     // parameter dictionary: at most 256 distinct rows (by bit pattern) give
     // the neuron kernel a 1-byte index per neuron instead of its rows
@@ -1288,10 +1337,14 @@ ns_status ns_upload_neurons(ns_handle* h, const ns_neuron_soa* s) {
     std::vector<uint8_t> pidx(np);
     std::vector<float> ptab;
     bool ok = true;
+    std::array<uint32_t, 8> prev{};
+    uint32_t prev_idx = 0;
+    bool have_prev = false;
     for (uint64_t i = 0; i < np && ok; ++i) {
       std::array<uint32_t, 8> key{};
       for (int q = 0; q < npar; ++q) std::memcpy(&key[q], &par[q][i], 4);
       if (model == NS_MODEL_LIF) std::memcpy(&key[7], &rsteps[i], 4);
+      if (have_prev && key == prev) { pidx[i] = (uint8_t)prev_idx; continue; }
       auto it = rows.find(key);
       if (it == rows.end()) {
         if (rows.size() == 256) { ok = false; break; }
@@ -1301,6 +1354,9 @@ ns_status ns_upload_neurons(ns_handle* h, const ns_neuron_soa* s) {
         std::memcpy(ptab.data() + at, key.data(), 32);
       }
       pidx[i] = (uint8_t)it->second;
+      prev = key;
+      prev_idx = it->second;
+      have_prev = true;
     }
     const uint8_t* want = ok ? h->pidx_buf : nullptr;
     if (want != d.pidx) drop_graphs(h);  // the kernel variant changes
@@ -1452,7 +1508,7 @@ ns_status ns_upload_csr(ns_handle* h, uint64_t n, uint64_t m, const uint64_t* ro
   float* wt = nullptr;
   uint8_t *ty = nullptr, *pl = nullptr;
   unsigned int* bad = nullptr;
-  if ((st = dalloc(h, tmp, &wt, h->m_pad)) || (st = dalloc(h, tmp, &bad, 2))) { free_bag(tmp); undo(); return st; }
+  if ((st = dalloc(h, tmp, &wt, h->m_pad)) || (st = dalloc(h, tmp, &bad, 3))) { free_bag(tmp); undo(); return st; }
   if (m) CK(cudaMemcpyAsync(wt, w, m * 4, cudaMemcpyHostToDevice, h->st));
   if (syn_type) {
     if ((st = dalloc(h, tmp, &ty, h->m_pad))) { free_bag(tmp); undo(); return st; }
@@ -1464,11 +1520,12 @@ ns_status ns_upload_csr(ns_handle* h, uint64_t n, uint64_t m, const uint64_t* ro
   }
   const int grid = h->sms * 8;
   k_check_rows<<<(unsigned)((n + 255) / 256), 256, 0, h->st>>>(rp, n, m, bad);
-  if (m) k_check_syn<<<grid, 256, 0, h->st>>>(cl, wt, ty, m, n, bad);
-  unsigned int badh = 0;
-  CK(cudaMemcpyAsync(&badh, bad, 4, cudaMemcpyDeviceToHost, h->st));
+  if (m) k_check_syn<<<grid, 256, 0, h->st>>>(cl, wt, ty, m, n, bad, bad + 2);
+  unsigned int flags[3] = {0u, 0u, 0u};
+  CK(cudaMemcpyAsync(flags, bad, 12, cudaMemcpyDeviceToHost, h->st));
   CK(cudaStreamSynchronize(h->st));
   CK(cudaGetLastError());
+  const unsigned int badh = flags[0];
   if (badh) {
     free_bag(tmp);
     undo();
@@ -1479,9 +1536,7 @@ ns_status ns_upload_csr(ns_handle* h, uint64_t n, uint64_t m, const uint64_t* ro
   }
   // synapse types present: the conductance kernels skip the rows of the others
   {
-    uint32_t mask = 0u;
-    if (syn_type) for (uint64_t e = 0; e < m && mask != 15u; ++e) mask |= 1u << (syn_type[e] & 3u);
-    else mask = m ? 1u : 0u;
+    const uint32_t mask = syn_type ? flags[2] : (m ? 1u : 0u);
     if (mask != h->type_mask) drop_graphs(h);  // captured launches carry the mask
     h->type_mask = mask;
   }
