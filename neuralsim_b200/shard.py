@@ -150,6 +150,10 @@ class VirtualShards:
         """Synaptic events of all ranks (each walks its own targets)."""
         return sum(int(e.counters()[3]) for e in self.ranks)
 
+    def lfp(self):
+        """lfp_signal of the network: the ranks' sums over their own neurons."""
+        return sum(e.lfp() for e in self.ranks)
+
     def close(self):
         for e in self.ranks:
             e.close()
@@ -183,6 +187,11 @@ class ShardedEngine:
 
     def run(self, steps):
         return self.engine.run(steps)
+
+    def lfp(self):
+        """This rank's share of lfp_signal (its own neurons); the network's
+        value is the sum over ranks."""
+        return self.engine.lfp()
 
     def close(self):
         self.engine.close()

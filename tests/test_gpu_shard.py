@@ -50,6 +50,16 @@ def test_sharded_reference_engine_with_phase2_rules(lib):
     assert np.array_equal(e, one.eligibility())
 
 
+def test_sharded_reference_conductance_mode_and_lfp(lib):
+    # the reference conductance mode with all four synapse types: rasters,
+    # state and conductance-driven dynamics equal; the LFP is each rank's
+    # sum over its own neurons, so only the FP64 summation order differs
+    net, cfg, drive = nets.lif_conductance_all_types(n=6000)
+    one, vs = compare(net, cfg, drive, 120, 2)
+    assert one.lfp() > 1e6
+    assert vs.lfp() == pytest.approx(one.lfp(), rel=1e-12)
+
+
 def test_sharded_rank_rejects_foreign_synapses(lib):
     net, cfg, drive = nets.izh_stdp(n=6000, k=20)
     part, _ = partition_network(net, 0, 2)
