@@ -163,46 +163,44 @@ __device__ __forceinline__ bool bit_of(const uint32_t* bm, uint32_t i) {
   return (bm[i >> 5] >> (i & 31)) & 1u;
 }
 
-// exclusive scan of n values by one 256-thread block (chunks of 1024), result
-// in out[0..n]; returns the total
+// exclusive scan of n values by one 256-thread block, result in out[0..n];
+// returns the total. Thread t owns a contiguous run of ceil(n / 256) values:
+// it sums the run (independent loads, two round trips for the whole scan
+// rather than one per 1024 values), the block scans the 256 sums, and the
+// thread writes the run's offsets (its second read of the run hits L1).
 __device__ uint32_t block_scan_u32(const uint32_t* in, uint32_t* out, uint32_t n) {
   __shared__ uint32_t s_w[8];
-  __shared__ uint32_t s_carry;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  if (tid == 0) s_carry = 0;
-  __syncthreads();
-  for (uint32_t b0 = 0; b0 < n; b0 += 1024) {
-    uint32_t v[4], loc = 0;
+  const uint32_t per = (n + 255u) / 256u;
+  const uint32_t b = min(n, (uint32_t)tid * per), e = min(n, b + per);
+  uint32_t loc = 0;
+#pragma unroll 8
+  for (uint32_t q = b; q < e; ++q) loc += in[q];
+  uint32_t inc = loc;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const uint32_t idx = b0 + 4u * tid + q;
-      v[q] = idx < n ? in[idx] : 0u;
-      loc += v[q];
-    }
-    uint32_t inc = loc;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
-      if (lane >= o) inc += y;
-    }
-    if (lane == 31) s_w[warp] = inc;
-    __syncthreads();
-    uint32_t wpre = 0;
-    for (int q = 0; q < warp; ++q) wpre += s_w[q];
-    uint32_t run = s_carry + wpre + inc - loc;
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const uint32_t idx = b0 + 4u * tid + q;
-      if (idx < n) out[idx] = run;
-      run += v[q];
-    }
-    __syncthreads();
-    if (tid == 255) s_carry = run;
-    __syncthreads();
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += y;
   }
-  if (tid == 0) out[n] = s_carry;
+  if (lane == 31) s_w[warp] = inc;
   __syncthreads();
-  return s_carry;
+  uint32_t wpre = 0, tot = 0;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const uint32_t x = s_w[q];
+    wpre += q < warp ? x : 0u;
+    tot += x;
+  }
+  uint32_t run = wpre + inc - loc;
+#pragma unroll 8
+  for (uint32_t q = b; q < e; ++q) {
+    const uint32_t x = in[q];
+    out[q] = run;
+    run += x;
+  }
+  if (tid == 0) out[n] = tot;
+  __syncthreads();
+  return tot;
 }
 
 // ---------------------------------------------------------------------------
@@ -1315,7 +1313,10 @@ __global__ void __launch_bounds__(256) k_lfp_pending(NsDev d, unsigned long long
   const uint64_t k = d.ctl->step_base;
   const uint32_t slot = (uint32_t)(k % d.D);
   long long acc = 0;
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < d.n;
+  // this rank's neurons (all of them without sharding)
+  const uint64_t lo = (uint64_t)d.tile0 * kTile;
+  const uint64_t hi = min((uint64_t)(d.tile0 + d.tiles_own) * kTile, d.n);
+  for (uint64_t i = lo + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < hi;
        i += (uint64_t)gridDim.x * blockDim.x) {
     const float vi = d.v[i];
     float lf = 0.f;
