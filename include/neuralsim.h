@@ -311,6 +311,17 @@ ns_status ns_weight_stats(ns_handle* h, double* mean, double* stddev);
  * neuron's per-type conductance stands for the sum of its synapses'
  * (conductances are >= 0: GABA types take |w|). */
 ns_status ns_get_lfp(ns_handle* h, double* lfp);
+/* Host stimulus: adds amounts[q] to the input current of neuron ids[q]
+ * (SimulationEngine::stimulate, engine.rs:156-161; the host-side edit that
+ * GpuBackend::upload_input_current carries, gpu_backend.rs). Amounts are
+ * summed per neuron in call order (as float) and join the input current of
+ * the next step after the synaptic input, before that step's drive. In the
+ * modes whose input current is state (DIRECT_DECAY, CONDUCTANCE_REF) it then
+ * stays and decays as the reference's input_current does; in the others it
+ * acts for one step. A sharded rank keeps the ids it owns. Refused while a
+ * learned HH macro-step is attached. */
+ns_status ns_add_input_current(ns_handle* h, uint64_t count, const uint32_t* ids,
+                               const double* amounts);
 
 /* --- the rest of phase 2: R-STDP eligibility and reward, short-term
  *     plasticity (engine.rs:457-463, :519-563, :626-631) ---------------- */

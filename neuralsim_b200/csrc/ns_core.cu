@@ -78,6 +78,13 @@ struct ns_handle {
   uint32_t shard_rank = 0, shard_world = 0;
   ncclComm_t nccl = nullptr;
   uint32_t type_mask = 1u;          // synapse types present in the CSR (bit per type)
+  // host stimulus pending for the next step: values summed in call order
+  // (float), the distinct ids touched, and a device staging buffer
+  std::vector<float> stim_acc;
+  std::vector<uint8_t> stim_mark;
+  std::vector<uint32_t> stim_ids;
+  void* stim_dev = nullptr;
+  size_t stim_dev_cap = 0;          // entries
 };
 
 namespace {
@@ -1152,6 +1159,7 @@ ns_status ns_destroy(ns_handle* h) {
   if (h->nccl) g_nccl.comm_destroy(h->nccl);
   if (h->ctl) cudaFree(h->ctl);
   if (h->stage) cudaFreeHost(h->stage);
+  if (h->stim_dev) cudaFree(h->stim_dev);
   if (h->st2) cudaStreamSynchronize(h->st2);
   if (h->ev_rows) cudaEventDestroy(h->ev_rows);
   if (h->ev_ltd) cudaEventDestroy(h->ev_ltd);
@@ -1317,7 +1325,7 @@ ns_status ns_upload_neurons(ns_handle* h, const ns_neuron_soa* s) {
     for (int t = 0; t < 4; ++t) DA(d.G[t], np)
     DA(d.bitmap, np / 32 + 2) DA(d.spk, 2 * np)
     DA(d.tile_cnt, 2 * ((uint64_t)h->ntiles + 1)) DA(d.tile_off, 2 * ((uint64_t)h->ntiles + 1))
-    DA(h->pidx_buf, np) DA(h->ptab_buf, 256 * 8)
+    DA(h->pidx_buf, np) DA(h->ptab_buf, 256 * 8) DA(d.stim, np)
 #undef DA
   }
   auto up = [&](void* dst, const void* src, size_t bytes) {
@@ -1383,6 +1391,10 @@ ns_status ns_upload_neurons(ns_handle* h, const ns_neuron_soa* s) {
   }
   CK(cudaStreamSynchronize(h->st));
   h->have_neurons = true;
+  // a new network drops any host stimulus still pending
+  h->stim_acc.assign(n, 0.0f);
+  h->stim_mark.assign(n, 0);
+  h->stim_ids.clear();
   if (h->have_csr) {
     ns_status r = alloc_dynamic(h);
     if (r) return r;
@@ -1756,6 +1768,44 @@ ns_status ns_upload_batch(ns_handle* h, uint32_t n_nets, const ns_net_desc* nets
   return NS_OK;
 }
 
+// The pending host stimulus goes to the device right before the next step
+// (one launch); that step's neuron kernel adds it to the input current.
+ns_status flush_stim(ns_handle* h) {
+  if (h->stim_ids.empty()) return NS_OK;
+  if (h->sur_on) {
+    h->stim_ids.clear();
+    std::fill(h->stim_acc.begin(), h->stim_acc.end(), 0.0f);
+    std::fill(h->stim_mark.begin(), h->stim_mark.end(), 0);
+    return fail(h, NS_ERR_UNSUPPORTED, "host stimulus with the learned HH macro-step attached (dropped)");
+  }
+  const size_t cnt = h->stim_ids.size();
+  if (cnt > h->stim_dev_cap) {
+    if (h->stim_dev) cudaFree(h->stim_dev);
+    h->stim_dev = nullptr;
+    h->stim_dev_cap = 0;
+    CK(cudaMalloc(&h->stim_dev, cnt * 8));
+    h->stim_dev_cap = cnt;
+  }
+  std::vector<uint32_t> ids;
+  ids.swap(h->stim_ids);
+  std::vector<float> vals(cnt);
+  for (size_t q = 0; q < cnt; ++q) {
+    vals[q] = h->stim_acc[ids[q]];
+    h->stim_acc[ids[q]] = 0.0f;
+    h->stim_mark[ids[q]] = 0;
+  }
+  uint32_t* dids = (uint32_t*)h->stim_dev;
+  float* dvals = (float*)((char*)h->stim_dev + h->stim_dev_cap * 4);
+  CK(cudaMemcpyAsync(dids, ids.data(), cnt * 4, cudaMemcpyHostToDevice, h->st));
+  CK(cudaMemcpyAsync(dvals, vals.data(), cnt * 4, cudaMemcpyHostToDevice, h->st));
+  const unsigned grid = (unsigned)std::min<size_t>((cnt + 255) / 256, (size_t)h->sms * 4);
+  ns::k_stim_apply<<<grid, 256, 0, h->st>>>(h->d, dids, dvals, (uint32_t)cnt);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(h->st));
+  h->launches += 1;
+  return NS_OK;
+}
+
 ns_status ns_step(ns_handle* h, uint32_t n_steps, ns_step_stats* out) {
   if (!h) return NS_ERR_NULL_HANDLE;
   ns_status r = ready(h);
@@ -1764,6 +1814,7 @@ ns_status ns_step(ns_handle* h, uint32_t n_steps, ns_step_stats* out) {
     return fail(h, NS_ERR_STATE, "sharded handle without NCCL: step with ns_shard_step_begin / ns_shard_step_end");
   CK(cudaSetDevice(h->dev));
   fill_scalars(h);
+  if (n_steps && (r = flush_stim(h))) return r;
   ns::Ctl before{};
   CK(cudaMemcpyAsync(&before, h->ctl, sizeof(before), cudaMemcpyDeviceToHost, h->st));
   uint32_t tuned = 0;
@@ -1793,6 +1844,7 @@ ns_status ns_step_traced(ns_handle* h, uint64_t* pos_out, uint64_t cap, uint64_t
   if (!n_events || (cap && !pos_out)) return fail(h, NS_ERR_INVALID_ARG, "null output");
   CK(cudaSetDevice(h->dev));
   fill_scalars(h);
+  if ((r = flush_stim(h))) return r;
   std::vector<void*> tmp;
   unsigned long long *off = nullptr, *pos = nullptr;
   ns_status st;
@@ -2315,6 +2367,7 @@ ns_status ns_profile_steps(ns_handle* h, uint32_t n_steps, double* kernel_ms, ui
   if (h->shard_world > 1) return fail(h, NS_ERR_UNSUPPORTED, "kernel profiles run on one GPU");
   CK(cudaSetDevice(h->dev));
   fill_scalars(h);
+  if (n_steps && (r = flush_stim(h))) return r;
   neuron_fn nf = pick_neuron(h->cfg.model, h->cfg.input_mode, h->d.pidx != nullptr);
   const bool ext = ext_on(h);
   prop_fn pf = pick_prop(h->cfg.input_mode, h->cfg.weight_format, ext);
@@ -2357,6 +2410,37 @@ ns_status ns_profile_steps(ns_handle* h, uint32_t n_steps, double* kernel_ms, ui
   for (auto& e : ev) cudaEventDestroy(e);
   h->launches += nl + 1 + (tail_on(h) ? (h->cfg.stdp_enabled ? 2u : 1u) * (uint64_t)n_steps : 0);
   return check_device_status(h);
+}
+
+ns_status ns_add_input_current(ns_handle* h, uint64_t count, const uint32_t* ids,
+                               const double* amounts) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  if (count && (!ids || !amounts)) return fail(h, NS_ERR_INVALID_ARG, "null ids or amounts");
+  if (!h->have_neurons) return fail(h, NS_ERR_STATE, "no neurons uploaded");
+  if (h->sur_on) return fail(h, NS_ERR_UNSUPPORTED, "host stimulus with the learned HH macro-step attached");
+  for (uint64_t q = 0; q < count; ++q) {
+    if (ids[q] >= h->n) return fail(h, NS_ERR_INVALID_ARG, "neuron id >= n");
+    if (!is_fin(amounts[q]) || !is_fin((float)amounts[q]))
+      return fail(h, NS_ERR_NONFINITE, "stimulus amount is not finite in float");
+  }
+  if (h->stim_acc.size() != h->n) {
+    h->stim_acc.assign(h->n, 0.0f);
+    h->stim_mark.assign(h->n, 0);
+    h->stim_ids.clear();
+  }
+  // a sharded rank keeps the stimulus of its own neurons
+  uint64_t lo = 0, hi = h->n;
+  if (h->shard_world > 1) ns_shard_range(h->n, h->shard_rank, h->shard_world, &lo, &hi);
+  for (uint64_t q = 0; q < count; ++q) {
+    const uint32_t i = ids[q];
+    if (i < lo || i >= hi) continue;
+    if (!h->stim_mark[i]) {
+      h->stim_mark[i] = 1;
+      h->stim_ids.push_back(i);
+    }
+    h->stim_acc[i] = h->stim_acc[i] + (float)amounts[q];
+  }
+  return NS_OK;
 }
 
 ns_status ns_get_lfp(ns_handle* h, double* lfp) {
@@ -2444,6 +2528,7 @@ ns_status ns_shard_step_begin(ns_handle* h) {
   if (h->shard_world == 0) return fail(h, NS_ERR_STATE, "not a sharded handle");
   CK(cudaSetDevice(h->dev));
   fill_scalars(h);
+  if ((r = flush_stim(h))) return r;
   if (h->sched == 0) h->sched = 3;
   neuron_fn nf = pick_neuron(h->cfg.model, h->cfg.input_mode, h->d.pidx != nullptr);
   nf<<<h->d.tiles_own, ns::kThreads, 0, h->st>>>(h->d, 0);

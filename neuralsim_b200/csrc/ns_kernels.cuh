@@ -60,6 +60,10 @@ struct Ctl {
   // FP64 total one step later
   long long lfp_step[4];
   double lfp_total;
+  // host stimulus (SimulationEngine::stimulate, engine.rs:156-161): the
+  // values in NsDev::stim join the input current at step stim_at - 1
+  // (0: none pending); the consuming thread zeroes them
+  unsigned long long stim_at;
 };
 
 struct Kick { uint32_t target; float amt; };
@@ -157,6 +161,7 @@ struct NsDev {
   float* elig;                     // eligibility values [m_pad]
   const uint8_t* elig_flag;        // synapse carries an eligibility trace [m_pad]
   const float* stp_f;              // STP factor per synapse, or null
+  float* stim;                     // pending host stimulus per neuron [n_pad]
 };
 
 __device__ __forceinline__ bool bit_of(const uint32_t* bm, uint32_t i) {
@@ -325,7 +330,7 @@ template <int MODEL, int MODE>
 __device__ __forceinline__ bool update_one(const NsDev& d, uint64_t k, uint64_t i, NState& st,
                                            const float* par, int rs, const float* S, float* G,
                                            float addI, float kick, float addg, const Kick* kicks,
-                                           int nk, float* lfp = nullptr) {
+                                           int nk, float stim = 0.f, float* lfp = nullptr) {
   float Iv = 0.f, kk = 0.f;
   const float vi = st.v;
   if (MODE == 0) {
@@ -351,6 +356,7 @@ __device__ __forceinline__ bool update_one(const NsDev& d, uint64_t k, uint64_t 
     }
     Iv = (MODE == 3) ? st.I + isyn : isyn;
   }
+  if (stim != 0.0f) Iv = Iv + stim;   // host stimulus, engine.rs:156-161
   Iv = Iv + addI;
   for (int q = 0; q < nk; ++q)
     if (kicks[q].target == (uint32_t)i) Iv = Iv + kicks[q].amt;
@@ -448,6 +454,7 @@ __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
     c->lfp_step[(k + 1) & 3] = 0ll;
   }
   long long lfp_fix = 0;
+  const bool stim_on = d.ctl->stim_at == k + 1;
   if (PT)
     for (uint32_t q = tid; q < d.ptab_rows * 8u; q += kThreads) s_tab[q] = __ldg(d.ptab + q);
   __syncthreads();
@@ -587,6 +594,12 @@ __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
       }
     }
     const uint8_t inhv[2] = {ih.x, ih.y};
+    float2 sti = make_float2(0.f, 0.f);
+    if (stim_on) {
+      sti = *reinterpret_cast<const float2*>(d.stim + i0);
+      if (sti.x != 0.0f || sti.y != 0.0f)
+        *reinterpret_cast<float2*>(d.stim + i0) = make_float2(0.f, 0.f);
+    }
     bool spk[2];
 #pragma unroll
     for (int e = 0; e < 2; ++e) {
@@ -600,7 +613,7 @@ __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
       for (int t = 0; t < 4; ++t) Ge[t] = COND ? G[t][e] : 0.f;
       float lf = 0.f;
       const bool sp = update_one<MODEL, MODE>(d, k, i, st[e], par[e], rs[e], Se, Ge, addI, kick,
-                                              addg, s_kick, nk, MODE == 3 ? &lf : nullptr);
+                                              addg, s_kick, nk, e == 0 ? sti.x : sti.y, MODE == 3 ? &lf : nullptr);
       if (MODE == 3) lfp_fix += __float2ll_rn(lf * 0x1p24f);
 #pragma unroll
       for (int t = 0; t < 4; ++t) if (COND) G[t][e] = Ge[t];
@@ -1333,6 +1346,14 @@ __global__ void __launch_bounds__(256) k_lfp_pending(NsDev d, unsigned long long
   }
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
   if ((threadIdx.x & 31) == 0 && acc) atomicAdd(out, (unsigned long long)acc);
+}
+
+// Pending host stimulus: distinct neuron ids, values accumulated on the
+// host in call order; they join the input current of the next step.
+__global__ void k_stim_apply(NsDev d, const uint32_t* ids, const float* vals, uint32_t cnt) {
+  for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < cnt; q += gridDim.x * blockDim.x)
+    d.stim[ids[q]] = d.stim[ids[q]] + vals[q];
+  if (blockIdx.x == 0 && threadIdx.x == 0) d.ctl->stim_at = d.ctl->step_base + 1;
 }
 
 __global__ void k_advance(Ctl* ctl, uint32_t steps) { ctl->step_base += steps; }

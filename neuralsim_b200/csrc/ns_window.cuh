@@ -62,6 +62,11 @@ __global__ void __launch_bounds__(kWinThreads, window_min_blocks<MODEL>()) k_win
   uint32_t dli;
   drive_key(d, i, dseed, dli);
   PoissonWords pw;
+  float stim0 = 0.f;
+  if (d.ctl->stim_at == k0 + 1) {
+    stim0 = d.stim[i];
+    if (stim0 != 0.0f) d.stim[i] = 0.f;
+  }
   const uint64_t words = d.n_pad >> 5;
   unsigned long long my_spk = 0;
   uint32_t slot = (uint32_t)(k0 % d.D);   // advanced by one (mod D) per step
@@ -128,8 +133,10 @@ __global__ void __launch_bounds__(kWinThreads, window_min_blocks<MODEL>()) k_win
     }
     float addI, kick, addg;
     drive_of(d, y, z, inh, addI, kick, addg);
+    const float stv = stim0;   // the host stimulus joins the window's first step
+    stim0 = 0.f;
     const bool sp = update_one<MODEL, MODE>(d, k, i, st, par, rs, S, G, addI, kick, addg,
-                                            s_kick, nk) && (i < d.n);
+                                            s_kick, nk, stv) && (i < d.n);
     if (sp) { d.last[i] = (long long)k; ++my_spk; }
     // compaction of this step's spikes into the segment, ascending
     const unsigned m = __ballot_sync(0xffffffffu, sp);

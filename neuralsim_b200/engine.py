@@ -324,6 +324,14 @@ class SimulationEngine:
         soa.params_per_neuron = PARAMS_PER_NEURON[self.config.model]
         self._check(self.lib.ns_upload_state(self._h, C.byref(soa), _ptr(st.get("w")), int(step)))
 
+    def stimulate(self, neuron_ids, currents):
+        """Adds currents to the input current of neurons before the next
+        step (SimulationEngine::stimulate, engine.rs:156-161); scalars or
+        equal-length sequences."""
+        ids = np.ascontiguousarray(np.atleast_1d(neuron_ids), dtype=np.uint32)
+        amt = np.ascontiguousarray(np.broadcast_to(np.atleast_1d(currents), ids.shape), dtype=np.float64)
+        self._check(self.lib.ns_add_input_current(self._h, ids.size, _ptr(ids), _ptr(amt)))
+
     def lfp(self) -> float:
         """lfp_signal (engine.rs:492) of the reference conductance mode."""
         x = C.c_double()

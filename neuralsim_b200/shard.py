@@ -154,6 +154,11 @@ class VirtualShards:
         """lfp_signal of the network: the ranks' sums over their own neurons."""
         return sum(e.lfp() for e in self.ranks)
 
+    def stimulate(self, neuron_ids, currents):
+        """Host stimulus: every rank keeps the neurons it owns."""
+        for e in self.ranks:
+            e.stimulate(neuron_ids, currents)
+
     def close(self):
         for e in self.ranks:
             e.close()
@@ -192,6 +197,11 @@ class ShardedEngine:
         """This rank's share of lfp_signal (its own neurons); the network's
         value is the sum over ranks."""
         return self.engine.lfp()
+
+    def stimulate(self, neuron_ids, currents):
+        """Host stimulus (every rank may pass the same list: each keeps the
+        neurons it owns)."""
+        self.engine.stimulate(neuron_ids, currents)
 
     def close(self):
         self.engine.close()

@@ -391,6 +391,16 @@ template <class R> struct Fast {
   // the FP64 total at the start of the next step.
   int64_t lfp_fix_prev = 0, lfp_fix_cur = 0;
   double lfp_d_prev = 0, lfp_d_cur = 0, lfp_total = 0;
+  // host stimulus (engine.rs:156-161) as the device applies it: amounts
+  // summed per neuron in call order, added to the input current of step
+  // stim_at - 1 after the synaptic input, before the drive
+  std::vector<R> stim;
+  uint64_t stim_at = 0;
+  void add_input_current(uint64_t cnt, const uint32_t* ids, const double* amounts) {
+    if (stim.size() != n) stim.assign(n, R(0));
+    for (uint64_t q = 0; q < cnt; ++q) stim[ids[q]] = stim[ids[q]] + (R)amounts[q];
+    stim_at = step + 1;
+  }
   bool cond() const { return c.input_mode == 3 || c.input_mode == 4; }
 
   R wget(uint64_t s) const { return bf16 ? (R)bf16_to_f32(wb[s]) : w[s]; }
@@ -686,6 +696,11 @@ template <class R> struct Fast {
           Ii = (c.input_mode == 3) ? Ii + isyn : isyn;
           break;
         }
+      }
+      if (stim_at == k + 1) {
+        const R sv = stim[i];
+        stim[i] = R(0);
+        if (sv != R(0)) Ii = Ii + sv;
       }
       Ii = Ii + d.add_I;
       for (const Kick& kk : kicks)
@@ -1409,6 +1424,15 @@ void or_fast_rates(void* s, double* rates) {
 }
 uint64_t or_fast_events(void* s) { uint64_t r = 0; FAST_DISPATCH(s, r = F->events); return r; }
 double or_fast_lfp(void* s) { double r = 0; FAST_DISPATCH(s, r = F->lfp()); return r; }
+void or_fast_add_input_current(void* s, uint64_t count, const uint32_t* ids, const double* amounts) {
+  FAST_DISPATCH(s, F->add_input_current(count, ids, amounts));
+}
+// SimulationEngine::stimulate (engine.rs:156-161): input_current += amount
+void or_lit_add_input_current(void* s, uint64_t count, const uint32_t* ids, const double* amounts) {
+  Lit* L = (Lit*)s;
+  for (uint64_t q = 0; q < count; ++q)
+    if (ids[q] < L->n) L->I[ids[q]] += amounts[q];
+}
 void or_fast_destroy(void* s) {
   auto* pr = (std::pair<int, void*>*)s;
   if (pr->first == 32) delete (Fast<float>*)pr->second; else delete (Fast<double>*)pr->second;

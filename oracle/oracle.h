@@ -128,6 +128,10 @@ uint64_t or_fast_events(void* s);
 /* lfp_signal (engine.rs:492) in the reference conductance mode, as the
  * device sums it (0 in the other modes) */
 double or_fast_lfp(void* s);
+/* host stimulus: the device's arithmetic (fast) and SimulationEngine::
+ * stimulate, engine.rs:156-161 (literal) */
+void or_fast_add_input_current(void* s, uint64_t count, const uint32_t* ids, const double* amounts);
+void or_lit_add_input_current(void* s, uint64_t count, const uint32_t* ids, const double* amounts);
 /* eligibility values (m), reward now and the sum of the reward after each
  * step (out2), and SimulationEngine::apply_reward as the device does it */
 void or_fast_eligibility(void* s, double* e);

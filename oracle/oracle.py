@@ -90,6 +90,8 @@ def load():
         "or_fast_rates": (None, [vp, vp]),
         "or_fast_events": (u64, [vp]),
         "or_fast_lfp": (C.c_double, [vp]),
+        "or_fast_add_input_current": (None, [vp, u64, vp, vp]),
+        "or_lit_add_input_current": (None, [vp, u64, vp, vp]),
         "or_fast_eligibility": (None, [vp, vp]),
         "or_fast_reward": (None, [vp, vp]),
         "or_fast_apply_reward": (None, [vp, C.c_double]),
@@ -200,6 +202,12 @@ class _Base:
 
     def events(self):
         return int(getattr(self.L, self.prefix + "events")(self.h))
+
+    def stimulate(self, ids, amounts):
+        """SimulationEngine::stimulate (engine.rs:156-161) for each pair."""
+        i = np.ascontiguousarray(np.atleast_1d(ids), dtype=np.uint32)
+        a = np.ascontiguousarray(np.broadcast_to(np.atleast_1d(amounts), i.shape), dtype=np.float64)
+        getattr(self.L, self.prefix + "add_input_current")(self.h, i.size, _p(i), _p(a))
 
     def lfp(self):
         """lfp_signal (engine.rs:492) as the device sums it."""

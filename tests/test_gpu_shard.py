@@ -60,6 +60,20 @@ def test_sharded_reference_conductance_mode_and_lfp(lib):
     assert vs.lfp() == pytest.approx(one.lfp(), rel=1e-12)
 
 
+def test_sharded_stimulus_equals_one_gpu(lib):
+    # each rank keeps the stimulus of the neurons it owns
+    net, cfg, drive = nets.izh_stdp(n=12_000, k=60)
+    one = SimulationEngine(net, cfg, drive)
+    vs = VirtualShards(net, cfg, drive, 2)
+    ids = list(range(0, 12_000, 37))
+    for e in (one, vs):
+        e.run(50)
+        e.stimulate(ids, [30.0])
+        e.run(100)
+    assert nets.rasters_equal(one.read_raster(0, 150), vs.read_raster(0, 150))
+    assert np.array_equal(one.download_state()["v"], vs.download_state()["v"])
+
+
 def test_sharded_rank_rejects_foreign_synapses(lib):
     net, cfg, drive = nets.izh_stdp(n=6000, k=20)
     part, _ = partition_network(net, 0, 2)
