@@ -171,6 +171,11 @@ typedef struct ns_config {
    * affine frame (see ns_download_state for the plain values). */
   int32_t consolidation_enabled;
   double consolidation_tau, consolidation_target, consolidation_drift;
+  /* Per-neuron firing-rate estimate kept every step without homeostasis too
+   * (SimulationEngine::firing_rate / mean_firing_rate, engine.rs:637-645,
+   * :809-826; FP64, r += (1000/dt * spiked - r) * dt/100). Homeostasis keeps
+   * it in any case. Tracking runs the step path (no windowed stepping). */
+  uint32_t track_rates;
 } ns_config;
 
 /* Fills cfg with the reference defaults: LIF, DIRECT_DECAY, dt 0.5 ms
@@ -291,7 +296,7 @@ ns_status ns_upload_state(ns_handle* h, const ns_neuron_soa* in, const float* w_
 /* Current global step index (the Philox counter and STDP clock). */
 ns_status ns_get_step(ns_handle* h, uint64_t* step);
 /* Per-neuron firing-rate estimate (engine.rs:637-642), FP64 on the device;
- * maintained only when homeostasis is enabled. */
+ * maintained when homeostasis or track_rates is enabled (zeros otherwise). */
 ns_status ns_download_rates(ns_handle* h, double* rates_out);
 /* Mean firing rate (Hz) of every network of the handle (n_nets entries; 1
  * for a single network) over the logged steps first_step .. first_step +

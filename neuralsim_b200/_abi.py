@@ -44,7 +44,7 @@ class NsConfig(C.Structure):
         ("reward_threshold", C.c_uint64), ("reward_decay", C.c_double),
         ("reward_signal", C.c_double), ("consolidation_enabled", C.c_int32),
         ("consolidation_tau", C.c_double), ("consolidation_target", C.c_double),
-        ("consolidation_drift", C.c_double),
+        ("consolidation_drift", C.c_double), ("track_rates", C.c_uint32),
     ]
 
 

@@ -83,6 +83,7 @@ struct ns_handle {
   std::vector<float> stim_acc;
   std::vector<uint8_t> stim_mark;
   std::vector<uint32_t> stim_ids;
+  bool stim_step = false;           // the next neuron launch takes the stimulus
   void* stim_dev = nullptr;
   size_t stim_dev_cap = 0;          // entries
 };
@@ -580,9 +581,11 @@ typedef void (*neuron_fn)(NsDev, uint32_t);
 typedef void (*prop_fn)(NsDev, uint32_t);
 typedef void (*ltd_fn)(NsDev, uint32_t);
 
-neuron_fn pick_neuron(uint32_t model, uint32_t mode, bool pt) {
-#define NSN(MO, MD) \
-  if (model == MO && mode == MD) return pt ? ns::k_neuron<MO, MD, true> : ns::k_neuron<MO, MD, false>;
+neuron_fn pick_neuron(uint32_t model, uint32_t mode, bool pt, bool stim = false) {
+#define NSN(MO, MD)                                                                  \
+  if (model == MO && mode == MD)                                                    \
+    return stim ? (pt ? ns::k_neuron<MO, MD, true, true> : ns::k_neuron<MO, MD, false, true>) \
+                : (pt ? ns::k_neuron<MO, MD, true, false> : ns::k_neuron<MO, MD, false, false>);
   NSN(0, 0) NSN(0, 1) NSN(0, 2) NSN(0, 3) NSN(0, 4)
   NSN(1, 0) NSN(1, 1) NSN(1, 2) NSN(1, 3) NSN(1, 4)
   NSN(2, 0) NSN(2, 1) NSN(2, 2) NSN(2, 3) NSN(2, 4)
@@ -626,7 +629,16 @@ void launch_tail(ns_handle* h, const NsDev& d, uint32_t j, cudaStream_t s) {
     ns::k_tail<false><<<h->sms * 8, 256, 0, s>>>(d, j);
 }
 
+// Homeostasis, which keeps the firing-rate estimate itself, or the estimate
+// alone when only track_rates asks for it.
+bool homeo_or_rates(const ns_handle* h) {
+  return h->cfg.homeostasis_enabled || h->cfg.track_rates;
+}
 void launch_homeo(ns_handle* h, const NsDev& d, uint32_t j, cudaStream_t s) {
+  if (!h->cfg.homeostasis_enabled) {
+    ns::k_rates<<<h->sms * 4, 256, 0, s>>>(d);
+    return;
+  }
   if (h->cfg.weight_format == NS_WEIGHT_BF16)
     ns::k_homeostasis<true><<<h->homeo_blocks, 256, 0, s>>>(d, j);
   else
@@ -657,8 +669,9 @@ cudaError_t shard_exchange(ns_handle* h) {
 // Enqueues one step (graph-node index j). With overlap, the LTD kernel of
 // step j runs on the side stream beside the neuron kernel of step j+1 and the
 // row walk of step j+1 waits for it; *ltd_pending tracks the open branch.
-cudaError_t enqueue_step(ns_handle* h, uint32_t j, bool* ltd_pending, uint32_t sched) {
-  neuron_fn nf = pick_neuron(h->cfg.model, h->cfg.input_mode, h->d.pidx != nullptr);
+cudaError_t enqueue_step(ns_handle* h, uint32_t j, bool* ltd_pending, uint32_t sched,
+                         bool stim = false) {
+  neuron_fn nf = pick_neuron(h->cfg.model, h->cfg.input_mode, h->d.pidx != nullptr, stim);
   nf<<<h->d.tiles_own, ns::kThreads, 0, h->st>>>(h->d, j);
   if (h->shard_world > 1) {
     // every rank's spike bitmap words, then the other ranks' tiles rebuilt
@@ -694,7 +707,7 @@ cudaError_t enqueue_step(ns_handle* h, uint32_t j, bool* ltd_pending, uint32_t s
     }
   }
   if (tail_on(h)) launch_tail(h, h->d, j, h->st);
-  if (h->cfg.homeostasis_enabled) launch_homeo(h, h->d, j, h->st);
+  if (homeo_or_rates(h)) launch_homeo(h, h->d, j, h->st);
   return cudaGetLastError();
 }
 
@@ -706,14 +719,14 @@ cudaError_t join_ltd(ns_handle* h, bool* ltd_pending) {
 
 uint64_t launches_per_step(const ns_handle* h, uint32_t sched) {
   const bool split = sched == 2 || sched == 4;
-  return 2u + ((split && h->cfg.stdp_enabled) ? 1u : 0u) + (h->cfg.homeostasis_enabled ? 1u : 0u) +
+  return 2u + ((split && h->cfg.stdp_enabled) ? 1u : 0u) + (homeo_or_rates(h) ? 1u : 0u) +
          (tail_on(h) ? 2u : 0u) + (h->shard_world > 1 ? 1u : 0u);
 }
 
 typedef void (*window_fn)(NsDev, uint32_t, uint32_t);
 
-window_fn pick_window(uint32_t model, uint32_t mode) {
-#define NSW(MO, MD) if (model == MO && mode == MD) return ns::k_window<MO, MD>;
+window_fn pick_window(uint32_t model, uint32_t mode, bool stim) {
+#define NSW(MO, MD) if (model == MO && mode == MD) return stim ? ns::k_window<MO, MD, true> : ns::k_window<MO, MD, false>;
   NSW(0, 0) NSW(0, 1) NSW(0, 2) NSW(0, 4)
   NSW(1, 0) NSW(1, 1) NSW(1, 2) NSW(1, 4)
   NSW(2, 0) NSW(2, 1) NSW(2, 2) NSW(2, 4)
@@ -731,14 +744,14 @@ window_fn pick_window_rows(uint32_t mode, uint32_t wf) {
 // Window length the handle's configuration allows (0 = step-synchronous).
 uint32_t window_len(const ns_config& c) {
   if (c.stdp_enabled || c.homeostasis_enabled || c.delay_steps < 2 || c.window_steps == 1) return 0;
-  if (c.rstdp_enabled || c.consolidation_enabled) return 0;
+  if (c.rstdp_enabled || c.consolidation_enabled || c.track_rates) return 0;
   if (c.input_mode == NS_INPUT_CONDUCTANCE_REF) return 0;
   uint32_t w = c.window_steps > 1 ? std::min(c.window_steps, c.delay_steps) : c.delay_steps;
   return std::min<uint32_t>(w, 1024u);
 }
 
 // Enqueues a window of Wc steps starting at graph-node offset j0.
-cudaError_t enqueue_window(ns_handle* h, uint32_t j0, uint32_t Wc) {
+cudaError_t enqueue_window(ns_handle* h, uint32_t j0, uint32_t Wc, bool stim = false) {
   const uint32_t nseg = h->d.nseg;
   if (h->sur_on) {
     h->sd.hstep = h->hstep;
@@ -748,7 +761,7 @@ cudaError_t enqueue_window(ns_handle* h, uint32_t j0, uint32_t Wc) {
     ns::k_window_sort<<<(unsigned)((pairs + 255) / 256), 256, 0, h->st>>>(h->d, h->sd, j0, Wc);
     h->launches += 2;
   } else {
-    pick_window(h->cfg.model, h->cfg.input_mode)<<<nseg, ns::kWinThreads, 0, h->st>>>(h->d, j0, Wc);
+    pick_window(h->cfg.model, h->cfg.input_mode, stim)<<<nseg, ns::kWinThreads, 0, h->st>>>(h->d, j0, Wc);
   }
   pick_window_rows(h->cfg.input_mode, h->cfg.weight_format)
       <<<h->win_rows_blocks, 256, 0, h->st>>>(h->d, j0, Wc);
@@ -1803,6 +1816,7 @@ ns_status flush_stim(ns_handle* h) {
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(h->st));
   h->launches += 1;
+  h->stim_step = true;
   return NS_OK;
 }
 
@@ -1814,12 +1828,32 @@ ns_status ns_step(ns_handle* h, uint32_t n_steps, ns_step_stats* out) {
     return fail(h, NS_ERR_STATE, "sharded handle without NCCL: step with ns_shard_step_begin / ns_shard_step_end");
   CK(cudaSetDevice(h->dev));
   fill_scalars(h);
+  const bool stim_now = n_steps && !h->stim_ids.empty();
   if (n_steps && (r = flush_stim(h))) return r;
   ns::Ctl before{};
   CK(cudaMemcpyAsync(&before, h->ctl, sizeof(before), cudaMemcpyDeviceToHost, h->st));
+  uint32_t left = n_steps;
+  if (stim_now) {
+    // the stimulated step runs alone, eagerly, with the kernel variant that
+    // reads the stimulus (a one-step window when stepping is windowed)
+    if (h->win) {
+      CK(enqueue_window(h, 0, 1, true));
+      h->win_ran = true;
+    } else {
+      bool pending = false;
+      CK(enqueue_step(h, 0, &pending, sched_of(h), true));
+      CK(join_ltd(h, &pending));
+      h->launches += launches_per_step(h, sched_of(h));
+    }
+    ns::k_advance<<<1, 1, 0, h->st>>>(h->ctl, 1);
+    h->launches += 1;
+    h->stim_step = false;
+    CK(cudaGetLastError());
+    left -= 1;
+  }
   uint32_t tuned = 0;
-  if ((r = autotune(h, n_steps, &tuned))) return r;
-  if ((r = run_steps(h, n_steps - tuned, sched_of(h)))) return r;
+  if ((r = autotune(h, left, &tuned))) return r;
+  if ((r = run_steps(h, left - tuned, sched_of(h)))) return r;
   ns::Ctl after{};
   CK(cudaMemcpyAsync(&after, h->ctl, sizeof(after), cudaMemcpyDeviceToHost, h->st));
   CK(cudaStreamSynchronize(h->st));
@@ -1853,7 +1887,8 @@ ns_status ns_step_traced(ns_handle* h, uint64_t* pos_out, uint64_t cap, uint64_t
     return st;
   }
   NsDev d = h->d;
-  neuron_fn nf = pick_neuron(h->cfg.model, h->cfg.input_mode, h->d.pidx != nullptr);
+  neuron_fn nf = pick_neuron(h->cfg.model, h->cfg.input_mode, h->d.pidx != nullptr, h->stim_step);
+  h->stim_step = false;
   const bool ext = ext_on(h);
   prop_fn pf = pick_prop(h->cfg.input_mode, h->cfg.weight_format, ext);
   nf<<<h->d.tiles_own, ns::kThreads, 0, h->st>>>(d, 0);
@@ -1863,7 +1898,7 @@ ns_status ns_step_traced(ns_handle* h, uint64_t* pos_out, uint64_t cap, uint64_t
   pf<<<h->prop_blocks, 256, 0, h->st>>>(d, 0);
   if (h->cfg.stdp_enabled) pick_ltd(h->cfg.weight_format, ext)<<<h->ltd_blocks, 256, 0, h->st>>>(d, 0);
   if (tail_on(h)) launch_tail(h, d, 0, h->st);
-  if (h->cfg.homeostasis_enabled) launch_homeo(h, d, 0, h->st);
+  if (homeo_or_rates(h)) launch_homeo(h, d, 0, h->st);
   ns::k_advance<<<1, 1, 0, h->st>>>(h->ctl, 1);
   h->launches += launches_per_step(h, 2) + 2;
   CK(cudaGetLastError());
@@ -2369,18 +2404,21 @@ ns_status ns_profile_steps(ns_handle* h, uint32_t n_steps, double* kernel_ms, ui
   fill_scalars(h);
   if (n_steps && (r = flush_stim(h))) return r;
   neuron_fn nf = pick_neuron(h->cfg.model, h->cfg.input_mode, h->d.pidx != nullptr);
+  // a pending stimulus goes with the first step
+  neuron_fn nf0 = pick_neuron(h->cfg.model, h->cfg.input_mode, h->d.pidx != nullptr, h->stim_step);
+  h->stim_step = false;
   const bool ext = ext_on(h);
   prop_fn pf = pick_prop(h->cfg.input_mode, h->cfg.weight_format, ext);
   ltd_fn lf = pick_ltd(h->cfg.weight_format, ext);
   // kernels in order neuron, rows, ltd (+ the R-STDP / consolidation tail),
   // homeostasis; serial, one event pair each
-  const bool on[4] = {true, true, h->cfg.stdp_enabled != 0 || tail_on(h), h->cfg.homeostasis_enabled != 0};
+  const bool on[4] = {true, true, h->cfg.stdp_enabled != 0 || tail_on(h), homeo_or_rates(h)};
   std::vector<cudaEvent_t> ev((size_t)n_steps * 8);
   for (auto& e : ev) CK(cudaEventCreate(&e));
   for (uint32_t j = 0; j < n_steps; ++j) {
     cudaEvent_t* e = &ev[(size_t)j * 8];
     CK(cudaEventRecord(e[0], h->st));
-    nf<<<h->d.tiles_own, ns::kThreads, 0, h->st>>>(h->d, j);
+    (j == 0 ? nf0 : nf)<<<h->d.tiles_own, ns::kThreads, 0, h->st>>>(h->d, j);
     if (tail_on(h)) ns::k_setup<<<1, 32, 0, h->st>>>(h->d, j);
     CK(cudaEventRecord(e[1], h->st));
     CK(cudaEventRecord(e[2], h->st));
@@ -2530,7 +2568,8 @@ ns_status ns_shard_step_begin(ns_handle* h) {
   fill_scalars(h);
   if ((r = flush_stim(h))) return r;
   if (h->sched == 0) h->sched = 3;
-  neuron_fn nf = pick_neuron(h->cfg.model, h->cfg.input_mode, h->d.pidx != nullptr);
+  neuron_fn nf = pick_neuron(h->cfg.model, h->cfg.input_mode, h->d.pidx != nullptr, h->stim_step);
+  h->stim_step = false;
   nf<<<h->d.tiles_own, ns::kThreads, 0, h->st>>>(h->d, 0);
   h->launches += 1;
   CK(cudaGetLastError());
@@ -2569,7 +2608,7 @@ ns_status ns_shard_step_end(ns_handle* h) {
     if (h->cfg.stdp_enabled) pick_ltd(h->cfg.weight_format, ext)<<<h->ltd_blocks, 256, 0, h->st>>>(h->d, 0);
   }
   if (tail_on(h)) launch_tail(h, h->d, 0, h->st);
-  if (h->cfg.homeostasis_enabled) launch_homeo(h, h->d, 0, h->st);
+  if (homeo_or_rates(h)) launch_homeo(h, h->d, 0, h->st);
   ns::k_advance<<<1, 1, 0, h->st>>>(h->ctl, 1);
   h->launches += launches_per_step(h, sched);
   CK(cudaGetLastError());

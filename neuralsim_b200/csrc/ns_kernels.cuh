@@ -422,7 +422,9 @@ __global__ void k_setup(NsDev d, uint32_t jstep) {
 // own slice of the spike buffer (warp ballots + a 32-entry scan), so no tile
 // waits for another; the last tile to finish does the step's bookkeeping.
 // ---------------------------------------------------------------------------
-template <int MODEL, int MODE, bool PT>
+// STIM: this step takes a pending host stimulus (the variant runs for that
+// one step; the others carry no stimulus code).
+template <int MODEL, int MODE, bool PT, bool STIM>
 __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
   __shared__ float s_tab[PT ? 256 * 8 : 1];
   __shared__ uint32_t s_off[kPairs * kWarps];
@@ -454,7 +456,7 @@ __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
     c->lfp_step[(k + 1) & 3] = 0ll;
   }
   long long lfp_fix = 0;
-  const bool stim_on = d.ctl->stim_at == k + 1;
+  const bool stim_on = STIM && d.ctl->stim_at == k + 1;
   if (PT)
     for (uint32_t q = tid; q < d.ptab_rows * 8u; q += kThreads) s_tab[q] = __ldg(d.ptab + q);
   __syncthreads();
@@ -1224,6 +1226,17 @@ __global__ void __launch_bounds__(256) k_homeostasis(NsDev d, uint32_t jstep) {
 }
 
 // ---------------------------------------------------------------------------
+// The firing-rate estimate without homeostasis (engine.rs:637-642, FP64):
+// the update k_homeostasis makes after its scaling, from this step's bitmap.
+__global__ void __launch_bounds__(256) k_rates(NsDev d) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < d.n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const double rate = d.rate[i];
+    const double inst = bit_of(d.bitmap, (uint32_t)i) ? 1000.0 / d.dt : 0.0;
+    d.rate[i] = rate + (inst - rate) * d.dt / 100.0;
+  }
+}
+
 // Single-network sharding (one rank per GPU, neurons split by tiles): after
 // the step's spike bitmap words of every rank have been gathered, one block
 // per tile of the other ranks ("ghost" tiles) rebuilds what the owner's

@@ -25,7 +25,9 @@ constexpr int kWinThreads = 256;   // neurons per segment (one block)
 template <int MODEL>
 __host__ __device__ constexpr int window_min_blocks() { return MODEL == 2 ? 3 : 4; }
 
-template <int MODEL, int MODE>
+// STIM: the window starts with the step that takes a pending host stimulus
+// (a one-step window; the other windows carry no stimulus code).
+template <int MODEL, int MODE, bool STIM>
 __global__ void __launch_bounds__(kWinThreads, window_min_blocks<MODEL>()) k_window(NsDev d, uint32_t j0, uint32_t W) {
   __shared__ uint32_t s_wcnt[kWinThreads / 32];
   __shared__ Kick s_kick[32];
@@ -63,7 +65,7 @@ __global__ void __launch_bounds__(kWinThreads, window_min_blocks<MODEL>()) k_win
   drive_key(d, i, dseed, dli);
   PoissonWords pw;
   float stim0 = 0.f;
-  if (d.ctl->stim_at == k0 + 1) {
+  if (STIM && d.ctl->stim_at == k0 + 1) {
     stim0 = d.stim[i];
     if (stim0 != 0.0f) d.stim[i] = 0.f;
   }
@@ -133,8 +135,11 @@ __global__ void __launch_bounds__(kWinThreads, window_min_blocks<MODEL>()) k_win
     }
     float addI, kick, addg;
     drive_of(d, y, z, inh, addI, kick, addg);
-    const float stv = stim0;   // the host stimulus joins the window's first step
-    stim0 = 0.f;
+    float stv = 0.f;
+    if (STIM) {   // the host stimulus joins the window's first step
+      stv = stim0;
+      stim0 = 0.f;
+    }
     const bool sp = update_one<MODEL, MODE>(d, k, i, st, par, rs, S, G, addI, kick, addg,
                                             s_kick, nk, stv) && (i < d.n);
     if (sp) { d.last[i] = (long long)k; ++my_spk; }

@@ -112,6 +112,7 @@ class SimConfig:
     consolidation_tau: float = 10000.0
     consolidation_target: float = 0.5
     consolidation_drift: float = 0.001
+    track_rates: int = 0
 
     def to_c(self):
         c = A.NsConfig()
@@ -372,6 +373,16 @@ class SimulationEngine:
         r = np.zeros(self.network.n, np.float64)
         self._check(self.lib.ns_download_rates(self._h, _ptr(r)))
         return r
+
+    def firing_rate(self, neuron: int) -> float:
+        """SimulationEngine::firing_rate (engine.rs:809-815): the neuron's
+        rate estimate (kept with homeostasis or track_rates), 0 out of range."""
+        return float(self.rates()[neuron]) if 0 <= neuron < self.network.n else 0.0
+
+    def mean_firing_rate(self) -> float:
+        """SimulationEngine::mean_firing_rate (engine.rs:818-826)."""
+        r = self.rates()
+        return float(r.sum() / r.size) if r.size else 0.0
 
     def step_traced(self, cap: int):
         pos = np.zeros(max(cap, 1), np.uint64)

@@ -870,7 +870,14 @@ template <class R> struct Fast {
   }
 
   void phase_d() {
-    if (!c.homeo) return;
+    if (!c.homeo) {
+      if (c.track_rates)
+        for (uint64_t i = 0; i < n; ++i) {
+          double inst = spiked[i] ? 1000.0 / c.dt : 0.0;
+          rate[i] += (inst - rate[i]) * c.dt / 100.0;
+        }
+      return;
+    }
     const double target = c.h_target;
     for (uint64_t i = 0; i < n; ++i) {
       double err = rate[i] - target;

@@ -56,6 +56,10 @@ typedef struct or_config {
   uint64_t reward_thr;
   double reward_decay, reward_init;
   double cons_tau, cons_target, cons_drift;
+  /* firing-rate estimate kept without homeostasis too (engine.rs:637-642;
+   * the literal engine always keeps it) */
+  int32_t track_rates;
+  int32_t pad4;
 } or_config;
 
 typedef struct or_net {

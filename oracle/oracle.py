@@ -31,6 +31,7 @@ class OrConfig(C.Structure):
         ("rstdp_wmin", C.c_double), ("rstdp_wmax", C.c_double), ("elig_tau", C.c_double),
         ("reward_thr", C.c_uint64), ("reward_decay", C.c_double), ("reward_init", C.c_double),
         ("cons_tau", C.c_double), ("cons_target", C.c_double), ("cons_drift", C.c_double),
+        ("track_rates", C.c_int32), ("pad4", C.c_int32),
     ]
 
 
@@ -158,6 +159,7 @@ def make_config(cfg, drive):
     c.cons = 1 if g("consolidation_enabled", False) else 0
     c.cons_tau, c.cons_target = g("consolidation_tau", 10000.0), g("consolidation_target", 0.5)
     c.cons_drift = g("consolidation_drift", 0.001)
+    c.track_rates = 1 if g("track_rates", 0) else 0
     return c
 
 

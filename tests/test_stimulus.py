@@ -95,3 +95,48 @@ def test_stimulus_arguments(lib):
     ref = SimulationEngine(net, cfg, drive)
     ref.run(50)
     assert nets.rasters_equal(eng.read_raster(0, 50), ref.read_raster(0, 50))
+
+
+# Firing-rate estimate without homeostasis (SimulationEngine::firing_rate /
+# mean_firing_rate, engine.rs:637-645, :809-826): kept when track_rates is on.
+
+def rate_net():
+    net, cfg, drive = nets.lif_reference_default(n=300, stdp=True, homeo=False)
+    cfg.track_rates = 1
+    return net, cfg, drive
+
+
+def test_tracked_rates_fast_vs_literal(oracle_lib):
+    net, cfg, drive = rate_net()
+    f = FastOracle(net, cfg, drive, precision=64)
+    l = LiteralOracle(net, cfg, drive, threads=2)
+    f.step(120)
+    l.step(120)
+    assert nets.rasters_equal(f.raster(), l.raster())
+    assert np.allclose(f.rates(), l.rates(), rtol=1e-12, atol=1e-12)
+    assert f.rates().max() > 0
+    cfg.track_rates = 0
+    g = FastOracle(net, cfg, drive, precision=64)
+    g.step(10)
+    assert not g.rates().any()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("which", ["ref_current", "lif_delta"])
+def test_tracked_rates_match_oracle(lib, which):
+    if which == "ref_current":
+        net, cfg, drive = rate_net()
+    else:
+        net, cfg, drive = nets.lif_delta(n=3000, k=40)   # windowed unless tracking
+        cfg.track_rates = 1
+    eng = SimulationEngine(net, cfg, drive)
+    eng.run(150)
+    o = FastOracle(net, cfg, drive, precision=32)
+    o.step(150)
+    assert nets.rasters_equal(eng.read_raster(0, 150), o.raster())
+    r = eng.rates()
+    assert np.array_equal(r, o.rates())
+    assert r.max() > 0
+    assert eng.mean_firing_rate() == pytest.approx(r.mean(), rel=1e-15)
+    assert eng.firing_rate(5) == r[5] and eng.firing_rate(net.n) == 0.0
+    assert eng.window()[0] <= 1   # tracking runs the step path
