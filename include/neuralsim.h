@@ -222,6 +222,9 @@ typedef struct ns_step_stats {
   uint64_t events;            /* synaptic events (sum of out-degree of spikers) */
   uint64_t last_step_spikes;
   double sim_time_ms;         /* FP64 device clock (engine.rs:388-389) */
+  uint64_t max_step_spikes;   /* largest spike count of one step since creation /
+                                 state upload (SimulationStats::active_neurons,
+                                 engine.rs:624) */
 } ns_step_stats;
 
 /* --- lifecycle: GpuBackend::new, gpu_backend.rs:98-124 ------------------ */

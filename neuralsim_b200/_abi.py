@@ -80,6 +80,7 @@ class NsStepStats(C.Structure):
     _fields_ = [
         ("steps_done", C.c_uint64), ("spikes", C.c_uint64), ("output_spikes", C.c_uint64),
         ("events", C.c_uint64), ("last_step_spikes", C.c_uint64), ("sim_time_ms", C.c_double),
+        ("max_step_spikes", C.c_uint64),
     ]
 
 

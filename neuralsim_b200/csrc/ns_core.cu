@@ -1863,6 +1863,7 @@ ns_status ns_step(ns_handle* h, uint32_t n_steps, ns_step_stats* out) {
     out->output_spikes = after.out_total - before.out_total;
     out->events = after.events_total - before.events_total;
     out->last_step_spikes = n_steps ? after.step_spikes[(after.step_base - 1) & 3] : 0;
+    out->max_step_spikes = after.max_step_spikes;
     out->sim_time_ms = after.sim_time;
   }
   if ((after.status & ns::kErrLogFull) && !(before.status & ns::kErrLogFull))

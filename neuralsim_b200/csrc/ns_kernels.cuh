@@ -64,6 +64,9 @@ struct Ctl {
   // values in NsDev::stim join the input current at step stim_at - 1
   // (0: none pending); the consuming thread zeroes them
   unsigned long long stim_at;
+  // largest spike count of one step (SimulationStats::active_neurons,
+  // engine.rs:624)
+  unsigned long long max_step_spikes;
 };
 
 struct Kick { uint32_t target; float amt; };
@@ -717,6 +720,7 @@ __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
     c->spk_acc[(k + 2) & 3] = 0ull;
     c->tiles_done = 0u;
     c->step_spikes[k & 3] = total;
+    if (total > c->max_step_spikes) c->max_step_spikes = total;
     c->spikes_total += total;
     c->sim_time += d.dt;  // FP64 clock, engine.rs:388-389
     unsigned ok = 0u;
@@ -1313,6 +1317,7 @@ __global__ void __launch_bounds__(kThreads) k_shard_merge(NsDev d, uint32_t jste
     cc->spk_acc[(k + 2) & 3] = 0ull;
     cc->tiles_done = 0u;
     cc->step_spikes[k & 3] = total;
+    if (total > cc->max_step_spikes) cc->max_step_spikes = total;
     cc->spikes_total += total;
     cc->sim_time += d.dt;
     unsigned ok = 0u;

@@ -284,6 +284,7 @@ __global__ void __launch_bounds__(256) k_window_finish(NsDev d, uint32_t j0, uin
   for (uint32_t q = 0; q < W; ++q) {
     all += d.step_total[q];
     c->step_spikes[(k0 + q) & 3] = d.step_total[q];
+    if (d.step_total[q] > c->max_step_spikes) c->max_step_spikes = d.step_total[q];
     c->sim_time += d.dt;
   }
   if (d.log_idx != nullptr && !(c->status & kErrLogFull)) {

@@ -222,6 +222,7 @@ class SimulationEngine:
         self._stats_total["spikes"] += out.spikes
         self._stats_total["output_spikes"] += out.output_spikes
         self._stats_total["events"] += out.events
+        self._last_out = out
         return out
 
     def step(self) -> StepResult:
@@ -245,9 +246,21 @@ class SimulationEngine:
         return int(s.value)
 
     def stats(self) -> dict:
+        """SimulationStats (engine.rs:22-33, filled at :617-670) from the
+        totals of this engine's runs, plus the step and event counts. The
+        mean firing rate needs the rate estimate (homeostasis or
+        track_rates); the weight moments are computed on demand."""
         out = dict(self._stats_total)
         out["steps"] = self.current_step()
         out["sim_time_ms"] = out["steps"] * self.config.dt_ms
+        last = getattr(self, "_last_out", None)
+        out["total_spikes"] = out["spikes"]
+        out["active_neurons"] = int(last.max_step_spikes) if last is not None else 0
+        out["weight_updates"] = int(last.last_step_spikes) if last is not None else 0
+        out["synchrony_index"] = out["weight_updates"] / self.network.n
+        out["mean_firing_rate"] = self.mean_firing_rate()
+        out["weight_mean"], out["weight_std"] = self.weight_stats()
+        out["seed"] = self.config.seed
         return out
 
     def weight_stats(self):

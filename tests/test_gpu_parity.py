@@ -510,3 +510,34 @@ def test_c2_full_size_deterministic(lib):
     assert np.array_equal(runs[0][2], runs[1][2])
     deg = np.diff(net.row_ptr.astype(np.int64))
     assert runs[0][3] == int(deg[runs[0][0]].sum()) and runs[0][3] > 0
+
+
+@pytest.mark.parametrize("which", ["ref_default", "windowed"])
+def test_simulation_stats_match_oracle(lib, which):
+    # SimulationStats (engine.rs:22-33, :617-670): totals, the largest step
+    # (active_neurons), the last step (weight_updates, synchrony), the mean
+    # rate estimate and the weight moments
+    if which == "ref_default":
+        net, cfg, drive = nets.lif_reference_default(n=2000)   # homeostasis keeps the rates
+    else:
+        net, cfg, drive = nets.lif_delta(n=4000, k=40)
+        cfg.spike_log_capacity = 10_000_000
+    eng = SimulationEngine(net, cfg, drive)
+    eng.run(120)
+    eng.run(80)
+    o = FastOracle(net, cfg, drive, precision=32)
+    o.step(200)
+    idx, off = o.raster()
+    counts = np.diff(off.astype(np.int64))
+    st = eng.stats()
+    assert st["total_spikes"] == len(idx)
+    assert st["active_neurons"] == counts.max() > 0
+    assert st["weight_updates"] == counts[-1]
+    assert st["synchrony_index"] == counts[-1] / net.n
+    if which == "ref_default":
+        assert st["mean_firing_rate"] == pytest.approx(o.rates().mean(), rel=1e-12)
+        w = o.weights()
+        assert st["weight_mean"] == pytest.approx(w.mean(), rel=1e-6)
+        assert st["weight_std"] == pytest.approx(w.std(), rel=1e-5)
+    else:
+        assert eng.window()[0] > 1
