@@ -148,9 +148,11 @@ class Drive:
 
 @dataclass
 class StepResult:
+    """StepResult (engine.rs:35-41)."""
     spike_count: int
     output_spike_count: int
     spiking_neurons: np.ndarray = field(default_factory=lambda: np.zeros(0, np.uint32))
+    output_spiking_neurons: np.ndarray = field(default_factory=lambda: np.zeros(0, np.uint32))
 
 
 class SimulationEngine:
@@ -231,9 +233,12 @@ class SimulationEngine:
         k = self.current_step()
         out = self.run(1)
         spikes = np.zeros(0, np.uint32)
+        outs = spikes
         if self.config.spike_log_capacity > 0:
             spikes = self.read_spikes(k, 1)[0]
-        return StepResult(int(out.spikes), int(out.output_spikes), spikes)
+            if self.network.is_output is not None:
+                outs = spikes[np.asarray(self.network.is_output)[spikes] != 0]
+        return StepResult(int(out.spikes), int(out.output_spikes), spikes, outs)
 
     def simulate_ms(self, duration_ms: float):
         steps = int(duration_ms / self.config.dt_ms)

@@ -541,3 +541,24 @@ def test_simulation_stats_match_oracle(lib, which):
         assert st["weight_std"] == pytest.approx(w.std(), rel=1e-5)
     else:
         assert eng.window()[0] > 1
+
+
+def test_step_result_lists(lib):
+    # StepResult (engine.rs:35-41): the step's ascending spiking neurons and
+    # the output neurons among them, as the oracle's raster has them
+    net, cfg, drive = nets.lif_reference_default(n=500)
+    net.is_output = (np.arange(net.n) % 5 == 0).astype(np.uint8)
+    eng = SimulationEngine(net, cfg, drive)
+    o = FastOracle(net, cfg, drive, precision=32)
+    o.step(30)
+    idx, off = o.raster()
+    seen_out = 0
+    for k in range(30):
+        r = eng.step()
+        want = idx[off[k]:off[k + 1]]
+        assert np.array_equal(r.spiking_neurons, want)
+        assert r.spike_count == len(want)
+        assert np.array_equal(r.output_spiking_neurons, want[want % 5 == 0])
+        assert r.output_spike_count == len(r.output_spiking_neurons)
+        seen_out += r.output_spike_count
+    assert seen_out > 0
