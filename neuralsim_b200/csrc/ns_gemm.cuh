@@ -56,6 +56,13 @@ __device__ __forceinline__ uint16_t f32_to_bf16_rn(float x) {
   return *reinterpret_cast<const uint16_t*>(&b);
 }
 
+// lo | hi << 16 as BF16, both rounded to nearest even by one packed
+// conversion (the same values as two f32_to_bf16_rn)
+__device__ __forceinline__ uint32_t pack_bf16x2_rn(float lo, float hi) {
+  const __nv_bfloat162 p = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<const uint32_t*>(&p);
+}
+
 // x = hi + lo with hi = bf16(x): the BF16 pair carries ~16 significant bits
 // of x into a tensor-core product whose weight column is duplicated.
 __device__ __forceinline__ void split_bf16(float x, uint16_t& hi, uint16_t& lo) {
@@ -170,8 +177,7 @@ __global__ void __launch_bounds__(128) k_gemm(Args g) {
               g.C[(uint64_t)r * g.ldc + j + q] = z0;
               g.C[(uint64_t)r * g.ldc + j + q + 1] = z1;
             }
-            packed[q / 2] = (uint32_t)f32_to_bf16_rn(silu_t(z0)) |
-                            ((uint32_t)f32_to_bf16_rn(silu_t(z1)) << 16);
+            packed[q / 2] = pack_bf16x2_rn(silu_t(z0), silu_t(z1));
           }
           uint4* hp = reinterpret_cast<uint4*>(g.H + (uint64_t)r * g.ldh + j);
           hp[0] = make_uint4(packed[0], packed[1], packed[2], packed[3]);

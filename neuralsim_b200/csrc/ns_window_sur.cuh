@@ -93,7 +93,7 @@ __device__ __forceinline__ void sur_hidden_epilogue(uint32_t taddr, const float*
     for (int q = 0; q < 16; q += 2) {
       const float a = gemm::silu_t(v[q] + bias[j + q]);
       const float b = gemm::silu_t(v[q + 1] + bias[j + q + 1]);
-      pk[q / 2] = (uint32_t)gemm::f32_to_bf16_rn(a) | ((uint32_t)gemm::f32_to_bf16_rn(b) << 16);
+      pk[q / 2] = gemm::pack_bf16x2_rn(a, b);
     }
     *reinterpret_cast<uint4*>(H + tc::kmajor_offset(r, j, 128)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
     *reinterpret_cast<uint4*>(H + tc::kmajor_offset(r, j + 8, 128)) = make_uint4(pk[4], pk[5], pk[6], pk[7]);
