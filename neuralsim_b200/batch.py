@@ -63,6 +63,13 @@ class BatchEngine(SimulationEngine):
         self.first_neuron = first.astype(np.int64)
         del keep
 
+    def stimulate_network(self, q, neuron_ids, currents):
+        """Host stimulus for neurons of network q, by their index inside it."""
+        ids = np.atleast_1d(np.asarray(neuron_ids, dtype=np.int64))
+        if ids.size and (ids.min() < 0 or ids.max() >= self.networks[q].n):
+            raise ValueError("neuron index outside network %d" % q)
+        self.stimulate(ids + int(self.first_neuron[q]), currents)
+
     def split(self, per_neuron):
         """Splits a per-neuron array of the concatenation into networks."""
         f = self.first_neuron

@@ -62,6 +62,36 @@ def test_lif_batch_equals_networks_alone(lib, window):
     b.close()
 
 
+@pytest.mark.parametrize("window", [0, 1])
+def test_batch_stimulus_equals_network_alone(lib, window):
+    # a stimulus given to one network of the batch (by local index) acts as
+    # on that network alone; the others are untouched
+    nets, seeds, cfg, drive = lif_batch(n_nets=5, window=window)
+    ids, amt = [1, 5, 5, 17], [2000.0, 800.0, 800.0, -500.0]   # ~10 mV for neuron 1
+    b = BatchEngine(nets, seeds, cfg, drive)
+    b.run(100)
+    b.stimulate_network(3, ids, amt)
+    b.run(200)
+    parts = b.read_rasters(0, 300)
+    for q, net in enumerate(nets):
+        c = copy.copy(cfg)
+        c.seed = seeds[q]
+        e = SimulationEngine(net, c, drive)
+        e.run(100)
+        if q == 3:
+            e.stimulate(ids, amt)
+        e.run(200)
+        assert tnets.rasters_equal(parts[q], e.read_raster(0, 300)), q
+        e.close()
+    c = copy.copy(cfg)
+    c.seed = seeds[3]
+    plain = alone(nets[3], seeds[3], cfg, drive, 300)[0]
+    assert not tnets.rasters_equal(parts[3], plain)   # the stimulus acted
+    with pytest.raises(ValueError):
+        b.stimulate_network(0, [nets[0].n], [1.0])
+    b.close()
+
+
 def test_izh_stdp_gauss_batch_equals_networks_alone(lib):
     # Gaussian drive pairs neurons (2i, 2i+1): odd sizes make pairs straddle
     # networks in the concatenation; STDP weights stay inside each block
