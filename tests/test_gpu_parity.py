@@ -562,3 +562,25 @@ def test_step_result_lists(lib):
         assert r.output_spike_count == len(r.output_spiking_neurons)
         seen_out += r.output_spike_count
     assert seen_out > 0
+
+
+@pytest.mark.parametrize("plastic", ["none", "last_target", "first_target"])
+def test_incoming_lists_edge_cases(lib, plastic):
+    # the plastic incoming lists (one stable sort by target, pointers from
+    # lower bounds): no plastic synapse at all, or all of them onto one end
+    net, cfg, drive = nets.izh_stdp(n=3000, k=30, wf=A.WEIGHT_F32)
+    if plastic == "none":
+        pl = np.zeros(net.m, np.uint8)
+    else:
+        t = net.n - 1 if plastic == "last_target" else 0
+        pl = (net.col == t).astype(np.uint8)
+        assert pl.sum() > 10
+    net.plastic = pl
+    eng = gpu_run(net, cfg, drive, 200)
+    o = FastOracle(net, cfg, drive, precision=32)
+    o.step(200)
+    assert nets.rasters_equal(eng.read_raster(0, 200), o.raster())
+    w = eng.download_state()["w"].astype(np.float64)
+    assert np.array_equal(w, o.weights())
+    changed = w != net.w.astype(np.float64)
+    assert not np.any(changed & (pl == 0))
