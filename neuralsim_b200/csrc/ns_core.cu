@@ -751,6 +751,12 @@ uint32_t window_len(const ns_config& c) {
 }
 
 // Enqueues a window of Wc steps starting at graph-node offset j0.
+// launches of one window: neuron window (+ fallback and sort with the
+// surrogate), rows, scan (spike log only), finish
+uint32_t window_launches(const ns_handle* h) {
+  return 3u + (h->d.log_idx ? 1u : 0u) + (h->sur_on ? 2u : 0u);
+}
+
 cudaError_t enqueue_window(ns_handle* h, uint32_t j0, uint32_t Wc, bool stim = false) {
   const uint32_t nseg = h->d.nseg;
   if (h->sur_on) {
@@ -765,9 +771,10 @@ cudaError_t enqueue_window(ns_handle* h, uint32_t j0, uint32_t Wc, bool stim = f
   }
   pick_window_rows(h->cfg.input_mode, h->cfg.weight_format)
       <<<h->win_rows_blocks, 256, 0, h->st>>>(h->d, j0, Wc);
-  ns::k_window_scan<<<Wc, 256, 0, h->st>>>(h->d, Wc);
+  // the segment offsets serve only the spike log
+  if (h->d.log_idx) ns::k_window_scan<<<Wc, 256, 0, h->st>>>(h->d, Wc);
   ns::k_window_finish<<<Wc, 256, 0, h->st>>>(h->d, j0, Wc);
-  h->launches += 4;
+  h->launches += window_launches(h) - (h->sur_on ? 2u : 0u);
   return cudaGetLastError();
 }
 
@@ -812,7 +819,7 @@ ns_status run_steps(ns_handle* h, uint32_t n, uint32_t sched) {
     if (r) return r;
     while (left >= S) {
       CK(cudaGraphLaunch(ex, h->st));
-      if (h->win) h->launches += ((S + h->wcur - 1) / h->wcur) * (4 + (h->sur_on ? 2 : 0)) + 1;
+      if (h->win) h->launches += ((S + h->wcur - 1) / h->wcur) * window_launches(h) + 1;
       else h->launches += (uint64_t)S * launches_per_step(h, sched) + 1;
       left -= S;
     }
@@ -947,7 +954,7 @@ ns_status autotune_window(ns_handle* h, uint32_t budget, uint32_t* used) {
     if ((ce = cudaEventSynchronize(e1)) != cudaSuccess) break;
     if ((ce = cudaEventElapsedTime(&ms, e0, e1)) != cudaSuccess) break;
     us[q] = ms * 1e3 / T;
-    h->launches += ((T + cand[q] - 1) / cand[q]) * 4 + 1;
+    h->launches += ((T + cand[q] - 1) / cand[q]) * window_launches(h) + 1;
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);

@@ -250,8 +250,20 @@ __global__ void __launch_bounds__(256) k_window_scan(NsDev d, uint32_t W) {
 // per step, as the step path does).
 __global__ void __launch_bounds__(256) k_window_finish(NsDev d, uint32_t j0, uint32_t W) {
   __shared__ int s_last;
+  __shared__ unsigned int s_sum;
   const uint32_t s = blockIdx.x;
   Ctl* c = d.ctl;
+  if (d.log_idx == nullptr && s < W) {
+    // no log, so no scan ran: block s totals step s's segment counts
+    if (threadIdx.x == 0) s_sum = 0u;
+    __syncthreads();
+    unsigned int t = 0u;
+    for (uint32_t seg = threadIdx.x; seg < d.nseg; seg += blockDim.x) t += d.seg_cnt[(uint64_t)s * d.nseg + seg];
+    t = __reduce_add_sync(0xffffffffu, t);
+    if ((threadIdx.x & 31) == 0 && t) atomicAdd(&s_sum, t);
+    __syncthreads();
+    if (threadIdx.x == 0) d.step_total[s] = s_sum;
+  }
   if (s < W && d.log_idx != nullptr && !(c->status & kErrLogFull)) {
     unsigned long long all = 0, before = 0;
     for (uint32_t q = 0; q < W; ++q) {

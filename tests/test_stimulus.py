@@ -140,3 +140,28 @@ def test_tracked_rates_match_oracle(lib, which):
     assert eng.mean_firing_rate() == pytest.approx(r.mean(), rel=1e-15)
     assert eng.firing_rate(5) == r[5] and eng.firing_rate(net.n) == 0.0
     assert eng.window()[0] <= 1   # tracking runs the step path
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("which", ["lif_delta_windowed", "hh_windowed"])
+def test_windowed_counters_without_log(lib, which):
+    # with the spike log off the window skips its segment scan: the step
+    # statistics equal those of the logged run
+    if which == "lif_delta_windowed":
+        net, cfg, drive = nets.lif_delta(n=3000, k=40)
+    else:
+        net, cfg, drive = nets.hh_cond(n=2000, k=40)
+        cfg.delay_steps, cfg.window_steps = 10, 0
+    n1 = 150 if which == "lif_delta_windowed" else 900
+    logged = SimulationEngine(net, cfg, drive)
+    a = [logged.run(n1), logged.run(77)]
+    cfg.spike_log_capacity = 0
+    bare = SimulationEngine(net, cfg, drive)
+    b = [bare.run(n1), bare.run(77)]
+    assert bare.window()[0] > 1 and logged.window()[0] > 1
+    for x, y in zip(a, b):
+        for f in ("steps_done", "spikes", "output_spikes", "events", "last_step_spikes",
+                  "max_step_spikes"):
+            assert getattr(x, f) == getattr(y, f), f
+    assert a[0].spikes + a[1].spikes > 0
+    assert np.array_equal(logged.download_state()["v"], bare.download_state()["v"])
