@@ -258,7 +258,9 @@ __global__ void __launch_bounds__(256) k_window_finish(NsDev d, uint32_t j0, uin
     if (threadIdx.x == 0) s_sum = 0u;
     __syncthreads();
     unsigned int t = 0u;
-    for (uint32_t seg = threadIdx.x; seg < d.nseg; seg += blockDim.x) t += d.seg_cnt[(uint64_t)s * d.nseg + seg];
+    const uint32_t* cnt = d.seg_cnt + (uint64_t)s * d.nseg;
+#pragma unroll 8
+    for (uint32_t seg = threadIdx.x; seg < d.nseg; seg += blockDim.x) t += cnt[seg];
     t = __reduce_add_sync(0xffffffffu, t);
     if ((threadIdx.x & 31) == 0 && t) atomicAdd(&s_sum, t);
     __syncthreads();
