@@ -312,15 +312,17 @@ __global__ void k_in_keys(const uint32_t* col, const uint8_t* pl, uint64_t m, ui
   }
 }
 
-// ptr[j] = first index of sorted keys with key >= j, j = 0..n: each q in
-// [0, m] sets the j in (keys[q-1], keys[q]] (keys[-1] = -1, keys[m] = n + 1)
+// ptr[j] = first index of the sorted keys with key >= j, j = 0..n, by a
+// binary search per pointer (no serial gap walks, whatever the key spread)
 __global__ void k_lower_bounds(const uint32_t* keys, uint64_t m, uint32_t n, uint64_t* ptr) {
-  for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q <= m;
-       q += (uint64_t)gridDim.x * blockDim.x) {
-    const int64_t prev = q == 0 ? -1 : (int64_t)keys[q - 1];
-    const int64_t cur = q == m ? (int64_t)n + 1 : (int64_t)keys[q];
-    const int64_t hi = cur < (int64_t)n ? cur : (int64_t)n;
-    for (int64_t j = prev + 1; j <= hi; ++j) ptr[j] = q;
+  for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j <= n;
+       j += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t lo = 0, hi = m;
+    while (lo < hi) {
+      const uint64_t mid = (lo + hi) >> 1;
+      if ((uint64_t)keys[mid] < j) lo = mid + 1; else hi = mid;
+    }
+    ptr[j] = lo;
   }
 }
 
