@@ -633,7 +633,8 @@ def run_surrogate_config(local, train_steps=12000, only_1m=False):
            "mlp": "5-128-128-4 SiLU, bf16 weights, fp32 accumulation (tcgen05)",
            "train_samples": int(len(x)), "train_steps": train_steps, "train_batch": 8192,
            "train_wall_s": round(train_s, 2), "final_loss": float(np.mean(losses[-100:])),
-           "envelope_mv": [S.V_LO, S.V_HI], "residual_mv": S.RESIDUAL_MV}
+           "envelope_mv": [S.V_LO, S.MACRO_V_HI], "training_envelope_mv": [S.V_LO, S.V_HI],
+           "residual_mv": S.RESIDUAL_MV}
     if not only_1m:
         res.update(_surrogate_eval(net, cfg, drive, sur, local, 10_000))
     big, bcfg, bdrive, _ = configs.hh_c4(n=1_000_000)

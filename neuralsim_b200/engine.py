@@ -455,9 +455,11 @@ class SimulationEngine:
         return out
 
     # -- learned HH macro-step (include/neuralsim_surrogate.h) --
-    def attach_surrogate(self, sur, v_lo=-85.0, v_hi=-52.0, residual_mv=0.5):
+    def attach_surrogate(self, sur, v_lo=-85.0, v_hi=-58.0, residual_mv=0.5):
         """Advance in-envelope neurons with the trained surrogate `sur`
-        (None detaches); the handle keeps its own copy of the weights."""
+        (None detaches); the handle keeps its own copy of the weights. The
+        default v_hi is surrogate.MACRO_V_HI: the macro-step stops short of
+        threshold, where the plain steps keep spike times accurate."""
         self._check(self.lib.ns_set_surrogate(self._h, sur.handle if sur is not None else None,
                                               float(v_lo), float(v_hi), float(residual_mv)))
 

@@ -23,6 +23,11 @@ SUBSTEPS = 10
 N_PARAMS = 17796
 # default training envelope of V (mV) and residual tolerance (mV)
 V_LO, V_HI, RESIDUAL_MV = -85.0, -52.0, 0.5
+# default upper bound of V for the macro-step: above it, on the approach to
+# threshold where a small error moves a spike most, the plain Rush-Larsen
+# steps take over (C4 network: mean spike-time error 0.09 ms at -58 mV,
+# 0.20 ms at -55 mV, 0.14-0.25 ms at the training bound -52 mV)
+MACRO_V_HI = -58.0
 
 
 def _p(a):
