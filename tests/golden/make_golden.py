@@ -50,6 +50,31 @@ def _with_stp(seed):
 
 
 # name -> (builder, steps, oracle precision)
+def _cond_stim_rates(seed):
+    # reference conductance mode, firing-rate tracking, host stimulus rounds
+    net, cfg, drive = nets.lif_reference_default(n=300, seed=seed, stdp=False, homeo=False,
+                                                 conductance=True)
+    cfg.track_rates = 1
+    return net, cfg, drive
+
+
+# (steps before the call, neuron ids, amounts) of a case's stimulus rounds
+STIM_ROUNDS = [(40, [3, 7, 7, 150], [20.0, 15.0, 5.0, 30.0]), (60, list(range(10, 200, 9)), [12.5])]
+
+
+def advance(obj, case):
+    """Steps an oracle (.step) or an engine (.run) through a case, with its
+    stimulus rounds when it has them."""
+    go = obj.run if hasattr(obj, "run") else obj.step
+    rounds = case[3] if len(case) > 3 else None
+    done = 0
+    for steps, ids, amt in rounds or ():
+        go(steps)
+        done += steps
+        obj.stimulate(ids, amt)
+    go(case[1] - done)
+
+
 CASES = {
     "lif_delta_n600": (lambda: nets.lif_delta(n=600, k=40, seed=143), 1500, 32),
     "izh_stdp_bf16_n800": (lambda: nets.izh_stdp(n=800, k=40, seed=144), 300, 32),
@@ -60,15 +85,16 @@ CASES = {
                                                   threshold=4), 300, 32),
     "izh_consolidation_f32_n800": (lambda: _consolidating(148), 300, 32),
     "lif_stp_n300": (lambda: _with_stp(149), 200, 32),
+    "lif_cond_stim_rates_n300": (lambda: _cond_stim_rates(150), 160, 32, STIM_ROUNDS),
 }
 
 
 def run_case(name):
     from oracle.oracle import FastOracle
-    build, steps, prec = CASES[name]
+    build, steps, prec = CASES[name][:3]
     net, cfg, drive = build()
     o = FastOracle(net, cfg, drive, precision=prec)
-    o.step(steps)
+    advance(o, CASES[name])
     idx, off = o.raster()
     st = o.state()
     out = {"idx": np.asarray(idx, np.uint32), "off": np.asarray(off, np.uint64),
@@ -78,6 +104,10 @@ def run_case(name):
     for k in ("u", "m", "h", "n", "pre", "post", "refr"):
         if k in st and st[k] is not None:
             out[k] = np.asarray(st[k])
+    if cfg.input_mode == A.INPUT_CONDUCTANCE_REF:
+        out["lfp"] = np.float64(o.lfp())
+    if getattr(cfg, "track_rates", 0):
+        out["rates"] = np.asarray(o.rates(), np.float64)
     if getattr(cfg, "rstdp_enabled", False):
         out["elig"] = np.asarray(o.eligibility(), np.float32 if prec == 32 else np.float64)
         out["reward"] = np.asarray(o.reward(), np.float64)

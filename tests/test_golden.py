@@ -15,7 +15,7 @@ import numpy as np
 import pytest
 
 import nets
-from golden.make_golden import CASES, net_digest
+from golden.make_golden import CASES, advance, net_digest
 
 HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 NAMES = sorted(CASES)
@@ -43,11 +43,11 @@ def test_oracle_reproduces_fixture(lib, oracle_lib, name):
 @pytest.mark.parametrize("name", NAMES)
 def test_gpu_reproduces_fixture(lib, name):
     from neuralsim_b200 import SimulationEngine
-    build, steps, prec = CASES[name]
+    build, steps, prec = CASES[name][:3]
     net, cfg, drive = build()
     f = fixture(name)
     eng = SimulationEngine(net, cfg, drive)
-    eng.run(steps)
+    advance(eng, CASES[name])
     raster = eng.read_raster(0, steps)
     st = eng.download_state()
     if name.startswith("lif_reference_default"):
@@ -62,6 +62,10 @@ def test_gpu_reproduces_fixture(lib, name):
         assert np.array_equal(st["w"].astype(np.float32), f["weights"])
         if "u" in f and name.startswith("izh"):
             assert np.array_equal(st["u"].astype(np.float64), f["u"])
+        if "lfp" in f:
+            assert eng.lfp() == f["lfp"]
+        if "rates" in f:
+            assert np.array_equal(eng.rates(), f["rates"])
         if "elig" in f:
             assert np.array_equal(eng.eligibility(), f["elig"])
             r, rs = eng.reward()
