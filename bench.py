@@ -66,8 +66,9 @@ def args_():
                    help="surrogate line: evaluate only the 1M-neuron network (profiling)")
     p.add_argument("--shard", action="store_true",
                    help="under torchrun: one network split over the GPUs (strong scaling) instead of replicas")
-    p.add_argument("--schedule", type=int, default=0, choices=[0, 1, 2, 3, 4],
-                   help="step schedule: 0 autotune, 1 fused, 2 split, 3 fused 4 blocks/SM, 4 split narrow LTD")
+    p.add_argument("--schedule", type=int, default=0, choices=[0, 1, 2, 3, 4, 5],
+                   help="step schedule: 0 autotune, 1 fused, 2 split, 3 fused 4 blocks/SM, "
+                        "4 split narrow LTD, 5 deferred LTD")
     return p.parse_args()
 
 
@@ -80,22 +81,6 @@ def peaks():
 
 
 PROFILE_UNIT_STEPS = 20
-
-
-def profile_traffic_ratio(kernel):
-    """DRAM bytes (read + write) per algorithmic byte of `kernel`, measured by
-    the committed ncu capture of the full-size workload (the launches of the
-    steps whose units bench.py records), or None."""
-    path = os.path.join(ROOT, "profiles", "izh_c2_step_kernels_ncu.md")
-    if not os.path.exists(path):
-        return None
-    for line in open(path):
-        if line.startswith(f"traffic_ratio_{kernel}:"):
-            try:
-                return float(line.split(":", 1)[1].strip().split()[0])
-            except ValueError:
-                return None
-    return None
 
 
 class ClockSampler:
@@ -161,23 +146,38 @@ def step_bytes(n, sim_steps, spikes, events, in_plastic):
     return 64.0 * n * sim_steps + 16.0 * spikes + 8.0 * events + 8.0 * in_plastic
 
 
-def kernel_bytes(n, spikes, events, in_plastic):
+def kernel_bytes(n, spikes, events, in_plastic, m_plastic, deferred):
     """Algorithmic HBM bytes per launch of each step kernel (one step):
     neuron: 64 N (v,u r/w; a,b,c,d; int64 accumulator read + zero; pre/post
             traces r/w) + 4 S (spike index);
     rows:   16 S (row_ptr pair) + 24 S (last r/w, trace bump r/w)
             + 8 E_out (column 4, bf16 weight read 2 and LTP write 2);
-    ltd:    16 S (incoming pointer pair) + 8 E_in,plastic (incoming entry
-            4 of the 8 B (source, position) pair counted as in the plan's
-            formula, bf16 weight read 2 + write 2).
+            deferred LTD adds 16 S (the row's trace start read + write);
+            its pending LTDs change weights the walk reads and writes anyway;
+    ltd:    eager: 16 S (incoming pointer pair) + 8 E_in,plastic (incoming
+            entry 4 of the 8 B (source, position) pair counted as in the
+            plan's formula, bf16 weight read 2 + write 2);
+            deferred (the row-block flush, a 32nd of the rows per step):
+            (16 + 16) N/32 (row_ptr pair, trace start read + write) +
+            8 M_plastic/32 (column 4, bf16 weight read 2 + write 2).
     Accumulator atomics and trace-record gathers hit L2-resident arrays and
     count as 0 HBM bytes. `sector_bytes` counts the 32-byte DRAM sector that a
-    random 2-byte weight access moves (read + write) for the LTD."""
+    random 2-byte weight access moves (read + write) for the eager LTD."""
+    # drive (precomputed one step ahead): the float written per neuron and
+    # the inhibitory flag read (a compute-bound kernel: Philox and Box-Muller)
+    if deferred:
+        return {
+            "neuron": 64.0 * n + 4.0 * spikes,
+            "rows": 56.0 * spikes + 8.0 * events,
+            "ltd": 32.0 * n / 32.0 + 8.0 * m_plastic / 32.0,
+            "drive": 5.0 * n,
+        }
     return {
         "neuron": 64.0 * n + 4.0 * spikes,
         "rows": 40.0 * spikes + 8.0 * events,
         "ltd": 16.0 * spikes + 8.0 * in_plastic,
         "ltd_sector": 16.0 * spikes + (8.0 + 64.0) * in_plastic,
+        "drive": 5.0 * n,
     }
 
 
@@ -275,13 +275,13 @@ def run_ours(a):
 
     extra = None
     if not a.no_extra:
-        batch = run_batch_config(local, rank, world, dist)
+        batch = run_batch_config(local, rank, world, dist, cpu=not a.no_cpu)
         if rank == 0 and world > 1:
             # single-GPU configurations are reported by the one-GPU run; the
             # other ranks would only wait for them
             extra = {"lif_batch_c3": batch}
         elif rank == 0:
-            extra = run_extra_configs(local)
+            extra = run_extra_configs(local, cpu=not a.no_cpu)
             extra["lif_batch_c3"] = batch
             extra["izh_c2_phase2_rules"] = run_phase2_rules(local)
             if not a.no_surrogate:
@@ -297,7 +297,8 @@ def run_ours(a):
 
     if rank == 0:
         peak, peak_src = peaks()
-        kb = kernel_bytes(net.n, prof_spikes, prof_events, prof_spikes * mean_in_plastic)
+        kb = kernel_bytes(net.n, prof_spikes, prof_events, prof_spikes * mean_in_plastic,
+                          float(np.count_nonzero(net.plastic)), sched == 5)
         total_prof_ms = sum(v[0] for v in prof.values())
         kernels = {}
         for name, (kms, kl) in prof.items():
@@ -305,6 +306,9 @@ def run_ours(a):
             kernels[name] = {"avg_launch_us": avg_s * 1e6, "share": kms / total_prof_ms,
                              "bytes_per_launch": kb.get(name),
                              "achieved_gbs": kb[name] / avg_s / 1e9 if name in kb else None}
+        if sched == 5 and "ltd" in kernels:
+            kernels["row_block_flush"] = kernels.pop("ltd")
+            kb["row_block_flush"] = kb.pop("ltd")
         if "ltd" in kernels:
             kernels["ltd"]["sector_bytes_per_launch"] = kb["ltd_sector"]
             kernels["ltd"]["sector_gbs"] = kb["ltd_sector"] / (kernels["ltd"]["avg_launch_us"] / 1e6) / 1e9
@@ -312,12 +316,11 @@ def run_ours(a):
         nk_bytes = kb[dom]
         nk_avg_s = kernels[dom]["avg_launch_us"] / 1e6
         achieved = nk_bytes / nk_avg_s / 1e9
-        ratio = profile_traffic_ratio(dom)
-        traffic = ratio * nk_bytes if ratio is not None else None
         value = events_all / (ms_max / 1e3)
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_max / a.steps,
+            "ms_per_sim_step": ms_max / a.steps / S,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded generator, configuration shapes)",
             "config": {
@@ -331,17 +334,17 @@ def run_ours(a):
                 "network_build_s": round(gen_s, 2),
                 "step_schedule": {1: "fused", 2: "split (LTD beside next neuron update)",
                                   3: "fused, 4 blocks/SM",
-                                  4: "split, narrow LTD grid"}.get(sched, "undecided"),
+                                  4: "split, narrow LTD grid",
+                                  5: "deferred LTD (row walks + row-block flush)"}.get(sched, "undecided"),
                 "autotune_us_per_step": sched_us,
             },
             "roofline": {
                 "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": traffic,
+                "frac": achieved / peak, "traffic": None,
+                "traffic_note": "DRAM bytes come from an ncu capture of this command, summarised "
+                                "under profiles/; bench.py does not measure them",
                 "kernel": dom, "bytes_per_launch": nk_bytes, "avg_launch_us": nk_avg_s * 1e6,
                 "peak_source": peak_src, "spikes_per_step_profiled": prof_spikes,
-                "traffic_ratio": ratio,
-                "traffic_gbs": traffic / nk_avg_s / 1e9 if traffic is not None else None,
-                "traffic_source": "profiles/izh_c2_step_kernels_ncu.md (DRAM / algorithmic bytes, full-size capture)",
                 "profile_first_steps_spikes_events": units,
                 "kernels": kernels,
             },
@@ -447,7 +450,31 @@ def timed_run(eng, steps, stream):
     return e0.elapsed_time(e1), c1[1] - c0[1], c1[3] - c0[3]
 
 
-def run_extra_configs(local):
+def literal_sample(net, cfg, drive, seconds, max_steps=2000):
+    """The CPU restatement of engine.rs (FP64, per-synapse state, OpenMP over
+    the neuron update as rayon parallelises it) on this host's cores, stepped
+    from rest for about `seconds` after one warm-up step."""
+    from oracle.oracle import LiteralOracle
+    threads = os.cpu_count() or 1
+    lit = LiteralOracle(net, cfg, drive, threads=threads)
+    lit.step(1)
+    e0 = lit.events()
+    t0 = time.perf_counter()
+    steps = 0
+    while steps < 2 or (time.perf_counter() - t0 < seconds and steps < max_steps):
+        lit.step(1)
+        steps += 1
+    dt = time.perf_counter() - t0
+    ev = lit.events() - e0
+    lit.close()
+    return {"value": ev / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "ns_per_step": dt * 1e9 / steps, "steps": steps, "events_in_sample": int(ev),
+            "x_realtime": steps * cfg.dt_ms / (dt * 1e3),
+            "sample": f"{steps} simulation steps from rest after 1 warm-up step ({dt:.1f} s); C++ "
+                      "restatement of engine.rs, FP64, per-synapse state; not the Rust binary"}
+
+
+def run_extra_configs(local, cpu=True):
     """The other configurations on this GPU: the plain LIF network (10k / 1M,
     dt 0.1 ms, 1 ms delay, 1 s) and the plain Hodgkin-Huxley network (100k /
     10M, Rush-Larsen, dt 0.01 ms, 1 ms delay), each timed with windowed
@@ -461,6 +488,7 @@ def run_extra_configs(local):
         cfg.device = local
         res = {"neurons": net.n, "synapses": net.m, "dt_ms": cfg.dt_ms,
                "delay_steps": cfg.delay_steps, "timed_steps": steps}
+        peak, _ = peaks()
         for label, wsteps in (("windowed", 0), ("per_step", 1)):
             cfg.window_steps = wsteps
             eng = SimulationEngine(net, cfg, drive)
@@ -468,10 +496,24 @@ def run_extra_configs(local):
             eng.run(warm)
             ms, spikes, events = timed_run(eng, steps, stream)
             eng.close()
+            s_step, e_step = spikes / steps, events / steps
+            # algorithmic bytes per step: LIF v + refractory r/w 16 and the
+            # int64 accumulator read + zero 16 per neuron; HH V, m, h, n r/w
+            # 32, AMPA / GABA conductances r/w 16 and two accumulator rows
+            # read + zero 16 (64 per neuron); 8 per spike (row_ptr pair) and
+            # per event (column 4, weight 4)
+            per_n = 32.0 if name == "lif_c1" else 64.0
+            b_step = per_n * net.n + 8.0 * s_step + 8.0 * e_step
             res[label] = {"ns_per_step": ms * 1e6 / steps,
                           "x_realtime": (steps * cfg.dt_ms) / ms,
                           "events_per_s": events / (ms / 1e3),
-                          "spikes_per_step": spikes / steps}
+                          "spikes_per_step": s_step,
+                          "bytes_per_step": b_step,
+                          "hbm_frac": b_step / (ms * 1e-3 / steps) / 1e9 / peak}
+        if cpu:
+            res["cpu_baseline"] = literal_sample(net, cfg, drive, 8.0 if name == "lif_c1" else 12.0)
+            res["speedup_vs_cpu_per_step"] = (res["cpu_baseline"]["ns_per_step"] /
+                                              res["windowed"]["ns_per_step"])
         out[name] = res
     return out
 
@@ -517,7 +559,7 @@ def run_phase2_rules(local, warm=500, steps=500):
     return out
 
 
-def run_batch_config(local, rank, world, dist, n_nets=256):
+def run_batch_config(local, rank, world, dist, n_nets=256, cpu=True):
     """The batched sweep: 256 LIF networks (log-uniform 2k..50k neurons,
     in-degree 50..200), one batch per GPU (networks bin-packed by size across
     ranks, no per-step communication), 1000 steps of dt 0.1 ms timed after
@@ -560,6 +602,7 @@ def run_batch_config(local, rank, world, dist, n_nets=256):
         # per-step-path bytes: v, refractory r/w 16 + accumulator read/zero 16
         # per neuron, col + w 8 per event, spike index 8
         bytes_step = 32.0 * n_all + 8.0 * s_step + 8.0 * e_step
+        peak, _ = peaks()
         res[label] = {"ms": ms, "ns_per_step": ms * 1e6 / steps,
                       "x_realtime": (steps * cfg.dt_ms) / ms,
                       "events_per_s": events / (ms / 1e3),
@@ -567,9 +610,52 @@ def run_batch_config(local, rank, world, dist, n_nets=256):
                       "spikes_per_step": s_step,
                       "rate_hz": s_step / n_all / (cfg.dt_ms / 1e3),
                       "step_path_bytes_per_s": bytes_step * steps / (ms / 1e3),
+                      "hbm_frac": bytes_step * steps / (ms / 1e3) / 1e9 / peak,
                       "window_steps": wlen,
                       "window_tuner_us_per_step": wtune}
+    if cpu and rank == 0 and world == 1:
+        res["cpu_baseline"] = batch_cpu_sample(nets, seeds, cfg, variants)
+        for label, _ in variants:
+            res[label]["speedup_vs_cpu_per_step"] = (res["cpu_baseline"][label]["ns_per_step"] /
+                                                     res[label]["ns_per_step"])
     return res
+
+
+def batch_cpu_sample(nets, seeds, cfg, variants, n_sample=8, seconds=1.5):
+    """The batch on the CPU restatement: the networks run one after another
+    (as independent engines would), sampled. Eight networks (the smallest,
+    the largest, six drawn at random) are each stepped from rest for about
+    `seconds`; the batch's time per step is their time per step scaled by
+    the batch's neurons + synapses over theirs."""
+    rng = np.random.default_rng(7)
+    sizes = np.array([x.n for x in nets])
+    pick = {int(np.argmin(sizes)), int(np.argmax(sizes))}
+    rest = [q for q in range(len(nets)) if q not in pick]
+    pick.update(int(q) for q in rng.choice(rest, n_sample - 2, replace=False))
+    pick = sorted(pick)
+    cost_all = float(sum(x.n + x.m for x in nets))
+    cost_s = float(sum(nets[q].n + nets[q].m for q in pick))
+    out = {"sampled_networks": pick, "scale": cost_all / cost_s}
+    for label, drv in variants:
+        ns_sum, ev_sum, steps_min, threads = 0.0, 0.0, None, 1
+        for q in pick:
+            c = copy.copy(cfg)
+            c.seed = seeds[q]
+            r = literal_sample(nets[q], c, drv, seconds)
+            ns_sum += r["ns_per_step"]
+            ev_sum += r["events_in_sample"] / r["steps"]
+            steps_min = r["steps"] if steps_min is None else min(steps_min, r["steps"])
+            threads = r["cores"]
+        ns_batch = ns_sum * out["scale"]
+        ev_batch = ev_sum * out["scale"]
+        out[label] = {"value": ev_batch / (ns_batch * 1e-9), "unit": UNIT, "cores": threads,
+                      "kind": "port", "ns_per_step": ns_batch,
+                      "x_realtime": cfg.dt_ms / (ns_batch * 1e-6),
+                      "sample": f"{len(pick)} of {len(nets)} networks, each stepped from rest for "
+                                f"about {seconds} s (at least {steps_min} steps), one after "
+                                "another; time per step scaled by neurons + synapses "
+                                f"(x{out['scale']:.1f}); C++ restatement of engine.rs, FP64"}
+    return out
 
 
 def _surrogate_eval(net, cfg, drive, sur, local, steps):
@@ -729,19 +815,21 @@ def run_cpu_baseline(net, cfg, drive, seconds, warm=None, events_per_step=None):
     dt = time.perf_counter() - t0
     ev = lit.events() - e0
     lit.close()
-    # the network bursts (50-step stretches of ~1M and of ~1k events per
-    # step), so a short sample's own event count says little; the rate is
-    # the workload's mean events per step over the measured time per step
-    # (the engine's per-step cost is dominated by its O(M) loops)
-    value = (events_per_step * steps / dt) if events_per_step else ev / dt
-    return {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+    # value: the events the sample itself processed over its time. The
+    # network bursts (50-step stretches of ~1M and of ~1k events per step)
+    # while the engine's per-step cost is set by its O(M) loops, so the
+    # per-simulation-step time is the stable figure; the rate at the GPU
+    # workload's mean activity is given beside it
+    return {"value": ev / dt, "unit": UNIT, "cores": threads, "kind": "port",
             "ms_per_sim_step": dt * 1e3 / steps, "events_in_sample": int(ev),
-            "mean_events_per_sim_step": events_per_step,
+            "events_per_sim_step": ev / steps,
+            "value_at_workload_mean_events": (events_per_step * steps / dt) if events_per_step else None,
+            "workload_mean_events_per_sim_step": events_per_step,
             "sample": f"{steps} simulation steps of the same 1M/100M network, started from the GPU "
                       f"run's state after its timed region, after 1 warm-up step ({dt:.1f} s); "
-                      "value = the workload's mean events per step (GPU run) / the measured time "
-                      "per step; C++ restatement of engine.rs, FP64, per-synapse state, OpenMP "
-                      "over the neuron update only (as rayon); not the Rust binary"}
+                      "value = the sample's own events / its time; C++ restatement of engine.rs, "
+                      "FP64, per-synapse state, OpenMP over the neuron update only (as rayon); "
+                      "not the Rust binary"}
 
 
 def run_reference(a):
@@ -774,7 +862,10 @@ def run_reference(a):
         lit.step(1)
     dt = time.perf_counter() - t0
     ev = lit.events() - e0
-    value = ev_mean * a.steps / dt
+    # the sample's own events over its own time (the bursty network makes
+    # this vary with where the sample falls; ms_per_sim_step is the stable
+    # figure, the engine's cost per step being set by its O(M) loops)
+    value = ev / dt
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": dt * 1e3 / a.steps, "higher_is_better": True,
@@ -784,14 +875,17 @@ def run_reference(a):
                                                 "one step = 1 simulation step"),
                    "neurons": net.n, "synapses": net.m, "sim_steps_per_step": 1},
         "impl": "reference",
+        "ms_per_sim_step": dt * 1e3 / a.steps,
+        "events_per_sim_step": ev / a.steps,
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "ms_per_sim_step": dt * 1e3 / a.steps, "events_in_sample": int(ev),
+                         "value_at_warmup_mean_events": ev_mean * a.steps / dt,
                          "sample": f"{a.steps} simulation steps after {a.warmup} warm-up steps, "
-                                   f"from the state {a.ref_warm_steps} steps after rest; value = "
-                                   f"the mean events per step of steps {a.ref_warm_steps // 3}.."
-                                   f"{a.ref_warm_steps} ({ev_mean:.0f}, the oracle's FP64 engine) / "
-                                   f"the measured time per step ({ev} events in the sample); "
-                                   "C++ restatement of engine.rs (the Rust crate does not build "
-                                   "here), FP64, per-synapse state, OpenMP over the neuron update"},
+                                   f"from the state {a.ref_warm_steps} steps after rest (the "
+                                   f"oracle's FP64 engine); value = the sample's own {ev} events "
+                                   "/ its time; C++ restatement of engine.rs (the Rust crate does "
+                                   "not build here), FP64, per-synapse state, OpenMP over the "
+                                   "neuron update"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out), flush=True)
@@ -803,9 +897,9 @@ def main():
         import torch
         torch.cuda.set_device(0)
         if a.only == "c1c4":
-            print(json.dumps(run_extra_configs(0)), flush=True)
+            print(json.dumps(run_extra_configs(0, cpu=not a.no_cpu)), flush=True)
         elif a.only == "c3":
-            print(json.dumps(run_batch_config(0, 0, 1, None, a.c3_nets)), flush=True)
+            print(json.dumps(run_batch_config(0, 0, 1, None, a.c3_nets, cpu=not a.no_cpu)), flush=True)
         elif a.only == "phase2":
             print(json.dumps(run_phase2_rules(0)), flush=True)
         else:

@@ -141,7 +141,14 @@ typedef struct ns_config {
    * kernel, 6 resident blocks per SM), 2 = split (LTD of step k on a second
    * stream beside the neuron update of step k+1), 3 = fused with 4 resident
    * blocks per SM, 4 = split with a narrow (2 blocks/SM) LTD grid that leaves
-   * room for the neuron kernel. All give bit-identical results. */
+   * room for the neuron kernel, 5 = deferred LTD: the LTD of synapse j->i
+   * at a spike of i waits, as a bit in i's 32-step spike history, until j's
+   * row is next walked (at j's spike, before delivery) or flushed (every
+   * row once per 32 steps, a 32nd of the rows per step, beside the walks),
+   * so LTD reads and writes weights in CSR order instead of at random
+   * positions. Schedule 5 applies to pair STDP on one GPU (no homeostasis,
+   * R-STDP, consolidation or STP; schedule 3 is run otherwise). All give
+   * bit-identical results. */
   uint32_t step_schedule;
   /* windowed stepping for delay_steps >= 2 without STDP or homeostasis: W
    * steps per neuron kernel (W <= delay_steps), one row-walk pass per window.
@@ -368,7 +375,7 @@ ns_status ns_upload_stp(ns_handle* h, const uint8_t* has_stp, const double* stp)
 ns_status ns_step_traced(ns_handle* h, uint64_t* pos_out, uint64_t cap, uint64_t* n_events);
 
 /* Schedule in use (0 while the autotuner has not decided) and the measured
- * microseconds per step of schedules 1..4 in us_per_step[4] (0 if untimed). */
+ * microseconds per step of schedules 1..5 in us_per_step[5] (0 if untimed). */
 ns_status ns_get_schedule(ns_handle* h, uint32_t* schedule, double* us_per_step);
 
 /* Windowed stepping: the window length in use (0 = step-synchronous), and
@@ -389,8 +396,11 @@ ns_status ns_counters(ns_handle* h, uint64_t out[4]);
 ns_status ns_get_stream(ns_handle* h, void** stream);
 
 /* Runs n_steps eagerly and serially with CUDA events around every kernel;
- * adds the device time (ms) and launch count of the neuron, row-walk, LTD and
- * homeostasis kernels to kernel_ms[4] / launches[4]. Same numerics as ns_step. */
+ * adds the device time (ms) and launch count of the neuron, row-walk, LTD
+ * (under schedule 5: the row-block flush), homeostasis and drive kernels to
+ * kernel_ms[5] / launches[5]. The kernels are the ones the step graphs run
+ * (the drive precomputed where graph chunks precompute it). Same numerics
+ * as ns_step. */
 ns_status ns_profile_steps(ns_handle* h, uint32_t n_steps, double* kernel_ms, uint64_t* launches);
 
 /* --- single-network sharding (one process per GPU; no counterpart in the
@@ -439,7 +449,10 @@ ns_status ns_shard_step_end(ns_handle* h);
  * until exit; n above NS_NOALLOC_MAX_NEURONS is rejected with
  * NS_ERR_INVALID_ARG. Nothing is allocated or freed. The first call on a
  * device looks up the array's device address (cudaGetSymbolAddress with that
- * device current): make that first call before any stream capture. All calls
+ * device current): make that first call before any stream capture. The
+ * address is kept for the life of the process and does not survive
+ * cudaDeviceReset: after a reset of the device, reload the library before
+ * calling this entry point on that device again. All calls
  * on a device share the one scratch array, so calls whose kernels overlap on
  * the GPU (different streams without ordering between them) race; order
  * them on one stream. */

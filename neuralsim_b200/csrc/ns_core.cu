@@ -32,7 +32,10 @@ struct ns_handle {
   int sms = 148;
   cudaStream_t st = nullptr;
   cudaStream_t st2 = nullptr;       // LTD of step k beside the neuron kernel of step k+1
+  cudaStream_t st3 = nullptr;       // drive of step k+1 beside the walks of step k
   cudaEvent_t ev_rows = nullptr, ev_ltd = nullptr;
+  cudaEvent_t ev_nrn = nullptr, ev_drv = nullptr;
+  int drive_blocks = 0;
   std::string err;
   bool have_neurons = false, have_csr = false;
   uint64_t n = 0, n_pad = 0, m = 0, m_pad = 0;
@@ -53,8 +56,13 @@ struct ns_handle {
   int fused_blocks[2] = {0, 0};
   int ltd_blocks = 0;
   int ltd_narrow_blocks = 0;
-  uint32_t sched = 0;               // 1 fused, 2 split, 3 fused (4 blocks/SM), 4 split (narrow LTD); 0 = undecided
-  double tune_us[5] = {0, 0, 0, 0, 0};
+  uint32_t sched = 0;               // 1 fused, 2 split, 3 fused (4 blocks/SM), 4 split (narrow LTD),
+                                    // 5 deferred LTD; 0 = undecided
+  double tune_us[6] = {0, 0, 0, 0, 0, 0};
+  // deferred LTD (schedule 5): LTDs wait in the spike histories of the trace
+  // records (pending); the rows' trace starts match the last step (synced)
+  bool defer_pending = false, defer_synced = false;
+  int flush_blocks = 0;
   int homeo_blocks = 0;
   int ntypes_acc = 1;
   // batch of networks: per-neuron network ids, per-network seeds and bases
@@ -605,6 +613,19 @@ prop_fn pick_prop(uint32_t mode, uint32_t wf, bool ext) {
 #undef NSR
 }
 
+// deferred LTD: row walks that apply the rows' pending LTDs first, and the
+// per-step row-block flush
+prop_fn pick_prop_defer(uint32_t mode, uint32_t wf) {
+  bool cond = mode == NS_INPUT_CONDUCTANCE_REF || mode == NS_INPUT_CONDUCTANCE_FRESH;
+  bool bf = wf == NS_WEIGHT_BF16;
+  if (cond) return bf ? ns::k_rows<true, true, false, true> : ns::k_rows<true, false, false, true>;
+  return bf ? ns::k_rows<false, true, false, true> : ns::k_rows<false, false, false, true>;
+}
+
+ltd_fn pick_flush(uint32_t wf) {
+  return wf == NS_WEIGHT_BF16 ? ns::k_flush<true> : ns::k_flush<false>;
+}
+
 ltd_fn pick_ltd(uint32_t wf, bool ext) {
   if (wf == NS_WEIGHT_BF16) return ext ? ns::k_ltd<true, true> : ns::k_ltd<true, false>;
   return ext ? ns::k_ltd<false, true> : ns::k_ltd<false, false>;
@@ -654,8 +675,66 @@ bool overlap_ltd(const ns_handle* h) {
   return h->cfg.stdp_enabled && !h->cfg.homeostasis_enabled && !tail_on(h);
 }
 
-// schedule a step uses (fused at 6 blocks/SM until the autotuner decides)
-uint32_t sched_of(const ns_handle* h) { return h->sched == 0 ? 1u : h->sched; }
+// Deferred LTD (schedule 5) serves pair STDP on one GPU: homeostasis and
+// the R-STDP / consolidation / STP rules read or write weights between the
+// walks of a step, sharded ranks keep the eager lists.
+bool defer_ok(const ns_handle* h) {
+  return h->cfg.stdp_enabled && !h->cfg.homeostasis_enabled && !ext_on(h) && h->shard_world <= 1 &&
+         !h->win;
+}
+
+// schedule a step uses (fused at 6 blocks/SM until the autotuner decides;
+// the deferred schedule falls back to the fused one where it does not apply)
+uint32_t sched_of(const ns_handle* h) {
+  const uint32_t s = h->sched == 0 ? 1u : h->sched;
+  return (s == 5 && !defer_ok(h)) ? 3u : s;
+}
+
+// Pending deferred LTDs applied: every row flushed to the last completed
+// step. Before the host reads or replaces weights and before eager steps.
+ns_status defer_settle(ns_handle* h) {
+  if (!h->defer_pending) return NS_OK;
+  if (h->cfg.weight_format == NS_WEIGHT_BF16)
+    ns::k_defer_flush_all<true><<<h->sms * 8, 256, 0, h->st>>>(h->d);
+  else
+    ns::k_defer_flush_all<false><<<h->sms * 8, 256, 0, h->st>>>(h->d);
+  h->launches += 1;
+  CK(cudaGetLastError());
+  h->defer_pending = false;
+  h->defer_synced = true;
+  return NS_OK;
+}
+
+// Trace starts of every row at the last completed step, from a state with no
+// LTD pending (after uploads and eager steps), before deferred steps.
+ns_status defer_prepare(ns_handle* h) {
+  if (h->defer_synced) return NS_OK;
+  ns::k_defer_sync<<<h->sms * 4, 256, 0, h->st>>>(h->d);
+  h->launches += 1;
+  CK(cudaGetLastError());
+  h->defer_synced = true;
+  return NS_OK;
+}
+
+ns_status defer_before(ns_handle* h, uint32_t sched) {
+  return sched == 5 ? defer_prepare(h) : defer_settle(h);
+}
+
+void defer_after(ns_handle* h, uint32_t sched, uint32_t n) {
+  if (n == 0) return;
+  if (sched == 5) h->defer_pending = true;
+  else h->defer_synced = false;
+}
+
+// An upload replaces state or weights: LTDs still pending are applied to
+// the weights first (a state upload may keep them), and the trace starts
+// are taken again from the uploaded state before the next deferred step.
+ns_status defer_reset(ns_handle* h) {
+  ns_status r = defer_settle(h);
+  h->defer_pending = false;
+  h->defer_synced = false;
+  return r;
+}
 
 // In-place all-gather of the step's spike bitmap: rank r owns words
 // [r*W, (r+1)*W), W = 64 words per tile times the tiles of a rank.
@@ -668,13 +747,82 @@ cudaError_t shard_exchange(ns_handle* h) {
   return r == ncclSuccess ? cudaSuccess : cudaErrorUnknown;
 }
 
+// The Poisson-kick, Gaussian and Poisson-conductance drives are computed by
+// k_drive ahead of the neuron kernel: inside graph chunks the drive of step
+// k+1 beside the walks of step k, in eager steps right before the neuron
+// kernel. The neuron kernel draws the reference-uniform drive itself.
+bool precompute_drive(const ns_handle* h) {
+  const uint32_t k = h->drive.kind;
+  return k == NS_DRIVE_POISSON_KICK || k == NS_DRIVE_GAUSS || k == NS_DRIVE_POISSON_CONDUCTANCE;
+}
+
+// The drive of an eager step j, on the handle's stream before its neuron
+// kernel; returns the device view to launch the neuron kernel with.
+NsDev with_drive(ns_handle* h, const NsDev& d, uint32_t j) {
+  NsDev dd = d;
+  if (precompute_drive(h)) {
+    ns::k_drive<<<h->drive_blocks, 256, 0, h->st>>>(dd, j);
+    h->launches += 1;
+  }
+  return dd;
+}
+
+// Drive of a step: drawn by the neuron kernel or precomputed right before it
+// (eager steps), read from the buffer with the next step's drive launched
+// beside the walks (graph chunks), or read from the buffer (the chunk's last
+// step).
+enum { kDriveEager = 0, kDriveNext = 1, kDriveLast = 2 };
+
 // Enqueues one step (graph-node index j). With overlap, the LTD kernel of
 // step j runs on the side stream beside the neuron kernel of step j+1 and the
 // row walk of step j+1 waits for it; *ltd_pending tracks the open branch.
 cudaError_t enqueue_step(ns_handle* h, uint32_t j, bool* ltd_pending, uint32_t sched,
-                         bool stim = false) {
+                         bool stim = false, int drv = kDriveEager, bool* drv_pending = nullptr) {
   neuron_fn nf = pick_neuron(h->cfg.model, h->cfg.input_mode, h->d.pidx != nullptr, stim);
-  nf<<<h->d.tiles_own, ns::kThreads, 0, h->st>>>(h->d, j);
+  NsDev dd = h->d;
+  cudaError_t e = cudaSuccess;
+  if (drv == kDriveEager) {
+    dd = with_drive(h, dd, j);
+  } else if (*drv_pending) {
+    e = cudaStreamWaitEvent(h->st, h->ev_drv, 0);
+    if (e != cudaSuccess) return e;
+    *drv_pending = false;
+  }
+  auto launch_neuron = [&](const NsDev& x) -> cudaError_t {
+    nf<<<h->d.tiles_own, ns::kThreads, 0, h->st>>>(x, j);
+    if (drv != kDriveNext) return cudaSuccess;
+    // the next step's drive beside this step's walks
+    cudaError_t r = cudaEventRecord(h->ev_nrn, h->st);
+    if (r == cudaSuccess) r = cudaStreamWaitEvent(h->st3, h->ev_nrn, 0);
+    if (r != cudaSuccess) return r;
+    ns::k_drive<<<h->drive_blocks, 256, 0, h->st3>>>(x, j + 1);
+    r = cudaEventRecord(h->ev_drv, h->st3);
+    if (r == cudaSuccess) *drv_pending = true;
+    return r;
+  };
+  if (sched == 5) {
+    // deferred LTD: neuron update; the flush of row block k mod 32 on the
+    // side stream beside this step's row walks and the next neuron update;
+    // the row walks wait for the previous step's flush
+    dd.defer = 1;
+    if ((e = launch_neuron(dd)) != cudaSuccess) return e;
+    if (*ltd_pending) {
+      e = cudaStreamWaitEvent(h->st, h->ev_ltd, 0);
+      if (e != cudaSuccess) return e;
+      *ltd_pending = false;
+    }
+    e = cudaEventRecord(h->ev_rows, h->st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(h->st2, h->ev_rows, 0);
+    if (e != cudaSuccess) return e;
+    pick_flush(h->cfg.weight_format)<<<h->flush_blocks, 256, 0, h->st2>>>(dd, j);
+    e = cudaEventRecord(h->ev_ltd, h->st2);
+    if (e != cudaSuccess) return e;
+    *ltd_pending = true;
+    pick_prop_defer(h->cfg.input_mode, h->cfg.weight_format)<<<h->prop_blocks, 256, 0, h->st>>>(dd, j);
+    if (h->cfg.track_rates) launch_homeo(h, dd, j, h->st);
+    return cudaGetLastError();
+  }
+  if ((e = launch_neuron(dd)) != cudaSuccess) return e;
   if (h->shard_world > 1) {
     // every rank's spike bitmap words, then the other ranks' tiles rebuilt
     cudaError_t e = shard_exchange(h);
@@ -720,6 +868,7 @@ cudaError_t join_ltd(ns_handle* h, bool* ltd_pending) {
 }
 
 uint64_t launches_per_step(const ns_handle* h, uint32_t sched) {
+  if (sched == 5) return 3u + (homeo_or_rates(h) ? 1u : 0u);
   const bool split = sched == 2 || sched == 4;
   return 2u + ((split && h->cfg.stdp_enabled) ? 1u : 0u) + (homeo_or_rates(h) ? 1u : 0u) +
          (tail_on(h) ? 2u : 0u) + (h->shard_world > 1 ? 1u : 0u);
@@ -781,7 +930,7 @@ cudaError_t enqueue_window(ns_handle* h, uint32_t j0, uint32_t Wc, bool stim = f
 }
 
 ns_status get_graph(ns_handle* h, uint32_t S, uint32_t sched, cudaGraphExec_t* out) {
-  const uint64_t key = ((uint64_t)(h->win ? h->wcur : 0u) << 40) | ((uint64_t)S * 4u + sched);
+  const uint64_t key = ((uint64_t)(h->win ? h->wcur : 0u) << 40) | ((uint64_t)S * 8u + sched);
   auto it = h->graphs.find(key);
   if (it != h->graphs.end()) { *out = it->second; return NS_OK; }
   cudaGraph_t g;
@@ -792,7 +941,14 @@ ns_status get_graph(ns_handle* h, uint32_t S, uint32_t sched, cudaGraphExec_t* o
     for (uint32_t j = 0; j < S && ce == cudaSuccess; j += h->wcur)
       ce = enqueue_window(h, j, std::min(h->wcur, S - j));
   } else {
-    for (uint32_t j = 0; j < S && ce == cudaSuccess; ++j) ce = enqueue_step(h, j, &pending, sched);
+    // the chunk's first drive, then each step's neuron kernel launches the
+    // next one beside its walks
+    const bool pre = precompute_drive(h);
+    bool dpend = false;
+    if (pre) ns::k_drive<<<h->drive_blocks, 256, 0, h->st>>>(h->d, 0);
+    for (uint32_t j = 0; j < S && ce == cudaSuccess; ++j)
+      ce = enqueue_step(h, j, &pending, sched, false,
+                        !pre ? kDriveEager : (j + 1 < S ? kDriveNext : kDriveLast), &dpend);
     if (ce == cudaSuccess) ce = join_ltd(h, &pending);
   }
   ns::k_advance<<<1, 1, 0, h->st>>>(h->ctl, S);
@@ -814,6 +970,11 @@ ns_status get_graph(ns_handle* h, uint32_t S, uint32_t sched, cudaGraphExec_t* o
 ns_status run_steps(ns_handle* h, uint32_t n, uint32_t sched) {
   const uint32_t S = h->cfg.graph_chunk;
   if (h->win && n) h->win_ran = true;
+  if (n) {
+    ns_status r = defer_before(h, sched);
+    if (r) return r;
+  }
+  defer_after(h, sched, n);
   uint32_t left = n;
   if (left >= S) {
     cudaGraphExec_t ex;
@@ -822,7 +983,7 @@ ns_status run_steps(ns_handle* h, uint32_t n, uint32_t sched) {
     while (left >= S) {
       CK(cudaGraphLaunch(ex, h->st));
       if (h->win) h->launches += ((S + h->wcur - 1) / h->wcur) * window_launches(h) + 1;
-      else h->launches += (uint64_t)S * launches_per_step(h, sched) + 1;
+      else h->launches += (uint64_t)S * launches_per_step(h, sched) + 1 + (precompute_drive(h) ? S : 0u);
       left -= S;
     }
   }
@@ -870,19 +1031,30 @@ ns_status autotune(ns_handle* h, uint32_t budget, uint32_t* used) {
   CK(cudaMemcpyAsync(&step, &h->ctl->step_base, 8, cudaMemcpyDeviceToHost, h->st));
   CK(cudaStreamSynchronize(h->st));
   if (step < h->next_tune_step) return NS_OK;
+  // the snapshot holds no pending deferred LTD; every candidate starts from it
+  ns_status rs = defer_settle(h);
+  if (rs) return rs;
+  const bool synced0 = h->defer_synced;
   Snapshot sn;
   CK(snapshot_take(h, sn));
   cudaEvent_t e0, e1;
   cudaError_t ce = cudaEventCreate(&e0);
   if (ce == cudaSuccess) ce = cudaEventCreate(&e1);
   if (ce != cudaSuccess) { snapshot_free(sn); return fail(h, NS_ERR_CUDA, cudaGetErrorString(ce)); }
-  const uint32_t cand[4] = {1, 2, 3, 4};
-  double us[5] = {0, 0, 0, 0, 0};
+  const uint32_t cand[5] = {1, 2, 3, 4, 5};
+  const int ncand = defer_ok(h) ? 5 : 4;
+  double us[6] = {0, 0, 0, 0, 0, 0};
   ns_status r = NS_OK;
-  for (int q = 0; q < 4 && r == NS_OK; ++q) {
-    if (q > 0 && (ce = snapshot_restore(h, sn)) != cudaSuccess) break;
+  for (int q = 0; q < ncand && r == NS_OK; ++q) {
+    if (q > 0) {
+      if ((ce = snapshot_restore(h, sn)) != cudaSuccess) break;
+      h->defer_pending = false;
+      h->defer_synced = synced0;
+    }
     cudaGraphExec_t ex;
     if ((r = get_graph(h, kTuneWindow, cand[q], &ex))) break;
+    if ((r = defer_before(h, cand[q]))) break;
+    defer_after(h, cand[q], kTuneWindow);
     float ms = 0;
     if ((ce = cudaEventRecord(e0, h->st)) != cudaSuccess) break;
     if ((ce = cudaGraphLaunch(ex, h->st)) != cudaSuccess) break;
@@ -890,7 +1062,8 @@ ns_status autotune(ns_handle* h, uint32_t budget, uint32_t* used) {
     if ((ce = cudaEventSynchronize(e1)) != cudaSuccess) break;
     if ((ce = cudaEventElapsedTime(&ms, e0, e1)) != cudaSuccess) break;
     us[cand[q]] = ms * 1e3 / kTuneWindow;
-    h->launches += (uint64_t)kTuneWindow * launches_per_step(h, cand[q]) + 1;
+    h->launches += (uint64_t)kTuneWindow * launches_per_step(h, cand[q]) + 1 +
+                   (precompute_drive(h) ? kTuneWindow : 0u);
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -898,7 +1071,7 @@ ns_status autotune(ns_handle* h, uint32_t budget, uint32_t* used) {
   if (r) return r;
   if (ce != cudaSuccess) return fail(h, NS_ERR_CUDA, std::string("autotune: ") + cudaGetErrorString(ce));
   uint32_t best = 1;
-  for (uint32_t q = 1; q <= 4; ++q) {
+  for (uint32_t q = 1; q <= (uint32_t)ncand; ++q) {
     h->tune_us[q] = us[q];
     if (us[q] < us[best]) best = q;
   }
@@ -1091,7 +1264,7 @@ ns_status ns_create(const ns_config* cfg, ns_handle** out) {
   *out = nullptr;
   const ns_config& c = *cfg;
   if (c.model > 2 || c.input_mode > 4 || c.hh_integrator > 1 || c.weight_format > 1 ||
-      c.step_schedule > 4 || c.window_steps > 4096)
+      c.step_schedule > 5 || c.window_steps > 4096)
     return fail(h, NS_ERR_INVALID_ARG, "unknown model / input mode / integrator / weight format");
   if (!(c.dt_ms > 0) || !is_fin(c.dt_ms)) return fail(h, NS_ERR_INVALID_ARG, "dt_ms must be > 0");
   if (c.delay_steps < 1 || c.delay_steps > 4096) return fail(h, NS_ERR_INVALID_ARG, "delay_steps in [1, 4096]");
@@ -1124,6 +1297,9 @@ ns_status ns_create(const ns_config* cfg, ns_handle** out) {
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->st2, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_rows, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_ltd, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->st3, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_nrn, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_drv, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, h->dev);
   if (e != cudaSuccess) {
     g_err = std::string("device init: ") + cudaGetErrorString(e);
@@ -1147,6 +1323,8 @@ ns_status ns_create(const ns_config* cfg, ns_handle** out) {
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pick_ltd(c.weight_format, ext), 256, 0) != cudaSuccess || nb < 1) nb = 4;
     h->ltd_blocks = h->sms * nb;
     h->ltd_narrow_blocks = h->sms * 2;
+    h->flush_blocks = h->sms * 2;
+    h->drive_blocks = h->sms * 2;
     nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ns::k_homeostasis<true>, 256, 0) != cudaSuccess || nb < 1) nb = 4;
     h->homeo_blocks = h->sms * nb;
@@ -1170,6 +1348,8 @@ ns_status ns_destroy(ns_handle* h) {
   if (!h) return NS_ERR_NULL_HANDLE;
   cudaSetDevice(h->dev);
   if (h->st) cudaStreamSynchronize(h->st);
+  if (h->st2) cudaStreamSynchronize(h->st2);
+  if (h->st3) cudaStreamSynchronize(h->st3);
   drop_graphs(h);
   free_bag(h->neuron_allocs);
   free_bag(h->csr_allocs);
@@ -1182,9 +1362,11 @@ ns_status ns_destroy(ns_handle* h) {
   if (h->ctl) cudaFree(h->ctl);
   if (h->stage) cudaFreeHost(h->stage);
   if (h->stim_dev) cudaFree(h->stim_dev);
-  if (h->st2) cudaStreamSynchronize(h->st2);
   if (h->ev_rows) cudaEventDestroy(h->ev_rows);
   if (h->ev_ltd) cudaEventDestroy(h->ev_ltd);
+  if (h->ev_nrn) cudaEventDestroy(h->ev_nrn);
+  if (h->ev_drv) cudaEventDestroy(h->ev_drv);
+  if (h->st3) cudaStreamDestroy(h->st3);
   if (h->st2) cudaStreamDestroy(h->st2);
   if (h->st) cudaStreamDestroy(h->st);
   delete h;
@@ -1221,6 +1403,10 @@ ns_status ns_upload_neurons(ns_handle* h, const ns_neuron_soa* s) {
   if (h->have_csr && s->n != h->n && !h->batch_uploading)
     return fail(h, NS_ERR_INVALID_ARG, "n differs from the CSR");
   CK(cudaSetDevice(h->dev));
+  {
+    ns_status r0 = defer_reset(h);
+    if (r0) return r0;
+  }
   CK(cudaStreamSynchronize(h->st));
   if (h->n_nets && !h->batch_uploading) {
     // a plain upload ends batch mode
@@ -1341,13 +1527,13 @@ ns_status ns_upload_neurons(ns_handle* h, const ns_neuron_soa* s) {
 #define DA(ptr, cnt) if ((st = dalloc(h, B, &(ptr), (cnt)))) return st;
     DA(d.v, np) DA(d.u, np) DA(d.I, np) DA(d.gm, np) DA(d.gh, np) DA(d.gn, np)
     DA(d.refr, np) DA(d.refr_steps, np) DA(d.inh, np) DA(d.outp, np)
-    DA(d.pre, np) DA(d.post, np) DA(d.rec, 2 * np) DA(d.last, np) DA(d.rate, np)
+    DA(d.pre, np) DA(d.post, np) DA(d.rec, 2 * np) DA(d.last, np) DA(d.rate, np) DA(d.lstart, np)
     for (int q = 0; q < 7; ++q) d.par[q] = nullptr;
     for (int q = 0; q < npar; ++q) DA(d.par[q], np)
     for (int t = 0; t < 4; ++t) DA(d.G[t], np)
     DA(d.bitmap, np / 32 + 2) DA(d.spk, 2 * np)
     DA(d.tile_cnt, 2 * ((uint64_t)h->ntiles + 1)) DA(d.tile_off, 2 * ((uint64_t)h->ntiles + 1))
-    DA(h->pidx_buf, np) DA(h->ptab_buf, 256 * 8) DA(d.stim, np)
+    DA(h->pidx_buf, np) DA(h->ptab_buf, 256 * 8) DA(d.stim, np) DA(d.drv, 2 * np)
 #undef DA
   }
   auto up = [&](void* dst, const void* src, size_t bytes) {
@@ -1513,6 +1699,10 @@ ns_status ns_upload_csr(ns_handle* h, uint64_t n, uint64_t m, const uint64_t* ro
       if (col[e] < lo || col[e] >= hi) return fail(h, NS_ERR_CSR, "a sharded rank's synapse targets a neuron it does not own");
   }
   CK(cudaSetDevice(h->dev));
+  {
+    ns_status r0 = defer_reset(h);
+    if (r0) return r0;
+  }
   CK(cudaStreamSynchronize(h->st));
   CK(cudaStreamSynchronize(h->st2));
   // everything is built into a new set of buffers (the handle keeps working
@@ -1850,6 +2040,8 @@ ns_status ns_step(ns_handle* h, uint32_t n_steps, ns_step_stats* out) {
       h->win_ran = true;
     } else {
       bool pending = false;
+      if ((r = defer_before(h, sched_of(h)))) return r;
+      defer_after(h, sched_of(h), 1);
       CK(enqueue_step(h, 0, &pending, sched_of(h), true));
       CK(join_ltd(h, &pending));
       h->launches += launches_per_step(h, sched_of(h));
@@ -1889,6 +2081,9 @@ ns_status ns_step_traced(ns_handle* h, uint64_t* pos_out, uint64_t cap, uint64_t
   CK(cudaSetDevice(h->dev));
   fill_scalars(h);
   if ((r = flush_stim(h))) return r;
+  // an eager step: deferred LTDs applied first
+  if ((r = defer_before(h, 1))) return r;
+  defer_after(h, 1, 1);
   std::vector<void*> tmp;
   unsigned long long *off = nullptr, *pos = nullptr;
   ns_status st;
@@ -1896,7 +2091,7 @@ ns_status ns_step_traced(ns_handle* h, uint64_t* pos_out, uint64_t cap, uint64_t
     free_bag(tmp);
     return st;
   }
-  NsDev d = h->d;
+  NsDev d = with_drive(h, h->d, 0);
   neuron_fn nf = pick_neuron(h->cfg.model, h->cfg.input_mode, h->d.pidx != nullptr, h->stim_step);
   h->stim_step = false;
   const bool ext = ext_on(h);
@@ -1991,6 +2186,7 @@ ns_status ns_download_state(ns_handle* h, ns_neuron_soa* o, float* w_out) {
   ns_status r = ready(h);
   if (r) return r;
   CK(cudaSetDevice(h->dev));
+  if ((r = defer_settle(h))) return r;
   CK(cudaStreamSynchronize(h->st));
   const uint64_t n = h->n;
   NsDev& d = h->d;
@@ -2065,6 +2261,7 @@ ns_status ns_upload_state(ns_handle* h, const ns_neuron_soa* in, const float* w_
   if (r) return r;
   if (in->n != h->n) return fail(h, NS_ERR_INVALID_ARG, "state n differs from the network");
   CK(cudaSetDevice(h->dev));
+  if ((r = defer_reset(h))) return r;
   CK(cudaStreamSynchronize(h->st));
   const uint64_t n = h->n;
   NsDev& d = h->d;
@@ -2186,8 +2383,10 @@ ns_status ns_upload_eligibility(ns_handle* h, const uint8_t* eligible, const flo
     for (uint64_t q = 0; q < h->m; ++q)
       if (!is_fin(values[q])) return fail(h, NS_ERR_NONFINITE, "non-finite eligibility value");
   CK(cudaSetDevice(h->dev));
+  ns_status r = defer_reset(h);
+  if (r) return r;
   CK(cudaStreamSynchronize(h->st));
-  ns_status r = set_eligibility(h, eligible, values);
+  r = set_eligibility(h, eligible, values);
   if (r) return r;
   if (h->have_neurons && h->ctl) return rebase_reward(h, 0u);
   return NS_OK;
@@ -2267,6 +2466,10 @@ ns_status ns_upload_stp(ns_handle* h, const uint8_t* has_stp, const double* stp)
   if (!h) return NS_ERR_NULL_HANDLE;
   if (!h->have_csr) return fail(h, NS_ERR_STATE, "upload the CSR first");
   CK(cudaSetDevice(h->dev));
+  {
+    ns_status r0 = defer_reset(h);
+    if (r0) return r0;
+  }
   CK(cudaStreamSynchronize(h->st));
   const bool cond = h->cfg.input_mode == NS_INPUT_CONDUCTANCE_REF ||
                     h->cfg.input_mode == NS_INPUT_CONDUCTANCE_FRESH;
@@ -2359,6 +2562,7 @@ ns_status ns_weight_stats(ns_handle* h, double* mean, double* stddev) {
   if (r) return r;
   if (h->m == 0) { *mean = 0; *stddev = 0; return NS_OK; }
   CK(cudaSetDevice(h->dev));
+  if ((r = defer_settle(h))) return r;
   double* acc = nullptr;
   CK(cudaMalloc(&acc, 16));
   CK(cudaMemsetAsync(acc, 0, 16, h->st));
@@ -2418,24 +2622,39 @@ ns_status ns_profile_steps(ns_handle* h, uint32_t n_steps, double* kernel_ms, ui
   neuron_fn nf0 = pick_neuron(h->cfg.model, h->cfg.input_mode, h->d.pidx != nullptr, h->stim_step);
   h->stim_step = false;
   const bool ext = ext_on(h);
-  prop_fn pf = pick_prop(h->cfg.input_mode, h->cfg.weight_format, ext);
-  ltd_fn lf = pick_ltd(h->cfg.weight_format, ext);
+  // the deferred schedule profiles its own kernels: the row walks that apply
+  // pending LTDs and the row-block flush (in the LTD slot)
+  const uint32_t psched = sched_of(h);
+  const bool dfr = psched == 5;
+  if ((r = defer_before(h, psched))) return r;
+  defer_after(h, psched, n_steps);
+  NsDev dd = h->d;
+  dd.defer = dfr ? 1 : 0;
+  // the drive precomputed as inside graph chunks, timed as its own kernel
+  const bool pre = precompute_drive(h);
+  prop_fn pf = dfr ? pick_prop_defer(h->cfg.input_mode, h->cfg.weight_format)
+                   : pick_prop(h->cfg.input_mode, h->cfg.weight_format, ext);
+  ltd_fn lf = dfr ? pick_flush(h->cfg.weight_format) : pick_ltd(h->cfg.weight_format, ext);
+  const int lblocks = dfr ? h->flush_blocks : h->ltd_blocks;
   // kernels in order neuron, rows, ltd (+ the R-STDP / consolidation tail),
-  // homeostasis; serial, one event pair each
-  const bool on[4] = {true, true, h->cfg.stdp_enabled != 0 || tail_on(h), homeo_or_rates(h)};
-  std::vector<cudaEvent_t> ev((size_t)n_steps * 8);
+  // homeostasis, drive; serial, one event pair each
+  const bool on[5] = {true, true, h->cfg.stdp_enabled != 0 || tail_on(h), homeo_or_rates(h), pre};
+  std::vector<cudaEvent_t> ev((size_t)n_steps * 10);
   for (auto& e : ev) CK(cudaEventCreate(&e));
   for (uint32_t j = 0; j < n_steps; ++j) {
-    cudaEvent_t* e = &ev[(size_t)j * 8];
+    cudaEvent_t* e = &ev[(size_t)j * 10];
+    CK(cudaEventRecord(e[8], h->st));
+    if (pre) ns::k_drive<<<h->drive_blocks, 256, 0, h->st>>>(dd, j);
+    CK(cudaEventRecord(e[9], h->st));
     CK(cudaEventRecord(e[0], h->st));
-    (j == 0 ? nf0 : nf)<<<h->d.tiles_own, ns::kThreads, 0, h->st>>>(h->d, j);
+    (j == 0 ? nf0 : nf)<<<h->d.tiles_own, ns::kThreads, 0, h->st>>>(dd, j);
     if (tail_on(h)) ns::k_setup<<<1, 32, 0, h->st>>>(h->d, j);
     CK(cudaEventRecord(e[1], h->st));
     CK(cudaEventRecord(e[2], h->st));
-    pf<<<h->prop_blocks, 256, 0, h->st>>>(h->d, j);
+    pf<<<h->prop_blocks, 256, 0, h->st>>>(dd, j);
     CK(cudaEventRecord(e[3], h->st));
     CK(cudaEventRecord(e[4], h->st));
-    if (h->cfg.stdp_enabled) lf<<<h->ltd_blocks, 256, 0, h->st>>>(h->d, j);
+    if (h->cfg.stdp_enabled) lf<<<lblocks, 256, 0, h->st>>>(dd, j);
     if (tail_on(h)) launch_tail(h, h->d, j, h->st);
     CK(cudaEventRecord(e[5], h->st));
     CK(cudaEventRecord(e[6], h->st));
@@ -2447,10 +2666,10 @@ ns_status ns_profile_steps(ns_handle* h, uint32_t n_steps, double* kernel_ms, ui
   CK(cudaStreamSynchronize(h->st));
   uint64_t nl = 0;
   for (uint32_t j = 0; j < n_steps; ++j)
-    for (int q = 0; q < 4; ++q) {
+    for (int q = 0; q < 5; ++q) {
       if (!on[q]) continue;
       float ms = 0;
-      CK(cudaEventElapsedTime(&ms, ev[(size_t)j * 8 + 2 * q], ev[(size_t)j * 8 + 2 * q + 1]));
+      CK(cudaEventElapsedTime(&ms, ev[(size_t)j * 10 + 2 * q], ev[(size_t)j * 10 + 2 * q + 1]));
       kernel_ms[q] += ms;
       launches[q] += 1;
       ++nl;
@@ -2580,7 +2799,8 @@ ns_status ns_shard_step_begin(ns_handle* h) {
   if (h->sched == 0) h->sched = 3;
   neuron_fn nf = pick_neuron(h->cfg.model, h->cfg.input_mode, h->d.pidx != nullptr, h->stim_step);
   h->stim_step = false;
-  nf<<<h->d.tiles_own, ns::kThreads, 0, h->st>>>(h->d, 0);
+  const NsDev dd = with_drive(h, h->d, 0);
+  nf<<<h->d.tiles_own, ns::kThreads, 0, h->st>>>(dd, 0);
   h->launches += 1;
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(h->st));
@@ -2630,7 +2850,7 @@ ns_status ns_get_schedule(ns_handle* h, uint32_t* schedule, double* us_per_step)
   if (!h) return NS_ERR_NULL_HANDLE;
   if (schedule) *schedule = h->sched;
   if (us_per_step)
-    for (int q = 0; q < 4; ++q) us_per_step[q] = h->tune_us[q + 1];
+    for (int q = 0; q < 5; ++q) us_per_step[q] = h->tune_us[q + 1];
   return NS_OK;
 }
 

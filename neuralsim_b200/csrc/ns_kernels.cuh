@@ -165,6 +165,20 @@ struct NsDev {
   const uint8_t* elig_flag;        // synapse carries an eligibility trace [m_pad]
   const float* stp_f;              // STP factor per synapse, or null
   float* stim;                     // pending host stimulus per neuron [n_pad]
+  // deferred LTD (step schedule 5): rec[k][i].x holds the bits of i's
+  // spikes over the last 32 steps (bit b: step k - b) instead of its decayed
+  // pre trace; per source j, lstart[j] = {pre trace after step astep (float
+  // bits), astep}: every LTD of j's synapses at steps <= astep is applied,
+  // those after wait for j's next row walk or for the row's flush, which
+  // comes every 32 steps (rows in 32 contiguous blocks, block k mod 32 at
+  // step k).
+  uint2* lstart;
+  int defer;
+  // drive precomputed by k_drive for the Poisson-kick, Gaussian and
+  // Poisson-conductance kinds, parity-buffered by step: drv[k & 1][i] is the
+  // amount drive_of gives neuron i at step k (the neuron kernel draws the
+  // reference-uniform kind itself)
+  float* drv;
 };
 
 __device__ __forceinline__ bool bit_of(const uint32_t* bm, uint32_t i) {
@@ -326,6 +340,64 @@ __device__ __forceinline__ void gauss_pair(const U4& x, float& z0, float& z1) {
   z1 = rr * sn;
 }
 
+// The drive amount of neuron i at step k from its precomputed value: the
+// current (uniform, Gaussian), the kick or the added conductance, by kind.
+__device__ __forceinline__ void drive_from(const NsDev& d, float val, float& addI, float& kick,
+                                           float& addg) {
+  addI = (d.drive_kind == 1 || d.drive_kind == 3) ? val : 0.f;
+  kick = d.drive_kind == 2 ? val : 0.f;
+  addg = d.drive_kind == 4 ? val : 0.f;
+}
+
+// Drive of step k for every neuron, precomputed one step ahead beside the
+// walks of the previous step (kinds 2, 3, 4: one Philox draw per neuron, or
+// per pair for the Gaussian drive; the same draws and arithmetic as the
+// neuron kernel's own). Thread per neuron pair.
+__global__ void __launch_bounds__(256) k_drive(NsDev d, uint32_t jstep) {
+  const uint64_t k = d.ctl->step_base + jstep;
+  float* out = d.drv + (k & 1) * d.n_pad;
+  const uint64_t pairs = d.n_pad >> 1;
+  for (uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; p < pairs;
+       p += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t i0 = 2 * p;
+    U4 y2[2] = {U4{0u, 0u, 0u, 0u}, U4{0u, 0u, 0u, 0u}};
+    float z[2] = {0.f, 0.f};
+    uchar2 ih = make_uchar2(0, 0);
+    if (d.drive_kind == 3) ih = *reinterpret_cast<const uchar2*>(d.inh + i0);
+    if (d.net_of == nullptr) {
+      if (d.drive_kind == 3) {
+        gauss_pair(draw(d.seed, (uint32_t)(i0 >> 1), k, kStreamDrive), z[0], z[1]);
+      } else {
+        y2[0] = poisson_draw(d.seed, (uint32_t)i0, k);
+        y2[1] = poisson_draw(d.seed, (uint32_t)(i0 + 1), k);
+      }
+    } else {
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        uint64_t sd;
+        uint32_t li;
+        drive_key(d, i0 + e, sd, li);
+        if (d.drive_kind == 3) {
+          float g0, g1;
+          gauss_pair(draw(sd, li >> 1, k, kStreamDrive), g0, g1);
+          z[e] = (li & 1u) ? g1 : g0;
+        } else {
+          y2[e] = poisson_draw(sd, li, k);
+        }
+      }
+    }
+    const uint8_t inhv[2] = {ih.x, ih.y};
+    float val[2];
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      float addI, kick, addg;
+      drive_of(d, y2[e], z[e], inhv[e], addI, kick, addg);
+      val[e] = d.drive_kind == 2 ? kick : (d.drive_kind == 4 ? addg : addI);
+    }
+    *reinterpret_cast<float2*>(out + i0) = make_float2(val[0], val[1]);
+  }
+}
+
 // Input assembly and model update of one neuron at step k (the arithmetic
 // the float oracle mirrors). S: delivered synaptic input per accumulator
 // type; G: the neuron's conductances (conductance modes).
@@ -417,11 +489,11 @@ __global__ void k_setup(NsDev d, uint32_t jstep) {
 }
 
 // ---------------------------------------------------------------------------
-// Kernel 1: fused drive + neuron update + trace decay + ordered compaction.
-// Thread t of tile T owns the neuron pairs (T*2048 + r*512 + 2t, +1), r < 4,
-// so every state array is read with 8-byte coalesced loads and one Philox
-// draw feeds the Gaussian drive of both neurons of a pair. All loads of a pair
-// are issued before any store. Each tile writes its spikes, ascending, to its
+// Kernel 1: neuron update + trace decay + ordered compaction, with the
+// step's drive (precomputed by k_drive one step ahead, or drawn here for the
+// reference-uniform kind). Thread t of tile T owns the neuron pairs
+// (T*2048 + r*512 + 2t, +1), r < 4, so every state array is read with 8-byte
+// coalesced loads. All loads of a pair are issued before any store. Each tile writes its spikes, ascending, to its
 // own slice of the spike buffer (warp ballots + a 32-entry scan), so no tile
 // waits for another; the last tile to finish does the step's bookkeeping.
 // ---------------------------------------------------------------------------
@@ -544,12 +616,18 @@ __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
       }
     }
     float2 p2 = make_float2(0.f, 0.f), q2 = make_float2(0.f, 0.f);
+    uint2 hist = make_uint2(0u, 0u);
     if (d.stdp) {
       p2 = *reinterpret_cast<const float2*>(d.pre + i0);
       q2 = *reinterpret_cast<const float2*>(d.post + i0);
+      if (d.defer) {
+        // spike bits of the previous step's records (the other parity)
+        const float4 pr = *reinterpret_cast<const float4*>(d.rec + (par_k ^ 1u) * d.n_pad + i0);
+        hist = make_uint2(__float_as_uint(pr.x), __float_as_uint(pr.z));
+      }
     }
-    uchar2 ih = make_uchar2(0, 0);
-    if (d.drive_kind == 3) ih = *reinterpret_cast<const uchar2*>(d.inh + i0);
+    float2 pdrv = make_float2(0.f, 0.f);
+    if (d.drive_kind >= 2) pdrv = *reinterpret_cast<const float2*>(d.drv + par_k * d.n_pad + i0);
     // ---- delivered synaptic input for this step (the slot is cleared) ----
     if (d.inbits && lane == 0) {
       uint32_t* ib = d.inbits + (uint64_t)slot * (d.n_pad >> 5) + ((i0 - 2 * (uint64_t)lane) >> 5);
@@ -564,41 +642,14 @@ __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
         *reinterpret_cast<longlong2*>(d.acc + ((uint64_t)t * d.D + slot) * d.n_pad + i0) =
             make_longlong2(0, 0);
     }
-    // ---- drive draws: one Philox per pair ----
-    U4 y2[2];
-    float z[2] = {0.f, 0.f};
-    if (d.net_of == nullptr) {
-      y2[0] = y2[1] = U4{0u, 0u, 0u, 0u};
-      if (d.drive_kind == 3) {
-        gauss_pair(draw(d.seed, (uint32_t)(i0 >> 1), k, kStreamDrive), z[0], z[1]);
-      } else if (d.drive_kind == 1) {
-        y2[0] = draw(d.seed, (uint32_t)i0, k, kStreamDrive);
-        y2[1] = draw(d.seed, (uint32_t)(i0 + 1), k, kStreamDrive);
-      } else if (d.drive_kind != 0) {
-        y2[0] = poisson_draw(d.seed, (uint32_t)i0, k);
-        y2[1] = poisson_draw(d.seed, (uint32_t)(i0 + 1), k);
-      }
-    } else {
-      // batch: the pair may straddle two networks, so each neuron draws
-      // from its own network's stream (Gaussian pairs by local index)
-#pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        uint64_t sd;
-        uint32_t li;
-        drive_key(d, i0 + e, sd, li);
-        y2[e] = U4{0u, 0u, 0u, 0u};
-        if (d.drive_kind == 3) {
-          float g0, g1;
-          gauss_pair(draw(sd, li >> 1, k, kStreamDrive), g0, g1);
-          z[e] = (li & 1u) ? g1 : g0;
-        } else if (d.drive_kind == 1) {
-          y2[e] = draw(sd, li, k, kStreamDrive);
-        } else if (d.drive_kind != 0) {
-          y2[e] = poisson_draw(sd, li, k);
-        }
-      }
+    // ---- drive: the reference-uniform kind draws here (one Philox per
+    // neuron; batches refuse this kind); the other kinds were precomputed
+    // by k_drive ----
+    U4 y2[2] = {U4{0u, 0u, 0u, 0u}, U4{0u, 0u, 0u, 0u}};
+    if (d.drive_kind == 1) {
+      y2[0] = draw(d.seed, (uint32_t)i0, k, kStreamDrive);
+      y2[1] = draw(d.seed, (uint32_t)(i0 + 1), k, kStreamDrive);
     }
-    const uint8_t inhv[2] = {ih.x, ih.y};
     float2 sti = make_float2(0.f, 0.f);
     if (stim_on) {
       sti = *reinterpret_cast<const float2*>(d.stim + i0);
@@ -610,7 +661,8 @@ __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
     for (int e = 0; e < 2; ++e) {
       const uint64_t i = i0 + e;
       float addI, kick, addg;
-      drive_of(d, y2[e], z[e], inhv[e], addI, kick, addg);
+      if (d.drive_kind >= 2) drive_from(d, e == 0 ? pdrv.x : pdrv.y, addI, kick, addg);
+      else drive_of(d, y2[e], 0.f, 0, addI, kick, addg);
       float Se[NT], Ge[4];
 #pragma unroll
       for (int t = 0; t < NT; ++t) Se[t] = S[t][e];
@@ -634,8 +686,16 @@ __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
       const float qv0 = q2.x * d.em, qv1 = q2.y * d.em;
       *reinterpret_cast<float2*>(d.pre + i0) = make_float2(pv0, pv1);
       *reinterpret_cast<float2*>(d.post + i0) = make_float2(qv0, qv1);
-      const float4 rr = make_float4(spk[0] ? -pv0 : pv0, spk[0] ? -qv0 : qv0,
-                                    spk[1] ? -pv1 : pv1, spk[1] ? -qv1 : qv1);
+      float4 rr;
+      if (d.defer) {
+        // deferred LTD: spike bits of the last 32 steps instead of the pre
+        // trace (the row walks take the source's pre trace from lstart)
+        rr = make_float4(__uint_as_float((hist.x << 1) | (spk[0] ? 1u : 0u)), spk[0] ? -qv0 : qv0,
+                         __uint_as_float((hist.y << 1) | (spk[1] ? 1u : 0u)), spk[1] ? -qv1 : qv1);
+      } else {
+        rr = make_float4(spk[0] ? -pv0 : pv0, spk[0] ? -qv0 : qv0,
+                         spk[1] ? -pv1 : pv1, spk[1] ? -qv1 : qv1);
+      }
       *reinterpret_cast<float4*>(rec_k + i0) = rr;
     }
     // ---- write back state ----
@@ -846,11 +906,50 @@ __device__ __forceinline__ float ext_store(const NsDev& d, const float* fr, uint
   return d.cons ? (w1 - fr[1]) * fr[2] : w1;
 }
 
+// Deferred LTD of one lane's four synapses of source j: pb[q] holds, for
+// synapse q, the bits (b = steps before the current one) of its target's
+// spikes whose LTD has not been applied; T = current step - astep, ps the
+// source's pre trace after step astep. The source's pre trace at step
+// astep + t is ps times exp(-dt/tau+) t times, one float rounding per
+// multiply: the chain the neuron kernel runs. Each LTD is the eager one,
+// w = clamp(w - A- pre), stored (BF16: rounded) before the next, in step order.
+template <bool BF16>
+__device__ __forceinline__ void apply_pending(const NsDev& d, float ps, uint32_t T, const uint32_t pb[4],
+                                              float w[4]) {
+  uint32_t U = pb[0] | pb[1] | pb[2] | pb[3];
+  if (!U) return;
+  float x = ps;
+  uint32_t t = 0;
+  do {
+    const uint32_t b = 31u - __clz(U);   // earliest pending step: k - b = astep + (T - b)
+    const uint32_t tt = T - b;
+    while (t < tt) { x = x * d.ep; ++t; }
+    const float dm = d.neg_a_minus * x;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      if ((pb[q] >> b) & 1u) {
+        float y = clampw(w[q] + dm, d.w_min, d.w_max);
+        if (BF16) y = bf16_bits_to_f32(f32_to_bf16_bits(y));
+        w[q] = y;
+      }
+    }
+    U &= ~(1u << b);
+  } while (U);
+}
+
+// Bits b in [lo, T-1] of a 32-step spike history (T >= 32: all from lo).
+__device__ __forceinline__ uint32_t pending_mask(uint32_t T, uint32_t lo) {
+  const uint32_t m = T >= 32u ? 0xffffffffu : ((1u << T) - 1u);
+  return m & ~((1u << lo) - 1u);
+}
+
 // Row walk of spiking source j (the item-th spike of the step): bookkeeping
 // (log entry, last spike step, trace bump), then the CSR row in 128-entry
 // chunks: accumulation into the delay slot and LTP (LTP then LTD when the
-// target spiked in this step too).
-template <bool COND, bool BF16, bool EXT>
+// target spiked in this step too). DEFER: the row's pending LTDs (its
+// targets' spikes since the row was last walked or flushed) are applied
+// first, so that delivery reads the weight the eager schedule would.
+template <bool COND, bool BF16, bool EXT, bool DEFER = false>
 __device__ __forceinline__ void row_item(const NsDev& d, const StepCtx& c, uint32_t item, uint32_t j,
                                          int lane, unsigned long long& ev, uint32_t& outs) {
   const bool STDP = c.stdp, HOMEO = c.homeo;
@@ -862,6 +961,7 @@ __device__ __forceinline__ void row_item(const NsDev& d, const StepCtx& c, uint3
   const uint8_t rp = STDP ? __ldg(d.row_plastic + j) : 0;
   const uint8_t rt = COND ? __ldg(d.row_type + j) : 0;
   float pj = 0.0f;
+  uint2 ls = make_uint2(0u, 0u);
   if (lane == 0) {
     const long long lst = d.last[j];
     if (c.log_ok) d.log_idx[c.log_base + item] = j;
@@ -874,10 +974,25 @@ __device__ __forceinline__ void row_item(const NsDev& d, const StepCtx& c, uint3
       const long long dk = lst < 0 ? -1 : (long long)k - lst;
       const float fp = (dk >= 0 && (unsigned long long)dk < d.Kp) ? d.Ep[dk] : 0.0f;
       const float fm = (dk >= 0 && (unsigned long long)dk < d.Km) ? d.Em[dk] : 0.0f;
-      pj = fabsf(rj.x) * fp + 1.0f;
+      // the decayed pre trace: the record's |x| (eager), or the trace the
+      // neuron kernel wrote this step (deferred: the record holds spike bits)
+      pj = (DEFER ? d.pre[j] : fabsf(rj.x)) * fp + 1.0f;
       d.pre[j] = pj;
       d.post[j] = fabsf(rj.y) * fm + 1.0f;
+      if (DEFER) {
+        ls = d.lstart[j];
+        d.lstart[j] = make_uint2(__float_as_uint(pj), (uint32_t)k);
+      }
     }
+  }
+  // deferred LTD: the row's trace start and the pending-bit mask (steps
+  // astep+1 .. k-1; step k's LTD is the same-step one below, with pj)
+  float dps = 0.0f;
+  uint32_t dT = 0u, dmask = 0u;
+  if (DEFER && STDP && rp) {
+    dps = __uint_as_float(__shfl_sync(0xffffffffu, ls.x, 0));
+    dT = __shfl_sync(0xffffffffu, (uint32_t)k - ls.y, 0);
+    dmask = pending_mask(dT, 1u);
   }
   const unsigned long long tbase = d.trace_pos ? d.trace_off[item] : 0ull;
   const uint64_t rb = beg & ~3ull;
@@ -903,11 +1018,19 @@ __device__ __forceinline__ void row_item(const NsDev& d, const StepCtx& c, uint3
     // target records for LTP, gathered before the atomics are issued
     bool pl[4] = {false, false, false, false};
     float tq[4];
+    uint32_t pb[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       pl[q] = STDP && rp && inr[q] && (rp == 1 || __ldg(d.plastic + e0 + q));
-      tq[q] = pl[q] ? c.rec_k[cc[q]].y : 0.f;
+      if (DEFER) {
+        const float2 r = pl[q] ? c.rec_k[cc[q]] : make_float2(0.f, 0.f);
+        tq[q] = r.y;
+        pb[q] = __float_as_uint(r.x) & dmask;
+      } else {
+        tq[q] = pl[q] ? c.rec_k[cc[q]].y : 0.f;
+      }
     }
+    if (DEFER) apply_pending<BF16>(d, dps, dT, pb, w);
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       if (!inr[q]) continue;
@@ -1051,6 +1174,112 @@ __device__ __forceinline__ void ltd_item(const NsDev& d, const StepCtx& c, uint3
   }
 }
 
+// Flush of source j's row (deferred LTD): applies the LTDs of its targets'
+// spikes at steps astep+1 .. k (a target that spikes at step k while j does
+// not included, as the eager LTD walk of step k would) and moves the row's
+// trace start to step k. The row of a source that spikes at step k is left
+// to that step's row walk. Only the synapses of row j are written (a 4-entry
+// group that reaches into a neighbouring row is written entry by entry).
+template <bool BF16>
+__device__ __forceinline__ void flush_row(const NsDev& d, uint64_t k, const float2* rec_k, uint32_t j,
+                                          int lane) {
+  const uint8_t rp = __ldg(d.row_plastic + j);
+  if (!rp) return;
+  if (__float_as_uint(rec_k[j].x) & 1u) return;
+  const uint2 ls = d.lstart[j];
+  const uint32_t T = (uint32_t)k - ls.y;
+  if (T == 0u) return;
+  const uint32_t mask = pending_mask(T, 0u);
+  const float ps = __uint_as_float(ls.x);
+  const uint64_t beg = __ldg(d.row_ptr + j), end = __ldg(d.row_ptr + j + 1);
+  const uint64_t rb = beg & ~3ull;
+  const uint32_t nrow = end > beg ? (uint32_t)((end - rb + 127) >> 7) : 0u;
+  for (uint32_t ch = 0; ch < nrow; ++ch) {
+    const uint64_t e0 = rb + 128ull * ch + 4ull * lane;
+    if (!(e0 < end && e0 + 4 > beg)) continue;
+    const uint4 c4 = __ldg(reinterpret_cast<const uint4*>(d.col + e0));
+    const uint32_t cc[4] = {c4.x, c4.y, c4.z, c4.w};
+    uint32_t pb[4];
+    bool all4 = true;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const uint64_t e = e0 + q;
+      const bool pl = e >= beg && e < end && (rp == 1 || __ldg(d.plastic + e));
+      all4 = all4 && pl;
+      pb[q] = pl ? (__float_as_uint(rec_k[cc[q]].x) & mask) : 0u;
+    }
+    if (!(pb[0] | pb[1] | pb[2] | pb[3])) continue;
+    float w[4];
+    load_w4(d, BF16, e0, w);
+    apply_pending<BF16>(d, ps, T, pb, w);
+    if (BF16) {
+      if (all4) {
+        uint2 raw;
+        raw.x = (uint32_t)f32_to_bf16_bits(w[0]) | ((uint32_t)f32_to_bf16_bits(w[1]) << 16);
+        raw.y = (uint32_t)f32_to_bf16_bits(w[2]) | ((uint32_t)f32_to_bf16_bits(w[3]) << 16);
+        *reinterpret_cast<uint2*>(d.w16 + e0) = raw;
+      } else {
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          if (pb[q]) d.w16[e0 + q] = f32_to_bf16_bits(w[q]);
+      }
+    } else {
+      if (all4) {
+        *reinterpret_cast<float4*>(d.w32 + e0) = make_float4(w[0], w[1], w[2], w[3]);
+      } else {
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          if (pb[q]) d.w32[e0 + q] = w[q];
+      }
+    }
+  }
+  if (lane == 0) {
+    // the pre trace at step k: the neuron kernel's decay chain from astep
+    float x = ps;
+    for (uint32_t t = 0; t < T; ++t) x = x * d.ep;
+    d.lstart[j] = make_uint2(__float_as_uint(x), (uint32_t)k);
+  }
+}
+
+// Deferred LTD, step k: the flush of row block k mod 32 (rows
+// [b * ceil(n/32), (b+1) * ceil(n/32))), one warp per row. Runs beside the
+// row walks of step k (the rows of step k's spikers are skipped) and the
+// neuron update of step k+1; the row walks of step k+1 wait for it.
+template <bool BF16>
+__global__ void __launch_bounds__(256) k_flush(NsDev d, uint32_t jstep) {
+  const uint64_t k = d.ctl->step_base + jstep;
+  const float2* rec_k = d.rec + (k & 1) * d.n_pad;
+  const uint64_t per = (d.n + 31) / 32;
+  const uint64_t r0 = (k & 31u) * per;
+  const uint64_t r1 = r0 + per < d.n ? r0 + per : d.n;
+  const int lane = threadIdx.x & 31;
+  const uint64_t nw = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  for (uint64_t j = r0 + blockIdx.x * (uint64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); j < r1; j += nw)
+    flush_row<BF16>(d, k, rec_k, (uint32_t)j, lane);
+}
+
+// Deferred LTD: every row flushed to the last completed step (before the
+// host reads or replaces weights, or an eager step runs).
+template <bool BF16>
+__global__ void __launch_bounds__(256) k_defer_flush_all(NsDev d) {
+  const uint64_t k = d.ctl->step_base - 1;
+  const float2* rec_k = d.rec + (k & 1) * d.n_pad;
+  const int lane = threadIdx.x & 31;
+  const uint64_t nw = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  for (uint64_t j = blockIdx.x * (uint64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); j < d.n; j += nw)
+    flush_row<BF16>(d, k, rec_k, (uint32_t)j, lane);
+}
+
+// Deferred LTD from a state with none pending (after uploads and eager
+// steps): every row's trace start is the pre trace after the last completed
+// step.
+__global__ void k_defer_sync(NsDev d) {
+  const uint32_t k1 = (uint32_t)(d.ctl->step_base - 1);
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < d.n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    d.lstart[i] = make_uint2(__float_as_uint(d.pre[i]), k1);
+}
+
 __device__ __forceinline__ void flush_counters(const NsDev& d, uint64_t k, unsigned long long ev,
                                                uint32_t outs, unsigned long long* s_ev,
                                                uint32_t* s_out) {
@@ -1100,7 +1329,7 @@ __global__ void __launch_bounds__(256, MINB) k_prop_fused(NsDev d, uint32_t jste
 
 // Kernel 2a / 2b (split schedule): the row walks, then the LTD lists on a
 // second stream beside the next step's neuron kernel.
-template <bool COND, bool BF16, bool EXT>
+template <bool COND, bool BF16, bool EXT, bool DEFER = false>
 __global__ void __launch_bounds__(256, 4) k_rows(NsDev d, uint32_t jstep) {
   __shared__ uint32_t s_toff[kSmemTiles + 1];
   __shared__ unsigned long long s_ev;
@@ -1114,7 +1343,7 @@ __global__ void __launch_bounds__(256, 4) k_rows(NsDev d, uint32_t jstep) {
   unsigned long long ev = 0ull;
   uint32_t outs = 0u;
   for (uint32_t item = wglob; item < c.cnt; item += nw)
-    row_item<COND, BF16, EXT>(d, c, item, sv.at(item), lane, ev, outs);
+    row_item<COND, BF16, EXT, DEFER>(d, c, item, sv.at(item), lane, ev, outs);
   flush_counters(d, c.k, ev, outs, &s_ev, &s_out);
 }
 

@@ -422,19 +422,21 @@ class SimulationEngine:
 
     def profile_steps(self, n_steps: int):
         """Per-kernel device time over n_steps eager serial steps:
-        {"neuron": (ms_total, launches), "rows": ..., "ltd": ..., "homeostasis": ...}"""
-        ms = (C.c_double * 4)()
-        ln = (C.c_uint64 * 4)()
+        {"neuron": (ms_total, launches), "rows": ..., "ltd": ..., "homeostasis": ...,
+        "drive": ...} (ltd: the row-block flush under the deferred-LTD schedule)"""
+        ms = (C.c_double * 5)()
+        ln = (C.c_uint64 * 5)()
         self._check(self.lib.ns_profile_steps(self._h, int(n_steps), ms, ln))
-        names = ("neuron", "rows", "ltd", "homeostasis")
-        return {names[q]: (ms[q], int(ln[q])) for q in range(4) if ln[q]}
+        names = ("neuron", "rows", "ltd", "homeostasis", "drive")
+        return {names[q]: (ms[q], int(ln[q])) for q in range(5) if ln[q]}
 
     def schedule(self):
         """(schedule in use, {schedule: measured us/step}) from the autotuner."""
         sc = C.c_uint32()
-        us = (C.c_double * 4)()
+        us = (C.c_double * 5)()
         self._check(self.lib.ns_get_schedule(self._h, C.byref(sc), us))
-        return int(sc.value), {q + 1: us[q] for q in range(4)}
+        # schedules 1-4 always; 5 (deferred LTD) where it applies and was timed
+        return int(sc.value), {q + 1: us[q] for q in range(5) if q < 4 or us[q] > 0}
 
     def window(self):
         """(window length in use, {candidate W: us per step} timed by the
