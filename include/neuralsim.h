@@ -347,6 +347,12 @@ ns_status ns_add_input_current(ns_handle* h, uint64_t count, const uint32_t* ids
 ns_status ns_upload_eligibility(ns_handle* h, const uint8_t* eligible, const float* values);
 /* Current eligibility values (m floats; 0 for synapses without a trace). */
 ns_status ns_download_eligibility(ns_handle* h, float* values_out);
+/* Per-synapse contribution averages of homeostatic scaling
+ * (SynapseState.contribution_avg, src/synapse/mod.rs:79, kept at delivery,
+ * engine.rs:448-452, :465-469), m floats in CSR order: for checkpoints.
+ * Download gives zeros without homeostasis; upload needs it enabled. */
+ns_status ns_download_contributions(ns_handle* h, float* values_out);
+ns_status ns_upload_contributions(ns_handle* h, const float* values);
 /* SimulationEngine::apply_reward (engine.rs:158-175): every eligible synapse
  * takes w = clamp(w + rstdp_lr*reward*e, rstdp_w_min, rstdp_w_max), e = 0,
  * now, whatever the size of reward. */

@@ -132,6 +132,8 @@ SIGNATURES = {
     "ns_add_input_current": (C.c_int32, [_P, C.c_uint64, C.c_void_p, C.c_void_p]),
     "ns_upload_eligibility": (C.c_int32, [_P, C.c_void_p, C.c_void_p]),
     "ns_download_eligibility": (C.c_int32, [_P, C.c_void_p]),
+    "ns_download_contributions": (C.c_int32, [_P, C.c_void_p]),
+    "ns_upload_contributions": (C.c_int32, [_P, C.c_void_p]),
     "ns_apply_reward": (C.c_int32, [_P, C.c_double]),
     "ns_get_reward": (C.c_int32, [_P, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "ns_set_reward": (C.c_int32, [_P, C.c_double]),

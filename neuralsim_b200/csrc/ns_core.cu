@@ -1323,8 +1323,10 @@ ns_status ns_create(const ns_config* cfg, ns_handle** out) {
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pick_ltd(c.weight_format, ext), 256, 0) != cudaSuccess || nb < 1) nb = 4;
     h->ltd_blocks = h->sms * nb;
     h->ltd_narrow_blocks = h->sms * 2;
-    h->flush_blocks = h->sms * 2;
-    h->drive_blocks = h->sms * 2;
+    nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pick_flush(c.weight_format), 256, 0) != cudaSuccess || nb < 1) nb = 4;
+    h->flush_blocks = h->sms * nb;
+    h->drive_blocks = h->sms * 4;
     nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ns::k_homeostasis<true>, 256, 0) != cudaSuccess || nb < 1) nb = 4;
     h->homeo_blocks = h->sms * nb;
@@ -2403,6 +2405,36 @@ ns_status ns_download_eligibility(ns_handle* h, float* values_out) {
     return NS_OK;
   }
   if (h->m) CK(copy_sync(h, values_out, h->d.elig, h->m * 4, cudaMemcpyDeviceToHost));
+  return NS_OK;
+}
+
+// Per-synapse contribution averages of homeostatic scaling
+// (SynapseState.contribution_avg, src/synapse/mod.rs:79; updated at delivery,
+// engine.rs:448-452, :465-469), CSR order, for checkpoints.
+ns_status ns_download_contributions(ns_handle* h, float* values_out) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  if (!values_out) return fail(h, NS_ERR_INVALID_ARG, "null output");
+  if (!h->have_csr) return fail(h, NS_ERR_STATE, "upload the CSR first");
+  CK(cudaSetDevice(h->dev));
+  CK(cudaStreamSynchronize(h->st));
+  if (!h->d.contrib) {
+    std::fill(values_out, values_out + h->m, 0.0f);
+    return NS_OK;
+  }
+  if (h->m) CK(copy_sync(h, values_out, h->d.contrib, h->m * 4, cudaMemcpyDeviceToHost));
+  return NS_OK;
+}
+
+ns_status ns_upload_contributions(ns_handle* h, const float* values) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  if (!values) return fail(h, NS_ERR_INVALID_ARG, "null values");
+  if (!h->have_csr || !h->have_neurons) return fail(h, NS_ERR_STATE, "upload the network first");
+  if (!h->d.contrib) return fail(h, NS_ERR_STATE, "homeostasis is not enabled in the config");
+  for (uint64_t q = 0; q < h->m; ++q)
+    if (!is_fin(values[q])) return fail(h, NS_ERR_NONFINITE, "non-finite contribution");
+  CK(cudaSetDevice(h->dev));
+  CK(cudaStreamSynchronize(h->st));
+  if (h->m) CK(copy_sync(h, h->d.contrib, values, h->m * 4, cudaMemcpyHostToDevice));
   return NS_OK;
 }
 

@@ -1183,15 +1183,16 @@ __device__ __forceinline__ void ltd_item(const NsDev& d, const StepCtx& c, uint3
 template <bool BF16>
 __device__ __forceinline__ void flush_row(const NsDev& d, uint64_t k, const float2* rec_k, uint32_t j,
                                           int lane) {
+  // the row's metadata in one round trip (independent loads)
   const uint8_t rp = __ldg(d.row_plastic + j);
-  if (!rp) return;
-  if (__float_as_uint(rec_k[j].x) & 1u) return;
+  const uint32_t hj = __float_as_uint(rec_k[j].x);
   const uint2 ls = d.lstart[j];
+  const uint64_t beg = __ldg(d.row_ptr + j), end = __ldg(d.row_ptr + j + 1);
+  if (!rp || (hj & 1u)) return;
   const uint32_t T = (uint32_t)k - ls.y;
   if (T == 0u) return;
   const uint32_t mask = pending_mask(T, 0u);
   const float ps = __uint_as_float(ls.x);
-  const uint64_t beg = __ldg(d.row_ptr + j), end = __ldg(d.row_ptr + j + 1);
   const uint64_t rb = beg & ~3ull;
   const uint32_t nrow = end > beg ? (uint32_t)((end - rb + 127) >> 7) : 0u;
   for (uint32_t ch = 0; ch < nrow; ++ch) {

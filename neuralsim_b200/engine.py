@@ -371,6 +371,44 @@ class SimulationEngine:
                 raise ValueError("eligibility arrays need one entry per synapse (m)")
         self._check(self.lib.ns_upload_eligibility(self._h, _ptr(el), _ptr(va)))
 
+    def contributions(self):
+        """Per-synapse contribution averages of homeostatic scaling (CSR
+        order; zeros without homeostasis)."""
+        c = np.zeros(max(self.network.m, 1), np.float32)
+        self._check(self.lib.ns_download_contributions(self._h, _ptr(c)))
+        return c[:self.network.m]
+
+    def upload_contributions(self, values):
+        va = np.ascontiguousarray(values, np.float32)
+        if va.size != self.network.m:
+            raise ValueError("contributions need one entry per synapse (m)")
+        self._check(self.lib.ns_upload_contributions(self._h, _ptr(va)))
+
+    def checkpoint(self):
+        """Everything a bit-exact resume needs: the device state and weights
+        (download_state), the step index, eligibility traces (R-STDP), the
+        contribution averages (homeostasis) and the reward."""
+        st = self.download_state()
+        st["step"] = self.current_step()
+        if self.config.rstdp_enabled:
+            st["eligibility"] = self.eligibility()
+            st["reward"] = self.reward_signal()
+        if self.config.homeostasis_enabled:
+            st["contributions"] = self.contributions()
+        return st
+
+    def restore(self, st: dict):
+        """Loads a checkpoint() (or a state read from a saved network):
+        state and weights at its step, then eligibility, contributions and
+        reward when present."""
+        self.upload_state(st, int(st.get("step", 0)))
+        if st.get("eligibility") is not None and self.config.rstdp_enabled:
+            self.upload_eligibility(st.get("eligible"), st["eligibility"])
+        if st.get("contributions") is not None and self.config.homeostasis_enabled:
+            self.upload_contributions(st["contributions"])
+        if st.get("reward") is not None and self.config.rstdp_enabled:
+            self.set_reward(float(st["reward"]))
+
     def apply_reward(self, reward: float):
         self._check(self.lib.ns_apply_reward(self._h, float(reward)))
 
