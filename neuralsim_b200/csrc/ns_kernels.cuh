@@ -985,15 +985,9 @@ __device__ __forceinline__ void row_item(const NsDev& d, const StepCtx& c, uint3
       }
     }
   }
-  // deferred LTD: the row's trace start and the pending-bit mask (steps
-  // astep+1 .. k-1; step k's LTD is the same-step one below, with pj)
-  float dps = 0.0f;
-  uint32_t dT = 0u, dmask = 0u;
-  if (DEFER && STDP && rp) {
-    dps = __uint_as_float(__shfl_sync(0xffffffffu, ls.x, 0));
-    dT = __shfl_sync(0xffffffffu, (uint32_t)k - ls.y, 0);
-    dmask = pending_mask(dT, 1u);
-  }
+  // deferred LTD: lane 0 holds the row's trace start; it is broadcast in
+  // the chunk loop after the chunk's loads and gathers are issued, so that
+  // they do not wait for lane 0's loads
   const unsigned long long tbase = d.trace_pos ? d.trace_off[item] : 0ull;
   const uint64_t rb = beg & ~3ull;
   const uint32_t nrow = end > beg ? (uint32_t)((end - rb + 127) >> 7) : 0u;
@@ -1025,12 +1019,21 @@ __device__ __forceinline__ void row_item(const NsDev& d, const StepCtx& c, uint3
       if (DEFER) {
         const float2 r = pl[q] ? c.rec_k[cc[q]] : make_float2(0.f, 0.f);
         tq[q] = r.y;
-        pb[q] = __float_as_uint(r.x) & dmask;
+        pb[q] = __float_as_uint(r.x);
       } else {
         tq[q] = pl[q] ? c.rec_k[cc[q]].y : 0.f;
       }
     }
-    if (DEFER) apply_pending<BF16>(d, dps, dT, pb, w);
+    if (DEFER && STDP && rp) {
+      // the row's pending-bit mask: steps astep+1 .. k-1 (step k's LTD is
+      // the same-step one below, with pj)
+      const float dps = __uint_as_float(__shfl_sync(0xffffffffu, ls.x, 0));
+      const uint32_t dT = __shfl_sync(0xffffffffu, (uint32_t)k - ls.y, 0);
+      const uint32_t dmask = pending_mask(dT, 1u);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) pb[q] &= dmask;
+      apply_pending<BF16>(d, dps, dT, pb, w);
+    }
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       if (!inr[q]) continue;

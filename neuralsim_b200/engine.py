@@ -392,7 +392,7 @@ class SimulationEngine:
         st["step"] = self.current_step()
         if self.config.rstdp_enabled:
             st["eligibility"] = self.eligibility()
-            st["reward"] = self.reward_signal()
+            st["reward"] = self.reward_signal
         if self.config.homeostasis_enabled:
             st["contributions"] = self.contributions()
         return st
