@@ -906,25 +906,41 @@ __device__ __forceinline__ float ext_store(const NsDev& d, const float* fr, uint
   return d.cons ? (w1 - fr[1]) * fr[2] : w1;
 }
 
-// Deferred LTD of one lane's four synapses of source j: pb[q] holds, for
-// synapse q, the bits (b = steps before the current one) of its target's
-// spikes whose LTD has not been applied; T = current step - astep, ps the
-// source's pre trace after step astep. The source's pre trace at step
-// astep + t is ps times exp(-dt/tau+) t times, one float rounding per
-// multiply: the chain the neuron kernel runs. Each LTD is the eager one,
-// w = clamp(w - A- pre), stored (BF16: rounded) before the next, in step order.
+// Deferred LTD. The source's pre trace at step astep + t is its value ps
+// after step astep times exp(-dt/tau+) t times, one float rounding per
+// multiply: the chain the neuron kernel runs. chain_fill computes it once per
+// row, converged across the warp: lane i keeps x_(i+1) in the warp's table
+// in shared memory (t = 1 .. min(T, 32)); returns x_min(T, 32).
+__device__ __forceinline__ float* warp_chain_table() {
+  __shared__ float s_chain[8][32];   // 256-thread blocks: one row of 32 per warp
+  return s_chain[threadIdx.x >> 5];
+}
+
+__device__ __forceinline__ float chain_fill(const NsDev& d, float ps, uint32_t T, int lane, float* xs) {
+  __syncwarp();
+  const uint32_t Tc = T < 32u ? T : 32u;
+  float x = ps, mine = 0.0f;
+  for (uint32_t i = 0; i < Tc; ++i) {
+    x = x * d.ep;
+    if ((uint32_t)lane == i) mine = x;
+  }
+  xs[lane] = mine;
+  __syncwarp();
+  return x;
+}
+
+// The pending LTDs of one lane's four synapses: pb[q] holds, for synapse q,
+// the bits (b = steps before the current one) of its target's spikes whose
+// LTD has not been applied; T = current step - astep, xs the row's chain
+// table. Each LTD is the eager one, w = clamp(w - A- pre), stored (BF16:
+// rounded) before the next, in step order (highest bit first).
 template <bool BF16>
-__device__ __forceinline__ void apply_pending(const NsDev& d, float ps, uint32_t T, const uint32_t pb[4],
-                                              float w[4]) {
+__device__ __forceinline__ void apply_pending(const NsDev& d, const float* xs, uint32_t T,
+                                              const uint32_t pb[4], float w[4]) {
   uint32_t U = pb[0] | pb[1] | pb[2] | pb[3];
-  if (!U) return;
-  float x = ps;
-  uint32_t t = 0;
-  do {
-    const uint32_t b = 31u - __clz(U);   // earliest pending step: k - b = astep + (T - b)
-    const uint32_t tt = T - b;
-    while (t < tt) { x = x * d.ep; ++t; }
-    const float dm = d.neg_a_minus * x;
+  while (U) {
+    const uint32_t b = 31u - __clz(U);   // step k - b = astep + (T - b)
+    const float dm = d.neg_a_minus * xs[T - b - 1u];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       if ((pb[q] >> b) & 1u) {
@@ -934,7 +950,7 @@ __device__ __forceinline__ void apply_pending(const NsDev& d, float ps, uint32_t
       }
     }
     U &= ~(1u << b);
-  } while (U);
+  }
 }
 
 // Bits b in [lo, T-1] of a 32-step spike history (T >= 32: all from lo).
@@ -1026,13 +1042,14 @@ __device__ __forceinline__ void row_item(const NsDev& d, const StepCtx& c, uint3
     }
     if (DEFER && STDP && rp) {
       // the row's pending-bit mask: steps astep+1 .. k-1 (step k's LTD is
-      // the same-step one below, with pj)
-      const float dps = __uint_as_float(__shfl_sync(0xffffffffu, ls.x, 0));
+      // the same-step one below, with pj); the chain table once per row
       const uint32_t dT = __shfl_sync(0xffffffffu, (uint32_t)k - ls.y, 0);
+      float* xs = warp_chain_table();
+      if (ch == 0) chain_fill(d, __uint_as_float(__shfl_sync(0xffffffffu, ls.x, 0)), dT, lane, xs);
       const uint32_t dmask = pending_mask(dT, 1u);
 #pragma unroll
       for (int q = 0; q < 4; ++q) pb[q] &= dmask;
-      apply_pending<BF16>(d, dps, dT, pb, w);
+      apply_pending<BF16>(d, xs, dT, pb, w);
     }
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
@@ -1195,7 +1212,9 @@ __device__ __forceinline__ void flush_row(const NsDev& d, uint64_t k, const floa
   const uint32_t T = (uint32_t)k - ls.y;
   if (T == 0u) return;
   const uint32_t mask = pending_mask(T, 0u);
-  const float ps = __uint_as_float(ls.x);
+  // the chain table; xT, the pre trace at step k, is the row's new start
+  float* xs = warp_chain_table();
+  const float xT = chain_fill(d, __uint_as_float(ls.x), T, lane, xs);
   const uint64_t rb = beg & ~3ull;
   const uint32_t nrow = end > beg ? (uint32_t)((end - rb + 127) >> 7) : 0u;
   for (uint32_t ch = 0; ch < nrow; ++ch) {
@@ -1215,7 +1234,7 @@ __device__ __forceinline__ void flush_row(const NsDev& d, uint64_t k, const floa
     if (!(pb[0] | pb[1] | pb[2] | pb[3])) continue;
     float w[4];
     load_w4(d, BF16, e0, w);
-    apply_pending<BF16>(d, ps, T, pb, w);
+    apply_pending<BF16>(d, xs, T, pb, w);
     if (BF16) {
       if (all4) {
         uint2 raw;
@@ -1237,12 +1256,7 @@ __device__ __forceinline__ void flush_row(const NsDev& d, uint64_t k, const floa
       }
     }
   }
-  if (lane == 0) {
-    // the pre trace at step k: the neuron kernel's decay chain from astep
-    float x = ps;
-    for (uint32_t t = 0; t < T; ++t) x = x * d.ep;
-    d.lstart[j] = make_uint2(__float_as_uint(x), (uint32_t)k);
-  }
+  if (lane == 0) d.lstart[j] = make_uint2(__float_as_uint(xT), (uint32_t)k);
 }
 
 // Deferred LTD, step k: the flush of row block k mod 32 (rows
