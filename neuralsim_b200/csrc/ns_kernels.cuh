@@ -979,26 +979,38 @@ __device__ __forceinline__ void row_item(const NsDev& d, const StepCtx& c, uint3
   float pj = 0.0f;
   uint2 ls = make_uint2(0u, 0u);
   if (lane == 0) {
+    // every load of the spike's bookkeeping is issued before any of its
+    // stores: the compiler cannot move a load past a store through another
+    // pointer, and a store-load order here costs a memory round trip each
     const long long lst = d.last[j];
+    const uint8_t isout = d.outp[j];
+    float2 rj = make_float2(0.f, 0.f);
+    float pdec = 0.f;
+    if (STDP) {
+      rj = c.rec_k[j];
+      if (DEFER) {
+        pdec = d.pre[j];
+        ls = d.lstart[j];
+      }
+    }
+    const long long dk = lst < 0 ? -1 : (long long)k - lst;
+    float fp = 0.f, fm = 0.f;
+    if (STDP) {
+      fp = (dk >= 0 && (unsigned long long)dk < d.Kp) ? d.Ep[dk] : 0.0f;
+      fm = (dk >= 0 && (unsigned long long)dk < d.Km) ? d.Em[dk] : 0.0f;
+    }
     if (c.log_ok) d.log_idx[c.log_base + item] = j;
     ev += end - beg;
-    outs += d.outp[j] ? 1u : 0u;
+    outs += isout ? 1u : 0u;
     d.last[j] = (long long)k;
     if (STDP) {
-      // spike-time trace bump: trace * exp(-(t - t_last)/tau) + 1
-      const float2 rj = c.rec_k[j];
-      const long long dk = lst < 0 ? -1 : (long long)k - lst;
-      const float fp = (dk >= 0 && (unsigned long long)dk < d.Kp) ? d.Ep[dk] : 0.0f;
-      const float fm = (dk >= 0 && (unsigned long long)dk < d.Km) ? d.Em[dk] : 0.0f;
-      // the decayed pre trace: the record's |x| (eager), or the trace the
+      // spike-time trace bump: trace * exp(-(t - t_last)/tau) + 1; the
+      // decayed pre trace is the record's |x| (eager) or the trace the
       // neuron kernel wrote this step (deferred: the record holds spike bits)
-      pj = (DEFER ? d.pre[j] : fabsf(rj.x)) * fp + 1.0f;
+      pj = (DEFER ? pdec : fabsf(rj.x)) * fp + 1.0f;
       d.pre[j] = pj;
       d.post[j] = fabsf(rj.y) * fm + 1.0f;
-      if (DEFER) {
-        ls = d.lstart[j];
-        d.lstart[j] = make_uint2(__float_as_uint(pj), (uint32_t)k);
-      }
+      if (DEFER) d.lstart[j] = make_uint2(__float_as_uint(pj), (uint32_t)k);
     }
   }
   // deferred LTD: lane 0 holds the row's trace start; it is broadcast in
