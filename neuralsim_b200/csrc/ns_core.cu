@@ -603,6 +603,17 @@ neuron_fn pick_neuron(uint32_t model, uint32_t mode, bool pt, bool stim = false)
   return nullptr;
 }
 
+// Launches neuron kernel nf for graph-node step j on stream s. Its inputs are
+// staged in shared memory by bulk copies (two sub-tile buffers per block)
+// when a buffer fits in kStageMaxBytes, else loaded directly.
+void launch_neuron_kernel(ns_handle* h, neuron_fn nf, NsDev x, uint32_t j, cudaStream_t s) {
+  const ns::StagePlan sp = ns::stage_plan((int)h->cfg.model, (int)h->cfg.input_mode, x.pidx != nullptr,
+                                          x.stdp, x.defer, x.drive_kind, x.type_mask);
+  const bool stg = sp.bytes <= ns::kStageMaxBytes;
+  x.stage = stg ? 1 : 0;
+  nf<<<h->d.tiles_own, ns::kThreads, stg ? 2u * sp.bytes : 0u, s>>>(x, j);
+}
+
 // EXT variants carry R-STDP eligibility, the consolidation frame and STP
 prop_fn pick_prop(uint32_t mode, uint32_t wf, bool ext) {
   bool cond = mode == NS_INPUT_CONDUCTANCE_REF || mode == NS_INPUT_CONDUCTANCE_FRESH;
@@ -789,7 +800,7 @@ cudaError_t enqueue_step(ns_handle* h, uint32_t j, bool* ltd_pending, uint32_t s
     *drv_pending = false;
   }
   auto launch_neuron = [&](const NsDev& x) -> cudaError_t {
-    nf<<<h->d.tiles_own, ns::kThreads, 0, h->st>>>(x, j);
+    launch_neuron_kernel(h, nf, x, j, h->st);
     if (drv != kDriveNext) return cudaSuccess;
     // the next step's drive beside this step's walks
     cudaError_t r = cudaEventRecord(h->ev_nrn, h->st);
@@ -1327,6 +1338,13 @@ ns_status ns_create(const ns_config* cfg, ns_handle** out) {
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pick_flush(c.weight_format), 256, 0) != cudaSuccess || nb < 1) nb = 4;
     h->flush_blocks = h->sms * nb;
     h->drive_blocks = h->sms * 4;
+    // the neuron kernels may stage two sub-tile buffers in shared memory
+    for (uint32_t mo = 0; mo < 3; ++mo)
+      for (uint32_t md = 0; md < 5; ++md)
+        for (int pt = 0; pt < 2; ++pt)
+          for (int sm = 0; sm < 2; ++sm)
+            cudaFuncSetAttribute(pick_neuron(mo, md, pt != 0, sm != 0),
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * (int)ns::kStageMaxBytes);
     nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ns::k_homeostasis<true>, 256, 0) != cudaSuccess || nb < 1) nb = 4;
     h->homeo_blocks = h->sms * nb;
@@ -2069,6 +2087,8 @@ ns_status ns_step(ns_handle* h, uint32_t n_steps, ns_step_stats* out) {
     out->max_step_spikes = after.max_step_spikes;
     out->sim_time_ms = after.sim_time;
   }
+  if ((after.status & ns::kErrStageWait) && !(before.status & ns::kErrStageWait))
+    return fail(h, NS_ERR_DEVICE_TIMEOUT, "a neuron kernel's staged loads did not arrive in time");
   if ((after.status & ns::kErrLogFull) && !(before.status & ns::kErrLogFull))
     return fail(h, NS_ERR_SPIKE_LOG_FULL, "spike log capacity exceeded; later steps not logged");
   return NS_OK;
@@ -2098,7 +2118,7 @@ ns_status ns_step_traced(ns_handle* h, uint64_t* pos_out, uint64_t cap, uint64_t
   h->stim_step = false;
   const bool ext = ext_on(h);
   prop_fn pf = pick_prop(h->cfg.input_mode, h->cfg.weight_format, ext);
-  nf<<<h->d.tiles_own, ns::kThreads, 0, h->st>>>(d, 0);
+  launch_neuron_kernel(h, nf, d, 0, h->st);
   if (tail_on(h)) ns::k_setup<<<1, 32, 0, h->st>>>(d, 0);
   ns::k_trace_offsets<<<1, 32, 0, h->st>>>(d, off);
   d.trace_pos = pos; d.trace_off = off; d.trace_cap = cap;
@@ -2679,7 +2699,7 @@ ns_status ns_profile_steps(ns_handle* h, uint32_t n_steps, double* kernel_ms, ui
     if (pre) ns::k_drive<<<h->drive_blocks, 256, 0, h->st>>>(dd, j);
     CK(cudaEventRecord(e[9], h->st));
     CK(cudaEventRecord(e[0], h->st));
-    (j == 0 ? nf0 : nf)<<<h->d.tiles_own, ns::kThreads, 0, h->st>>>(dd, j);
+    launch_neuron_kernel(h, j == 0 ? nf0 : nf, dd, j, h->st);
     if (tail_on(h)) ns::k_setup<<<1, 32, 0, h->st>>>(h->d, j);
     CK(cudaEventRecord(e[1], h->st));
     CK(cudaEventRecord(e[2], h->st));
@@ -2832,7 +2852,7 @@ ns_status ns_shard_step_begin(ns_handle* h) {
   neuron_fn nf = pick_neuron(h->cfg.model, h->cfg.input_mode, h->d.pidx != nullptr, h->stim_step);
   h->stim_step = false;
   const NsDev dd = with_drive(h, h->d, 0);
-  nf<<<h->d.tiles_own, ns::kThreads, 0, h->st>>>(dd, 0);
+  launch_neuron_kernel(h, nf, dd, 0, h->st);
   h->launches += 1;
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(h->st));

@@ -17,6 +17,7 @@
 #include <cstdint>
 #include "ns_device.cuh"
 #include "ns_hh.cuh"
+#include "ns_tc.cuh"
 
 namespace ns {
 
@@ -29,6 +30,7 @@ constexpr uint32_t kSmemTiles = 4096;       // tile offsets kept in shared memor
 
 // device status bits (host maps them to ns_status)
 constexpr uint32_t kErrLogFull = 2u;
+constexpr uint32_t kErrStageWait = 4u;   // a neuron kernel's staged loads did not arrive
 
 struct Ctl {
   unsigned long long step_base;   // global step of graph node 0
@@ -179,7 +181,77 @@ struct NsDev {
   // amount drive_of gives neuron i at step k (the neuron kernel draws the
   // reference-uniform kind itself)
   float* drv;
+  // the neuron kernel stages its sub-tiles' input arrays in shared memory
+  // with bulk copies (stage_plan); 0: direct loads
+  int stage;
 };
+
+// ---------------------------------------------------------------------------
+// Staged loads of the neuron kernel. A tile of 2048 neurons is updated in four
+// sub-tiles of 512 (one neuron pair per thread); every input array's 512
+// entries of a sub-tile are brought into shared memory by one bulk copy
+// (cp.async.bulk, completion counted in bytes on an mbarrier), two
+// sub-tiles in flight at a time. stage_plan gives each array's byte offset in
+// a sub-tile buffer (kNoStage: not read) and the buffer's size; host and
+// device compute it from the same fields.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kStageSub = 512;                 // neurons per sub-tile
+constexpr uint32_t kNoStage = 0xffffffffu;
+constexpr uint32_t kStageMaxBytes = 32u * 1024u;    // per buffer (two per block)
+
+struct StagePlan {
+  uint32_t v, u, refr, gm, gh, gn, I, par[7], rsteps, pidx, acc[4], G[4], pre, post, rec, drv;
+  uint32_t bytes;
+};
+
+__host__ __device__ __forceinline__ StagePlan stage_plan(int model, int mode, bool pt, int stdp,
+                                                         int defer, int drive_kind,
+                                                         uint32_t type_mask) {
+  StagePlan p;
+  uint32_t off = 0;
+  auto take = [&](bool on, uint32_t esz) -> uint32_t {
+    if (!on) return kNoStage;
+    const uint32_t at = off;
+    off += kStageSub * esz;
+    return at;
+  };
+  const bool cond = mode == 3 || mode == 4;
+  const int np = model == 0 ? 5 : (model == 1 ? 4 : 7);
+  p.v = take(true, 4);
+  p.u = take(model == 1, 4);
+  p.refr = take(model == 0, 4);
+  p.gm = take(model == 2, 4);
+  p.gh = take(model == 2, 4);
+  p.gn = take(model == 2, 4);
+  p.I = take(mode == 0 || mode == 3, 4);
+  for (int q = 0; q < 7; ++q) p.par[q] = take(!pt && q < np, 4);
+  p.rsteps = take(!pt && model == 0, 4);
+  p.pidx = take(pt, 1);
+  for (int t = 0; t < 4; ++t) p.acc[t] = take(cond ? ((type_mask >> t) & 1u) != 0u : t == 0, 8);
+  for (int t = 0; t < 4; ++t) p.G[t] = take(cond, 4);
+  p.pre = take(stdp != 0, 4);
+  p.post = take(stdp != 0, 4);
+  p.rec = take(stdp != 0 && defer != 0, 8);
+  p.drv = take(drive_kind >= 2, 4);
+  p.bytes = off;
+  return p;
+}
+
+// Thread 0 enqueues the bulk copies of sub-tile `sub` of the block's tile
+// (first neuron `first`) into buffer `buf`, completing on `mbar`.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* mbar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          tc::smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(tc::smem_u32(mbar))
+      : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc::smem_u32(mbar)),
+               "r"(bytes)
+               : "memory");
+}
 
 __device__ __forceinline__ bool bit_of(const uint32_t* bm, uint32_t i) {
   return (bm[i >> 5] >> (i & 31)) & 1u;
@@ -501,6 +573,8 @@ __global__ void k_setup(NsDev d, uint32_t jstep) {
 // one step; the others carry no stimulus code).
 template <int MODEL, int MODE, bool PT, bool STIM>
 __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
+  extern __shared__ __align__(128) uint8_t s_stage[];   // two sub-tile buffers when staged
+  __shared__ __align__(8) uint64_t s_mbar[2];
   __shared__ float s_tab[PT ? 256 * 8 : 1];
   __shared__ uint32_t s_off[kPairs * kWarps];
   __shared__ uint32_t s_me[kPairs * kWarps], s_mo[kPairs * kWarps];
@@ -556,35 +630,100 @@ __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
   const uint64_t base = (uint64_t)tile * kTile;
   const int nk = s_nk;
 
+  // ---- staged loads: plan, barriers, the first two sub-tiles in flight ----
+  const bool stg = d.stage != 0;
+  const StagePlan sp = stage_plan(MODEL, MODE, PT, d.stdp, d.defer, d.drive_kind, d.type_mask);
+  const uint32_t prev_k = par_k ^ 1u;
+  auto issue = [&](int sub) {
+    uint8_t* buf = s_stage + (uint32_t)(sub & 1) * sp.bytes;
+    uint64_t* mb = &s_mbar[sub & 1];
+    const uint64_t f = base + (uint64_t)sub * kStageSub;
+    tc::fence_proxy_async();
+    mbar_expect_tx(mb, sp.bytes);
+    auto cp = [&](uint32_t off, const void* src, uint32_t esz) {
+      if (off != kNoStage)
+        bulk_g2s(buf + off, reinterpret_cast<const uint8_t*>(src) + f * esz, kStageSub * esz, mb);
+    };
+    cp(sp.v, d.v, 4);
+    cp(sp.u, d.u, 4);
+    cp(sp.refr, d.refr, 4);
+    cp(sp.gm, d.gm, 4);
+    cp(sp.gh, d.gh, 4);
+    cp(sp.gn, d.gn, 4);
+    cp(sp.I, d.I, 4);
+#pragma unroll
+    for (int q = 0; q < 7; ++q) cp(sp.par[q], d.par[q], 4);
+    cp(sp.rsteps, d.refr_steps, 4);
+    cp(sp.pidx, d.pidx, 1);
+#pragma unroll
+    for (int t = 0; t < 4; ++t) cp(sp.acc[t], d.acc + ((uint64_t)t * d.D + slot) * d.n_pad, 8);
+#pragma unroll
+    for (int t = 0; t < 4; ++t) cp(sp.G[t], d.G[t], 4);
+    cp(sp.pre, d.pre, 4);
+    cp(sp.post, d.post, 4);
+    cp(sp.rec, d.rec + prev_k * d.n_pad, 8);
+    cp(sp.drv, d.drv + par_k * d.n_pad, 4);
+  };
+  if (stg) {
+    if (tid == 0) {
+      tc::mbar_init(&s_mbar[0], 1);
+      tc::mbar_init(&s_mbar[1], 1);
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (tid == 0) {
+      issue(0);
+      issue(1);
+    }
+  }
+
 #pragma unroll 1
   for (int r = 0; r < kPairs; ++r) {
     const uint64_t i0 = base + (uint64_t)r * 512 + 2 * (uint64_t)tid;
-    // ---- every load of the pair ----
+    // ---- the pair's inputs: from the staged sub-tile, or loaded here ----
+    const uint8_t* sb = s_stage + (uint32_t)(r & 1) * sp.bytes;
+    if (stg) {
+      bool ok = tc::mbar_wait(&s_mbar[r & 1], (uint32_t)(r >> 1) & 1u, 1u << 22);
+      if (!__syncthreads_and(ok)) {
+        // the copies did not arrive: record it, give the ones in flight a
+        // bounded time to land, and leave the tile (the step is reported)
+        if (tid == 0) {
+          atomicOr(&d.ctl->status, kErrStageWait);
+          tc::mbar_wait(&s_mbar[0], 1u, 1u << 22);
+          tc::mbar_wait(&s_mbar[1], 1u, 1u << 22);
+        }
+        __syncthreads();
+        return;
+      }
+    }
+#define NS_LD(T, off, gptr, esz) \
+    (stg ? *reinterpret_cast<const T*>(sb + (off) + (esz) * 2u * (uint32_t)tid) \
+         : *reinterpret_cast<const T*>(gptr))
     NState st[2];
-    const float2 v2 = *reinterpret_cast<const float2*>(d.v + i0);
+    const float2 v2 = NS_LD(float2, sp.v, d.v + i0, 4u);
     st[0].v = v2.x; st[1].v = v2.y;
     if (MODEL == 1) {
-      const float2 u2 = *reinterpret_cast<const float2*>(d.u + i0);
+      const float2 u2 = NS_LD(float2, sp.u, d.u + i0, 4u);
       st[0].u = u2.x; st[1].u = u2.y;
     }
     if (MODEL == 0) {
-      const int2 r2 = *reinterpret_cast<const int2*>(d.refr + i0);
+      const int2 r2 = NS_LD(int2, sp.refr, d.refr + i0, 4u);
       st[0].refr = r2.x; st[1].refr = r2.y;
     }
     if (MODEL == 2) {
-      const float2 a = *reinterpret_cast<const float2*>(d.gm + i0);
-      const float2 b = *reinterpret_cast<const float2*>(d.gh + i0);
-      const float2 c = *reinterpret_cast<const float2*>(d.gn + i0);
+      const float2 a = NS_LD(float2, sp.gm, d.gm + i0, 4u);
+      const float2 b = NS_LD(float2, sp.gh, d.gh + i0, 4u);
+      const float2 c = NS_LD(float2, sp.gn, d.gn + i0, 4u);
       st[0].m = a.x; st[1].m = a.y; st[0].h = b.x; st[1].h = b.y; st[0].n = c.x; st[1].n = c.y;
     }
     if (MODE == 0 || MODE == 3) {
-      const float2 c = *reinterpret_cast<const float2*>(d.I + i0);
+      const float2 c = NS_LD(float2, sp.I, d.I + i0, 4u);
       st[0].I = c.x; st[1].I = c.y;
     }
     float par[2][7];
     int rs[2] = {0, 0};
     if (PT) {
-      const uchar2 ix = *reinterpret_cast<const uchar2*>(d.pidx + i0);
+      const uchar2 ix = NS_LD(uchar2, sp.pidx, d.pidx + i0, 1u);
       const float* t0 = s_tab + 8u * ix.x;
       const float* t1 = s_tab + 8u * ix.y;
 #pragma unroll
@@ -593,11 +732,11 @@ __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
     } else {
 #pragma unroll
       for (int q = 0; q < NP; ++q) {
-        const float2 pv = *reinterpret_cast<const float2*>(d.par[q] + i0);
+        const float2 pv = NS_LD(float2, sp.par[q], d.par[q] + i0, 4u);
         par[0][q] = pv.x; par[1][q] = pv.y;
       }
       if (MODEL == 0) {
-        const int2 r2 = *reinterpret_cast<const int2*>(d.refr_steps + i0);
+        const int2 r2 = NS_LD(int2, sp.rsteps, d.refr_steps + i0, 4u);
         rs[0] = r2.x; rs[1] = r2.y;
       }
     }
@@ -605,29 +744,35 @@ __global__ void __launch_bounds__(kThreads) k_neuron(NsDev d, uint32_t jstep) {
 #pragma unroll
     for (int t = 0; t < NT; ++t)
       accv[t] = (!COND || ((d.type_mask >> t) & 1u))
-                    ? *reinterpret_cast<const longlong2*>(d.acc + ((uint64_t)t * d.D + slot) * d.n_pad + i0)
+                    ? NS_LD(longlong2, sp.acc[t], d.acc + ((uint64_t)t * d.D + slot) * d.n_pad + i0, 8u)
                     : make_longlong2(0, 0);
     float G[4][2];
     if (COND) {
 #pragma unroll
       for (int t = 0; t < 4; ++t) {
-        const float2 g2 = *reinterpret_cast<const float2*>(d.G[t] + i0);
+        const float2 g2 = NS_LD(float2, sp.G[t], d.G[t] + i0, 4u);
         G[t][0] = g2.x; G[t][1] = g2.y;
       }
     }
     float2 p2 = make_float2(0.f, 0.f), q2 = make_float2(0.f, 0.f);
     uint2 hist = make_uint2(0u, 0u);
     if (d.stdp) {
-      p2 = *reinterpret_cast<const float2*>(d.pre + i0);
-      q2 = *reinterpret_cast<const float2*>(d.post + i0);
+      p2 = NS_LD(float2, sp.pre, d.pre + i0, 4u);
+      q2 = NS_LD(float2, sp.post, d.post + i0, 4u);
       if (d.defer) {
         // spike bits of the previous step's records (the other parity)
-        const float4 pr = *reinterpret_cast<const float4*>(d.rec + (par_k ^ 1u) * d.n_pad + i0);
+        const float4 pr = NS_LD(float4, sp.rec, d.rec + prev_k * d.n_pad + i0, 8u);
         hist = make_uint2(__float_as_uint(pr.x), __float_as_uint(pr.z));
       }
     }
     float2 pdrv = make_float2(0.f, 0.f);
-    if (d.drive_kind >= 2) pdrv = *reinterpret_cast<const float2*>(d.drv + par_k * d.n_pad + i0);
+    if (d.drive_kind >= 2) pdrv = NS_LD(float2, sp.drv, d.drv + par_k * d.n_pad + i0, 4u);
+#undef NS_LD
+    if (stg) {
+      // every thread has its pair's inputs: the buffer takes sub-tile r + 2
+      __syncthreads();
+      if (tid == 0 && r + 2 < kPairs) issue(r + 2);
+    }
     // ---- delivered synaptic input for this step (the slot is cleared) ----
     if (d.inbits && lane == 0) {
       uint32_t* ib = d.inbits + (uint64_t)slot * (d.n_pad >> 5) + ((i0 - 2 * (uint64_t)lane) >> 5);
