@@ -2087,6 +2087,8 @@ ns_status ns_step(ns_handle* h, uint32_t n_steps, ns_step_stats* out) {
     out->max_step_spikes = after.max_step_spikes;
     out->sim_time_ms = after.sim_time;
   }
+  if ((after.status & ns::kErrDeferWindow) && !(before.status & ns::kErrDeferWindow))
+    return fail(h, NS_ERR_STATE, "a deferred-LTD row went more than 32 steps without a walk or flush");
   if ((after.status & ns::kErrStageWait) && !(before.status & ns::kErrStageWait))
     return fail(h, NS_ERR_DEVICE_TIMEOUT, "a neuron kernel's staged loads did not arrive in time");
   if ((after.status & ns::kErrLogFull) && !(before.status & ns::kErrLogFull))

@@ -31,6 +31,7 @@ constexpr uint32_t kSmemTiles = 4096;       // tile offsets kept in shared memor
 // device status bits (host maps them to ns_status)
 constexpr uint32_t kErrLogFull = 2u;
 constexpr uint32_t kErrStageWait = 4u;   // a neuron kernel's staged loads did not arrive
+constexpr uint32_t kErrDeferWindow = 8u; // a deferred-LTD row went more than 32 steps unflushed
 
 struct Ctl {
   unsigned long long step_base;   // global step of graph node 0
@@ -1098,8 +1099,15 @@ __device__ __forceinline__ void apply_pending(const NsDev& d, const float* xs, u
   }
 }
 
-// Bits b in [lo, T-1] of a 32-step spike history (T >= 32: all from lo).
+// Bits b in [lo, T-1] of a 32-step spike history whose chain index T - b - 1
+// lies in the 32-entry table (b >= T - 32). T never exceeds 32 when every
+// row is flushed every 32 steps; should it, the older bits are dropped here
+// and the walk records kErrDeferWindow.
 __device__ __forceinline__ uint32_t pending_mask(uint32_t T, uint32_t lo) {
+  if (T > 32u) {
+    if (T >= 64u) return 0u;
+    lo = lo > T - 32u ? lo : T - 32u;
+  }
   const uint32_t m = T >= 32u ? 0xffffffffu : ((1u << T) - 1u);
   return m & ~((1u << lo) - 1u);
 }
@@ -1201,6 +1209,7 @@ __device__ __forceinline__ void row_item(const NsDev& d, const StepCtx& c, uint3
       // the row's pending-bit mask: steps astep+1 .. k-1 (step k's LTD is
       // the same-step one below, with pj); the chain table once per row
       const uint32_t dT = __shfl_sync(0xffffffffu, (uint32_t)k - ls.y, 0);
+      if (dT > 32u && ch == 0 && lane == 0) atomicOr(&d.ctl->status, kErrDeferWindow);
       float* xs = warp_chain_table();
       if (ch == 0) chain_fill(d, __uint_as_float(__shfl_sync(0xffffffffu, ls.x, 0)), dT, lane, xs);
       const uint32_t dmask = pending_mask(dT, 1u);
@@ -1368,6 +1377,7 @@ __device__ __forceinline__ void flush_row(const NsDev& d, uint64_t k, const floa
   if (!rp || (hj & 1u)) return;
   const uint32_t T = (uint32_t)k - ls.y;
   if (T == 0u) return;
+  if (T > 32u && lane == 0) atomicOr(&d.ctl->status, kErrDeferWindow);
   const uint32_t mask = pending_mask(T, 0u);
   // the chain table; xT, the pre trace at step k, is the row's new start
   float* xs = warp_chain_table();
