@@ -1427,20 +1427,109 @@ __device__ __forceinline__ void flush_row(const NsDev& d, uint64_t k, const floa
 }
 
 // Deferred LTD, step k: the flush of row block k mod 32 (rows
-// [b * ceil(n/32), (b+1) * ceil(n/32))), one warp per row. Runs beside the
-// row walks of step k (the rows of step k's spikers are skipped) and the
-// neuron update of step k+1; the row walks of step k+1 wait for it.
+// [b * ceil(n/32), (b+1) * ceil(n/32))). Runs beside the row walks of step k
+// (the rows of step k's spikers are skipped) and the neuron update of step
+// k+1; the row walks of step k+1 wait for it.
+//
+// A block takes tasks of kFlushRows consecutive rows. First one thread per
+// row reads the row's metadata, computes its pre-trace chain table into
+// shared memory and moves its trace start to step k; then the block streams
+// the task's contiguous CSR range, four positions per thread (coalesced
+// column and weight loads), each position finding its row in the task's row
+// pointers, gathering its target's spike bits and applying the pending LTDs
+// with its row's table. Only changed weights are written, so a 4-entry group
+// at a task's edge or over a spiking row touches nothing it does not own.
+constexpr uint32_t kFlushRows = 32;
+
 template <bool BF16>
 __global__ void __launch_bounds__(256) k_flush(NsDev d, uint32_t jstep) {
+  __shared__ float s_tab[kFlushRows][33];
+  __shared__ uint64_t s_beg[kFlushRows + 1];
+  __shared__ uint32_t s_T[kFlushRows], s_mask[kFlushRows];
+  __shared__ uint8_t s_rp[kFlushRows];
   const uint64_t k = d.ctl->step_base + jstep;
   const float2* rec_k = d.rec + (k & 1) * d.n_pad;
   const uint64_t per = (d.n + 31) / 32;
   const uint64_t r0 = (k & 31u) * per;
   const uint64_t r1 = r0 + per < d.n ? r0 + per : d.n;
-  const int lane = threadIdx.x & 31;
-  const uint64_t nw = (uint64_t)gridDim.x * (blockDim.x >> 5);
-  for (uint64_t j = r0 + blockIdx.x * (uint64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); j < r1; j += nw)
-    flush_row<BF16>(d, k, rec_k, (uint32_t)j, lane);
+  const uint32_t tid = threadIdx.x;
+  const uint64_t ntask = r1 > r0 ? (r1 - r0 + kFlushRows - 1) / kFlushRows : 0;
+  for (uint64_t task = blockIdx.x; task < ntask; task += gridDim.x) {
+    const uint64_t ja = r0 + task * kFlushRows;
+    const uint32_t nrows = (uint32_t)(ja + kFlushRows <= r1 ? kFlushRows : r1 - ja);
+    // ---- phase 1: one thread per row ----
+    uint32_t live = 0u;
+    if (tid < nrows) {
+      const uint64_t j = ja + tid;
+      const uint8_t rp = __ldg(d.row_plastic + j);
+      const uint32_t hj = __float_as_uint(rec_k[j].x);
+      const uint2 ls = d.lstart[j];
+      s_beg[tid] = __ldg(d.row_ptr + j);
+      uint32_t T = (rp && !(hj & 1u)) ? (uint32_t)k - ls.y : 0u;
+      if (T > 32u) atomicOr(&d.ctl->status, kErrDeferWindow);
+      s_T[tid] = T;
+      s_mask[tid] = T ? pending_mask(T, 0u) : 0u;
+      s_rp[tid] = rp;
+      if (T) {
+        float x = __uint_as_float(ls.x);
+        const uint32_t Tc = T < 32u ? T : 32u;
+        for (uint32_t i = 0; i < Tc; ++i) {
+          x = x * d.ep;
+          s_tab[tid][i] = x;
+        }
+        d.lstart[j] = make_uint2(__float_as_uint(x), (uint32_t)k);
+        live = 1u;
+      }
+    }
+    if (tid == 0) s_beg[nrows] = __ldg(d.row_ptr + ja + nrows);
+    if (!__syncthreads_or(live)) continue;
+    // ---- phase 2: the task's positions, four per thread ----
+    const uint64_t pa = s_beg[0], pb_end = s_beg[nrows];
+    for (uint64_t e0 = (pa & ~3ull) + 4ull * tid; e0 < pb_end; e0 += 4ull * blockDim.x) {
+      // the row of the first position at or after pa in this group
+      const uint64_t ef = e0 < pa ? pa : e0;
+      uint32_t lo = 0, hi = nrows;      // largest t with s_beg[t] <= ef
+      while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (s_beg[mid] <= ef) lo = mid; else hi = mid;
+      }
+      const uint4 c4 = __ldg(reinterpret_cast<const uint4*>(d.col + e0));
+      const uint32_t cc[4] = {c4.x, c4.y, c4.z, c4.w};
+      uint32_t pb[4] = {0u, 0u, 0u, 0u};
+      uint32_t tq[4] = {0u, 0u, 0u, 0u};
+      uint32_t t = lo;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const uint64_t e = e0 + q;
+        if (e < pa || e >= pb_end) continue;
+        while (t + 1 < nrows && s_beg[t + 1] <= e) ++t;
+        tq[q] = t;
+        if (!s_T[t]) continue;
+        if (s_rp[t] != 1 && !__ldg(d.plastic + e)) continue;
+        pb[q] = __float_as_uint(rec_k[cc[q]].x) & s_mask[t];
+      }
+      if (!(pb[0] | pb[1] | pb[2] | pb[3])) continue;
+      float w[4];
+      load_w4(d, BF16, e0, w);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        uint32_t U = pb[q];
+        if (!U) continue;
+        const uint32_t T = s_T[tq[q]];
+        const float* xs = s_tab[tq[q]];
+        float y = w[q];
+        while (U) {
+          const uint32_t b = 31u - __clz(U);
+          y = clampw(y + d.neg_a_minus * xs[T - b - 1u], d.w_min, d.w_max);
+          if (BF16) y = bf16_bits_to_f32(f32_to_bf16_bits(y));
+          U &= ~(1u << b);
+        }
+        if (BF16) d.w16[e0 + q] = f32_to_bf16_bits(y);
+        else d.w32[e0 + q] = y;
+      }
+    }
+    __syncthreads();
+  }
 }
 
 // Deferred LTD: every row flushed to the last completed step (before the
