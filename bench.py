@@ -590,6 +590,7 @@ def run_batch_config(local, rank, world, dist, n_nets=256, cpu=True):
         eng.run(steps)
         ms, spikes, events = timed_run(eng, steps, stream)
         wlen, wtune = eng.window()
+        plan, (_, shape_us) = eng.window_plan(), eng.walk_shape()
         eng.close()
         if dist:
             t = torch.tensor([ms, float(spikes), float(events)], dtype=torch.float64,
@@ -612,7 +613,10 @@ def run_batch_config(local, rank, world, dist, n_nets=256, cpu=True):
                       "step_path_bytes_per_s": bytes_step * steps / (ms / 1e3),
                       "hbm_frac": bytes_step * steps / (ms / 1e3) / 1e9 / peak,
                       "window_steps": wlen,
-                      "window_tuner_us_per_step": wtune}
+                      "window_tuner_us_per_step": wtune,
+                      "window_plan": plan,
+                      "walk_shape_tuner_us_per_step": {f"{l} lanes x {b or 'max'} blocks/SM": t
+                                                       for (l, b), t in shape_us.items()}}
     if cpu and rank == 0 and world == 1:
         res["cpu_baseline"] = batch_cpu_sample(nets, seeds, cfg, variants)
         for label, _ in variants:

@@ -390,6 +390,26 @@ ns_status ns_get_schedule(ns_handle* h, uint32_t* schedule, double* us_per_step)
  * ns_config.window_steps is 0. */
 ns_status ns_get_window(ns_handle* h, uint32_t* window, uint32_t* candidates, double* us_per_step);
 
+/* Windowed stepping: the shape of the window's row walk, which the window
+ * tuner picks per network after the window length. lanes = lanes walking one
+ * spiking row (32, 16 or 8: a warp has 32/lanes rows in flight),
+ * blocks_per_sm = the walk's grid per SM. The candidates timed (lanes,
+ * blocks per SM with 0 = the occupancy limit) and their microseconds per
+ * step in cand_*[4] and us_per_step[4] (0 where untimed). Every shape gives
+ * the same results (integer accumulation). 0s when stepping is not
+ * windowed. No reference counterpart: the reference walks on the host. */
+ns_status ns_get_walk_shape(ns_handle* h, uint32_t* lanes, uint32_t* blocks_per_sm, uint32_t* cand_lanes,
+                            uint32_t* cand_blocks_per_sm, double* us_per_step);
+
+/* Fixes the windowed plan instead of tuning it: window length (2..1024,
+ * clamped to the configuration's window), lanes per row (8, 16, 32) and
+ * blocks per SM (0 = occupancy limit; larger values are clamped to it). The
+ * plan outlives re-uploads. All three 0 hands the choice back to the tuner,
+ * which runs at the next ns_step. For a host-side cache of tuned plans per
+ * network-size bucket. NS_ERR_STATE while a learned macro-step is
+ * attached. */
+ns_status ns_set_window_plan(ns_handle* h, uint32_t window, uint32_t lanes, uint32_t blocks_per_sm);
+
 /* Kernel launches issued by this handle since creation (own kernels only). */
 ns_status ns_launch_count(ns_handle* h, uint64_t* launches);
 

@@ -99,6 +99,8 @@ SIGNATURES = {
     "ns_set_drive": (C.c_int32, [_P, C.POINTER(NsDrive)]),
     "ns_upload_batch": (C.c_int32, [_P, C.c_uint32, C.POINTER(NsNetDesc), _P]),
     "ns_get_window": (C.c_int32, [_P, _P, _P, _P]),
+    "ns_get_walk_shape": (C.c_int32, [_P, _P, _P, _P, _P, _P]),
+    "ns_set_window_plan": (C.c_int32, [_P, C.c_uint32, C.c_uint32, C.c_uint32]),
     "ns_network_rates": (C.c_int32, [_P, C.c_uint64, C.c_uint32, _P]),
     # neuralsim_surrogate.h
     "ns_sur_create": (C.c_int32, [C.c_int32, _P, C.c_float, C.c_uint32, C.c_uint64, C.POINTER(_P)]),

@@ -29,7 +29,7 @@ class BatchEngine(SimulationEngine):
     """Steps `networks` (all of one neuron model, one SimConfig and one drive
     kind) together; network q draws its drive from seeds[q]."""
 
-    def __init__(self, networks, seeds, config: SimConfig, drive: Drive = None):
+    def __init__(self, networks, seeds, config: SimConfig, drive: Drive = None, plan_cache=None):
         self.networks = list(networks)
         self.seeds = [int(s) for s in seeds]
         if not self.networks or len(self.seeds) != len(self.networks):
@@ -37,7 +37,7 @@ class BatchEngine(SimulationEngine):
         if any(x.model != self.networks[0].model for x in self.networks):
             raise ValueError("all networks of a batch use one neuron model")
         self.first_neuron = None
-        super().__init__(_BatchShape(self.networks), config, drive)
+        super().__init__(_BatchShape(self.networks), config, drive, plan_cache=plan_cache)
 
     def _upload(self, _shape):
         nets = self.networks

@@ -50,6 +50,14 @@ struct ns_handle {
   uint32_t tune_w[4] = {0, 0, 0, 0};    // window candidates timed, and their us per step
   double tune_w_us[4] = {0, 0, 0, 0};
   int win_rows_blocks = 0;
+  // shape of the window row walk: lanes per row (32, 16, 8) and blocks per
+  // SM (win_bps, 0 = the occupancy limit); timed by the window tuner per
+  // network unless the host fixed a plan (ns_set_window_plan)
+  uint32_t win_lanes = 32, win_bps = 0;
+  bool plan_fixed = false;
+  uint32_t plan_w = 0;
+  uint32_t tune_lanes[4] = {0, 0, 0, 0}, tune_bps[4] = {0, 0, 0, 0};
+  double tune_shape_us[4] = {0, 0, 0, 0};
   std::map<uint64_t, cudaGraphExec_t> graphs;   // (window, steps, schedule)
   uint64_t launches = 0;
   int prop_blocks = 0;
@@ -896,11 +904,39 @@ window_fn pick_window(uint32_t model, uint32_t mode, bool stim) {
   return nullptr;
 }
 
-window_fn pick_window_rows(uint32_t mode, uint32_t wf) {
+window_fn pick_window_rows(uint32_t mode, uint32_t wf, uint32_t lanes = 32) {
   bool cond = mode == NS_INPUT_CONDUCTANCE_REF || mode == NS_INPUT_CONDUCTANCE_FRESH;
   bool bf = wf == NS_WEIGHT_BF16;
-  if (cond) return bf ? ns::k_window_rows<true, true> : ns::k_window_rows<true, false>;
-  return bf ? ns::k_window_rows<false, true> : ns::k_window_rows<false, false>;
+#define NSR(L) \
+  if (lanes == L) {                                                                          \
+    if (cond) return bf ? ns::k_window_rows<true, true, L> : ns::k_window_rows<true, false, L>; \
+    return bf ? ns::k_window_rows<false, true, L> : ns::k_window_rows<false, false, L>;        \
+  }
+  NSR(8) NSR(16) NSR(32)
+#undef NSR
+  return nullptr;
+}
+
+// Occupancy limit (blocks per SM) of the window row walk with `lanes` lanes
+// per row.
+int walk_occupancy(const ns_handle* h, uint32_t lanes) {
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &nb, pick_window_rows(h->cfg.input_mode, h->cfg.weight_format, lanes), 256, 0) != cudaSuccess ||
+      nb < 1) {
+    cudaGetLastError();
+    nb = 4;
+  }
+  return nb;
+}
+
+// Sets the walk's shape: lanes per row and blocks per SM (0 = occupancy
+// limit; larger values are clamped to it).
+void set_walk_shape(ns_handle* h, uint32_t lanes, uint32_t bps) {
+  const int occ = walk_occupancy(h, lanes);
+  h->win_lanes = lanes;
+  h->win_bps = (bps == 0 || (int)bps > occ) ? 0u : bps;
+  h->win_rows_blocks = h->sms * (h->win_bps ? (int)h->win_bps : occ);
 }
 
 // Window length the handle's configuration allows (0 = step-synchronous).
@@ -931,7 +967,7 @@ cudaError_t enqueue_window(ns_handle* h, uint32_t j0, uint32_t Wc, bool stim = f
   } else {
     pick_window(h->cfg.model, h->cfg.input_mode, stim)<<<nseg, ns::kWinThreads, 0, h->st>>>(h->d, j0, Wc);
   }
-  pick_window_rows(h->cfg.input_mode, h->cfg.weight_format)
+  pick_window_rows(h->cfg.input_mode, h->cfg.weight_format, h->win_lanes)
       <<<h->win_rows_blocks, 256, 0, h->st>>>(h->d, j0, Wc);
   // the segment offsets serve only the spike log
   if (h->d.log_idx) ns::k_window_scan<<<Wc, 256, 0, h->st>>>(h->d, Wc);
@@ -941,7 +977,10 @@ cudaError_t enqueue_window(ns_handle* h, uint32_t j0, uint32_t Wc, bool stim = f
 }
 
 ns_status get_graph(ns_handle* h, uint32_t S, uint32_t sched, cudaGraphExec_t* out) {
-  const uint64_t key = ((uint64_t)(h->win ? h->wcur : 0u) << 40) | ((uint64_t)S * 8u + sched);
+  // chunk length and schedule; window length and the walk's shape
+  const uint64_t shape = h->win ? ((uint64_t)h->wcur | (uint64_t)(h->win_lanes >> 3) << 11 |
+                                   (uint64_t)h->win_bps << 14) : 0ull;
+  const uint64_t key = (shape << 36) | ((uint64_t)S * 8u + sched);
   auto it = h->graphs.find(key);
   if (it != h->graphs.end()) { *out = it->second; return NS_OK; }
   cudaGraph_t g;
@@ -1110,6 +1149,7 @@ ns_status autotune_window(ns_handle* h, uint32_t budget, uint32_t* used) {
     return NS_OK;
   }
   if (h->next_tune_step != 0) return NS_OK;
+  if (h->plan_fixed) { h->next_tune_step = ~0ull; return NS_OK; }
   uint32_t cand[4] = {0, 0, 0, 0};
   int nc = 0;
   for (uint32_t w = h->win; w >= 2 && nc < 4; w = (w + 1) / 2) {
@@ -1118,7 +1158,7 @@ ns_status autotune_window(ns_handle* h, uint32_t budget, uint32_t* used) {
   }
   // every candidate replays a whole number of windows of the longest one
   const uint32_t T = std::max<uint32_t>(kTuneWindow / h->win, 1u) * h->win;
-  if (nc < 2 || budget < T) return NS_OK;
+  if (budget < T) return NS_OK;
   Snapshot sn;
   CK(snapshot_take(h, sn));
   h->win_ran = true;
@@ -1126,34 +1166,78 @@ ns_status autotune_window(ns_handle* h, uint32_t budget, uint32_t* used) {
   cudaError_t ce = cudaEventCreate(&e0);
   if (ce == cudaSuccess) ce = cudaEventCreate(&e1);
   if (ce != cudaSuccess) { snapshot_free(sn); return fail(h, NS_ERR_CUDA, cudaGetErrorString(ce)); }
-  double us[4] = {0, 0, 0, 0};
   ns_status r = NS_OK;
-  for (int q = 0; q < nc && r == NS_OK; ++q) {
-    if (q > 0 && (ce = snapshot_restore(h, sn)) != cudaSuccess) break;
-    h->wcur = cand[q];
+  bool first = true;
+  // one timed replay of the snapshot's T steps under the current plan
+  auto time_plan = [&](double* us) -> bool {
+    if (!first && (ce = snapshot_restore(h, sn)) != cudaSuccess) return false;
+    first = false;
     cudaGraphExec_t ex;
-    if ((r = get_graph(h, T, 1, &ex))) break;
+    if ((r = get_graph(h, T, 1, &ex))) return false;
     float ms = 0;
-    if ((ce = cudaEventRecord(e0, h->st)) != cudaSuccess) break;
-    if ((ce = cudaGraphLaunch(ex, h->st)) != cudaSuccess) break;
-    if ((ce = cudaEventRecord(e1, h->st)) != cudaSuccess) break;
-    if ((ce = cudaEventSynchronize(e1)) != cudaSuccess) break;
-    if ((ce = cudaEventElapsedTime(&ms, e0, e1)) != cudaSuccess) break;
-    us[q] = ms * 1e3 / T;
-    h->launches += ((T + cand[q] - 1) / cand[q]) * window_launches(h) + 1;
+    if ((ce = cudaEventRecord(e0, h->st)) != cudaSuccess) return false;
+    if ((ce = cudaGraphLaunch(ex, h->st)) != cudaSuccess) return false;
+    if ((ce = cudaEventRecord(e1, h->st)) != cudaSuccess) return false;
+    if ((ce = cudaEventSynchronize(e1)) != cudaSuccess) return false;
+    if ((ce = cudaEventElapsedTime(&ms, e0, e1)) != cudaSuccess) return false;
+    *us = ms * 1e3 / T;
+    h->launches += ((T + h->wcur - 1) / h->wcur) * window_launches(h) + 1;
+    return true;
+  };
+  // 1. the window length, with the default walk (32 lanes, full occupancy)
+  double us[4] = {0, 0, 0, 0};
+  set_walk_shape(h, 32, 0);
+  bool ok = true;
+  for (int q = 0; q < nc && ok; ++q) {
+    h->wcur = cand[q];
+    ok = time_plan(&us[q]);
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  snapshot_free(sn);
-  if (r) { h->wcur = h->win; return r; }
-  if (ce != cudaSuccess) { h->wcur = h->win; return fail(h, NS_ERR_CUDA, std::string("autotune: ") + cudaGetErrorString(ce)); }
   int best = 0;
-  for (int q = 0; q < nc; ++q) {
+  for (int q = 0; ok && q < nc; ++q) {
     h->tune_w[q] = cand[q];
     h->tune_w_us[q] = us[q];
     if (us[q] < us[best]) best = q;
   }
-  h->wcur = cand[best];
+  if (ok) h->wcur = cand[best];
+  // 2. the walk's shape at that length: 16 and 8 lanes per row, then half the
+  // occupancy limit with the faster lane count
+  uint32_t sl[4] = {32, 16, 8, 0}, sb[4] = {0, 0, 0, 0};
+  double su[4] = {ok ? us[best] : 0.0, 0, 0, 0};
+  int ns_ = 1;
+  for (int q = 1; q < 3 && ok; ++q) {
+    set_walk_shape(h, sl[q], 0);
+    ok = time_plan(&su[q]);
+    ns_ = q + 1;
+  }
+  int bs = 0;
+  for (int q = 1; ok && q < 3; ++q)
+    if (su[q] < su[bs]) bs = q;
+  if (ok) {
+    const int occ = walk_occupancy(h, sl[bs]);
+    if (occ >= 2) {
+      sl[3] = sl[bs];
+      sb[3] = (uint32_t)(occ / 2);
+      set_walk_shape(h, sl[3], sb[3]);
+      ok = time_plan(&su[3]);
+      ns_ = 4;
+      if (ok && su[3] < su[bs]) bs = 3;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  snapshot_free(sn);
+  if (!ok) {
+    h->wcur = h->win;
+    set_walk_shape(h, 32, 0);
+    if (r) return r;
+    return fail(h, NS_ERR_CUDA, std::string("autotune: ") + cudaGetErrorString(ce));
+  }
+  for (int q = 0; q < 4; ++q) {
+    h->tune_lanes[q] = q < ns_ ? sl[q] : 0u;
+    h->tune_bps[q] = q < ns_ ? sb[q] : 0u;
+    h->tune_shape_us[q] = q < ns_ ? su[q] : 0.0;
+  }
+  set_walk_shape(h, sl[bs], sb[bs]);
   h->next_tune_step = ~0ull;
   *used = T;
   return NS_OK;
@@ -1676,6 +1760,11 @@ static ns_status alloc_dynamic(ns_handle* h) {
   h->win = h->shard_world > 1 ? 0u : window_len(c);
   h->wcur = h->win;
   h->next_tune_step = 0;
+  if (h->win && h->plan_fixed) {
+    // a plan the host fixed (ns_set_window_plan) outlives re-uploads
+    h->wcur = std::min(std::max(h->plan_w, 2u), h->win);
+    h->next_tune_step = ~0ull;
+  }
   d.inbits = nullptr; d.seg_cnt = nullptr; d.seg_lst = nullptr; d.seg_off = nullptr;
   d.step_total = nullptr; d.nseg = 0; d.wmax = 0;
   if (h->win) {
@@ -1690,10 +1779,8 @@ static ns_status alloc_dynamic(ns_handle* h) {
     if (c.model == NS_MODEL_HH &&
         (st = dalloc(h, B, &h->hstep, h->n_pad)))
       return st;
-    int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pick_window_rows(c.input_mode, c.weight_format), 256, 0) != cudaSuccess || nb < 1) nb = 4;
-    h->win_rows_blocks = h->sms * nb;
-    cudaGetLastError();
+    if (!h->plan_fixed) set_walk_shape(h, 32, 0);
+    else set_walk_shape(h, h->win_lanes, h->win_bps);
   }
   // reset the control block: counters, log, tickets; reward and frame origin
   CK(cudaMemsetAsync(h->ctl, 0, sizeof(ns::Ctl), h->st));
@@ -3023,6 +3110,49 @@ ns_status ns_get_window(ns_handle* h, uint32_t* window, uint32_t* candidates, do
   for (int q = 0; q < 4; ++q) {
     if (candidates) candidates[q] = h->tune_w[q];
     if (us_per_step) us_per_step[q] = h->tune_w_us[q];
+  }
+  return NS_OK;
+}
+
+ns_status ns_set_window_plan(ns_handle* h, uint32_t window, uint32_t lanes, uint32_t blocks_per_sm) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  if (window == 0 && lanes == 0 && blocks_per_sm == 0) {
+    // back to the tuner: it runs again at the next step
+    h->plan_fixed = false;
+    h->plan_w = 0;
+    if (h->win) {
+      h->wcur = h->win;
+      set_walk_shape(h, 32, 0);
+      h->next_tune_step = 0;
+    }
+    return NS_OK;
+  }
+  if (lanes != 8 && lanes != 16 && lanes != 32)
+    return fail(h, NS_ERR_INVALID_ARG, "lanes per row must be 8, 16 or 32");
+  if (window < 2 || window > 1024) return fail(h, NS_ERR_INVALID_ARG, "window must be 2..1024 steps");
+  if (h->sur_on) return fail(h, NS_ERR_STATE, "the learned macro-step fixes the window");
+  h->plan_fixed = true;
+  h->plan_w = window;
+  if (h->win) {
+    h->wcur = std::min(window, h->win);
+    set_walk_shape(h, lanes, blocks_per_sm);
+    h->next_tune_step = ~0ull;
+  } else {
+    h->win_lanes = lanes;
+    h->win_bps = blocks_per_sm;
+  }
+  return NS_OK;
+}
+
+ns_status ns_get_walk_shape(ns_handle* h, uint32_t* lanes, uint32_t* blocks_per_sm, uint32_t* cand_lanes,
+                            uint32_t* cand_blocks_per_sm, double* us_per_step) {
+  if (!h) return NS_ERR_NULL_HANDLE;
+  if (lanes) *lanes = h->win ? h->win_lanes : 0u;
+  if (blocks_per_sm) *blocks_per_sm = h->win ? (uint32_t)(h->win_rows_blocks / std::max(h->sms, 1)) : 0u;
+  for (int q = 0; q < 4; ++q) {
+    if (cand_lanes) cand_lanes[q] = h->tune_lanes[q];
+    if (cand_blocks_per_sm) cand_blocks_per_sm[q] = h->tune_bps[q];
+    if (us_per_step) us_per_step[q] = h->tune_shape_us[q];
   }
   return NS_OK;
 }

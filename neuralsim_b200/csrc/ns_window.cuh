@@ -181,10 +181,17 @@ __global__ void __launch_bounds__(kWinThreads, window_min_blocks<MODEL>()) k_win
 }
 
 // One warp per non-empty (step, segment): row walks into slot (k + D) mod D.
-template <bool COND, bool BF16>
+// LANES lanes walk one row (4 entries per lane per chunk of 4 LANES), so a
+// warp has 32 / LANES of the segment's rows in flight: the walk's shape,
+// chosen per network-size bucket by the window tuner. Integer atomics make
+// the result independent of the shape.
+template <bool COND, bool BF16, int LANES = 32>
 __global__ void __launch_bounds__(256) k_window_rows(NsDev d, uint32_t j0, uint32_t W) {
+  static_assert(LANES == 8 || LANES == 16 || LANES == 32, "8, 16 or 32 lanes per row");
+  constexpr uint32_t kGroups = 32u / LANES;
   __shared__ unsigned long long s_ev;
   const int lane = threadIdx.x & 31;
+  const uint32_t grp = (uint32_t)lane / LANES, glane = (uint32_t)lane % LANES;
   if (threadIdx.x == 0) s_ev = 0ull;
   __syncthreads();
   const uint64_t k0 = d.ctl->step_base + j0;
@@ -200,14 +207,14 @@ __global__ void __launch_bounds__(256) k_window_rows(NsDev d, uint32_t j0, uint3
     const uint64_t k = k0 + s;
     const uint32_t slot = (uint32_t)((k + d.D) % d.D);
     const uint32_t* lst = d.seg_lst + (uint64_t)s * d.n_pad + (uint64_t)seg * kWinThreads;
-    for (uint32_t l = 0; l < c; ++l) {
+    for (uint32_t l = grp; l < c; l += kGroups) {
       const uint32_t j = __ldg(lst + l);
       const uint64_t beg = __ldg(d.row_ptr + j), end = __ldg(d.row_ptr + j + 1);
       const uint8_t rt = COND ? __ldg(d.row_type + j) : 0;
-      if (lane == 0) ev += end - beg;
+      if (glane == 0) ev += end - beg;
       const uint64_t rb = beg & ~3ull;
-      for (uint64_t b = rb; b < end; b += 128) {
-        const uint64_t e0 = b + 4ull * lane;
+      for (uint64_t b = rb; b < end; b += 4u * LANES) {
+        const uint64_t e0 = b + 4ull * glane;
         if (e0 >= end || e0 + 4 <= beg) continue;
         const uint4 c4 = __ldg(reinterpret_cast<const uint4*>(d.col + e0));
         float w[4];

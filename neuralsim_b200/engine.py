@@ -160,9 +160,11 @@ class SimulationEngine:
     like the Mutex-guarded reference engine, src/simulation/scheduler.rs:23)."""
 
     def __init__(self, network: Network, config: SimConfig = None, drive: Drive = None,
-                 shard=None):
+                 shard=None, plan_cache=None):
         """shard: (rank, world) for one rank of a sharded network (see
-        neuralsim_b200.shard.partition_network); None for a whole network."""
+        neuralsim_b200.shard.partition_network); None for a whole network.
+        plan_cache: a neuralsim_b200.tune.PlanCache (or its file's path)
+        holding windowed plans per network-size bucket (use_plan_cache)."""
         self.lib = A.load()
         self.config = config or SimConfig(model=network.model)
         if self.config.model != network.model:
@@ -182,6 +184,9 @@ class SimulationEngine:
             self.close()
             raise
         self._stats_total = {"spikes": 0, "output_spikes": 0, "events": 0}
+        self._plan_cache, self._plan_key, self._plan_done = None, None, True
+        if plan_cache is not None:
+            self.use_plan_cache(plan_cache)
 
     # -- uploads (init_gpu, engine.rs:181-252) --
     def _upload(self, net: Network):
@@ -221,6 +226,8 @@ class SimulationEngine:
     def run(self, n_steps: int) -> A.NsStepStats:
         out = A.NsStepStats()
         self._check(self.lib.ns_step(self._h, int(n_steps), C.byref(out)))
+        if not self._plan_done:
+            self._record_plan()
         self._stats_total["spikes"] += out.spikes
         self._stats_total["output_spikes"] += out.output_spikes
         self._stats_total["events"] += out.events
@@ -484,6 +491,64 @@ class SimulationEngine:
         us = np.zeros(4, np.float64)
         self._check(self.lib.ns_get_window(self._h, C.byref(w), _ptr(cand), _ptr(us)))
         return int(w.value), {int(c): float(t) for c, t in zip(cand, us) if c}
+
+    def walk_shape(self):
+        """(lanes per row, blocks per SM) of the window row walk in use, and
+        {(lanes, blocks per SM or 0 = occupancy limit): us per step} timed by
+        the window tuner."""
+        lanes, bps = C.c_uint32(), C.c_uint32()
+        cl = np.zeros(4, np.uint32)
+        cb = np.zeros(4, np.uint32)
+        us = np.zeros(4, np.float64)
+        self._check(self.lib.ns_get_walk_shape(self._h, C.byref(lanes), C.byref(bps), _ptr(cl),
+                                               _ptr(cb), _ptr(us)))
+        return (int(lanes.value), int(bps.value)), {(int(a), int(b)): float(t)
+                                                     for a, b, t in zip(cl, cb, us) if a}
+
+    def window_plan(self):
+        """The windowed plan in use: {"window", "lanes", "blocks_per_sm"}
+        (None when stepping is not windowed)."""
+        w, _ = self.window()
+        if not w:
+            return None
+        (lanes, bps), _ = self.walk_shape()
+        return {"window": w, "lanes": lanes, "blocks_per_sm": bps}
+
+    def use_plan_cache(self, cache):
+        """Windowed plans per network-size bucket (neuralsim_b200.tune): a
+        cached plan for this network's bucket is fixed at once (no tuning);
+        otherwise the plan the window tuner picks at the next step is stored
+        in the cache. Returns the cached plan or None."""
+        from . import tune
+        if not isinstance(cache, tune.PlanCache):
+            cache = tune.PlanCache(cache)
+        c = self.config
+        self._plan_cache = cache
+        self._plan_key = tune.bucket_key(c.model, c.input_mode, c.weight_format, c.delay_steps,
+                                         self.network.n, self.network.m)
+        plan = cache.get(self._plan_key)
+        if plan is not None:
+            self.set_window_plan(plan["window"], plan["lanes"], plan["blocks_per_sm"])
+        self._plan_done = plan is not None
+        return plan
+
+    def _record_plan(self):
+        w, tried = self.window()
+        if not w:
+            self._plan_done = True      # not windowed: nothing to cache
+            return
+        if not tried:
+            return                      # the tuner has not run yet
+        shape, shape_us = self.walk_shape()
+        plan = self.window_plan()
+        us = min(shape_us.values()) if shape_us else min(tried.values())
+        self._plan_cache.put(self._plan_key, plan, us)
+        self._plan_done = True
+
+    def set_window_plan(self, window, lanes, blocks_per_sm):
+        """Fixes the windowed plan (no tuning); (0, 0, 0) hands it back to
+        the window tuner."""
+        self._check(self.lib.ns_set_window_plan(self._h, int(window), int(lanes), int(blocks_per_sm)))
 
     def network_rates(self, first_step, n_steps):
         """Mean firing rate (Hz) of every network of the handle after the
