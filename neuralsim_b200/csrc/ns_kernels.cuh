@@ -1431,21 +1431,18 @@ __device__ __forceinline__ void flush_row(const NsDev& d, uint64_t k, const floa
 // (the rows of step k's spikers are skipped) and the neuron update of step
 // k+1; the row walks of step k+1 wait for it.
 //
-// A block takes tasks of kFlushRows consecutive rows. One round trip brings
-// the rows' metadata and CSR bounds (one thread per row). Then every thread
-// issues the loads of all its 4-position groups of the task at once (column
-// and weight together; groups whose rows have nothing pending load nothing)
-// and the gathers of their targets' spike bits, while the rows' threads
-// compute the pre-trace chain tables into shared memory and move the rows'
-// starts to step k. After one barrier the pending LTDs are applied. Only
-// changed weights are written, so a group at a task's edge or over a spiking
-// row touches nothing it does not own.
+// A block takes tasks of kFlushRows consecutive rows. First one thread per
+// row reads the row's metadata, computes its pre-trace chain table into
+// shared memory and moves its trace start to step k; then the block streams
+// the task's contiguous CSR range, four positions per thread (coalesced
+// column and weight loads), each position finding its row in the task's row
+// pointers, gathering its target's spike bits and applying the pending LTDs
+// with its row's table. Only changed weights are written, so a 4-entry group
+// at a task's edge or over a spiking row touches nothing it does not own.
 constexpr uint32_t kFlushRows = 32;
-constexpr uint32_t kFlushGroups = 4;   // 4-position groups per thread and pass
 
 template <bool BF16>
-__global__ void __launch_bounds__(256, 4) k_flush(NsDev d, uint32_t jstep) {
-  constexpr uint32_t G = kFlushGroups;
+__global__ void __launch_bounds__(256) k_flush(NsDev d, uint32_t jstep) {
   __shared__ float s_tab[kFlushRows][33];
   __shared__ uint64_t s_beg[kFlushRows + 1];
   __shared__ uint32_t s_T[kFlushRows], s_mask[kFlushRows];
@@ -1460,117 +1457,75 @@ __global__ void __launch_bounds__(256, 4) k_flush(NsDev d, uint32_t jstep) {
   for (uint64_t task = blockIdx.x; task < ntask; task += gridDim.x) {
     const uint64_t ja = r0 + task * kFlushRows;
     const uint32_t nrows = (uint32_t)(ja + kFlushRows <= r1 ? kFlushRows : r1 - ja);
-    // ---- the rows' metadata and CSR bounds, one thread per row ----
-    uint32_t T = 0u;
-    float ps = 0.0f;
-    if (tid <= nrows) s_beg[tid] = __ldg(d.row_ptr + ja + tid);
+    // ---- phase 1: one thread per row ----
+    uint32_t live = 0u;
     if (tid < nrows) {
       const uint64_t j = ja + tid;
       const uint8_t rp = __ldg(d.row_plastic + j);
       const uint32_t hj = __float_as_uint(rec_k[j].x);
       const uint2 ls = d.lstart[j];
-      T = (rp && !(hj & 1u)) ? (uint32_t)k - ls.y : 0u;
+      s_beg[tid] = __ldg(d.row_ptr + j);
+      uint32_t T = (rp && !(hj & 1u)) ? (uint32_t)k - ls.y : 0u;
       if (T > 32u) atomicOr(&d.ctl->status, kErrDeferWindow);
-      ps = __uint_as_float(ls.x);
       s_T[tid] = T;
       s_mask[tid] = T ? pending_mask(T, 0u) : 0u;
       s_rp[tid] = rp;
+      if (T) {
+        float x = __uint_as_float(ls.x);
+        const uint32_t Tc = T < 32u ? T : 32u;
+        for (uint32_t i = 0; i < Tc; ++i) {
+          x = x * d.ep;
+          s_tab[tid][i] = x;
+        }
+        d.lstart[j] = make_uint2(__float_as_uint(x), (uint32_t)k);
+        live = 1u;
+      }
     }
-    if (!__syncthreads_or(T != 0u)) continue;
-    const uint64_t pa = s_beg[0], pend = s_beg[nrows];
-    // passes of 4 G blockDim positions; the first one (which always runs)
-    // also writes the chain tables
-    bool tab = false;
-    for (uint64_t base = pa & ~3ull; base < pend || !tab; base += 4ull * G * blockDim.x) {
-      uint32_t t0[G], pb[G][4];
-      uint4 c4[G];
-      uint2 wh[G];      // BF16 weights
-      float4 wf[G];     // FP32 weights
-      uint32_t live = 0u;
-#pragma unroll
-      for (uint32_t g = 0; g < G; ++g) {
-        const uint64_t e0 = base + 4ull * (tid + blockDim.x * g);
-        t0[g] = 0u;
-        if (e0 >= pend) continue;
-        const uint64_t ef = e0 < pa ? pa : e0;
-        uint32_t lo = 0, hi = nrows;      // largest t with s_beg[t] <= ef
-        while (hi - lo > 1) {
-          const uint32_t mid = (lo + hi) >> 1;
-          if (s_beg[mid] <= ef) lo = mid; else hi = mid;
-        }
-        t0[g] = lo;
-        bool any = s_T[lo] != 0u;
-        for (uint32_t t = lo; t + 1 < nrows && s_beg[t + 1] <= e0 + 3; ++t) any |= s_T[t + 1] != 0u;
-        if (!any) continue;
-        live |= 1u << g;
-        c4[g] = __ldg(reinterpret_cast<const uint4*>(d.col + e0));
-        if (BF16) wh[g] = *reinterpret_cast<const uint2*>(d.w16 + e0);
-        else wf[g] = *reinterpret_cast<const float4*>(d.w32 + e0);
+    if (tid == 0) s_beg[nrows] = __ldg(d.row_ptr + ja + nrows);
+    if (!__syncthreads_or(live)) continue;
+    // ---- phase 2: the task's positions, four per thread ----
+    const uint64_t pa = s_beg[0], pb_end = s_beg[nrows];
+    for (uint64_t e0 = (pa & ~3ull) + 4ull * tid; e0 < pb_end; e0 += 4ull * blockDim.x) {
+      // the row of the first position at or after pa in this group
+      const uint64_t ef = e0 < pa ? pa : e0;
+      uint32_t lo = 0, hi = nrows;      // largest t with s_beg[t] <= ef
+      while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (s_beg[mid] <= ef) lo = mid; else hi = mid;
       }
-      // the targets' spike bits of the pending steps
+      const uint4 c4 = __ldg(reinterpret_cast<const uint4*>(d.col + e0));
+      const uint32_t cc[4] = {c4.x, c4.y, c4.z, c4.w};
+      uint32_t pb[4] = {0u, 0u, 0u, 0u};
+      uint32_t tq[4] = {0u, 0u, 0u, 0u};
+      uint32_t t = lo;
 #pragma unroll
-      for (uint32_t g = 0; g < G; ++g) {
-        const uint64_t e0 = base + 4ull * (tid + blockDim.x * g);
-        const uint32_t cc[4] = {c4[g].x, c4[g].y, c4[g].z, c4[g].w};
-        uint32_t t = t0[g];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          pb[g][q] = 0u;
-          const uint64_t e = e0 + q;
-          if (!((live >> g) & 1u) || e < pa || e >= pend) continue;
-          while (t + 1 < nrows && s_beg[t + 1] <= e) ++t;
-          if (!s_T[t]) continue;
-          if (s_rp[t] != 1 && !__ldg(d.plastic + e)) continue;
-          pb[g][q] = __float_as_uint(rec_k[cc[q]].x) & s_mask[t];
-        }
+      for (int q = 0; q < 4; ++q) {
+        const uint64_t e = e0 + q;
+        if (e < pa || e >= pb_end) continue;
+        while (t + 1 < nrows && s_beg[t + 1] <= e) ++t;
+        tq[q] = t;
+        if (!s_T[t]) continue;
+        if (s_rp[t] != 1 && !__ldg(d.plastic + e)) continue;
+        pb[q] = __float_as_uint(rec_k[cc[q]].x) & s_mask[t];
       }
-      if (!tab) {
-        // the chain tables and the rows' new starts, while the loads fly
-        tab = true;
-        if (T) {
-          const uint32_t j = (uint32_t)(ja + tid);
-          float x = ps;
-          const uint32_t Tc = T < 32u ? T : 32u;
-          for (uint32_t i = 0; i < Tc; ++i) {
-            x = x * d.ep;
-            s_tab[tid][i] = x;
-          }
-          d.lstart[j] = make_uint2(__float_as_uint(x), (uint32_t)k);
-        }
-        __syncthreads();
-      }
+      if (!(pb[0] | pb[1] | pb[2] | pb[3])) continue;
+      float w[4];
+      load_w4(d, BF16, e0, w);
 #pragma unroll
-      for (uint32_t g = 0; g < G; ++g) {
-        if (!(pb[g][0] | pb[g][1] | pb[g][2] | pb[g][3])) continue;
-        const uint64_t e0 = base + 4ull * (tid + blockDim.x * g);
-        float w[4];
-        if (BF16) {
-          w[0] = bf16_bits_to_f32((uint16_t)(wh[g].x & 0xffffu));
-          w[1] = bf16_bits_to_f32((uint16_t)(wh[g].x >> 16));
-          w[2] = bf16_bits_to_f32((uint16_t)(wh[g].y & 0xffffu));
-          w[3] = bf16_bits_to_f32((uint16_t)(wh[g].y >> 16));
-        } else {
-          w[0] = wf[g].x; w[1] = wf[g].y; w[2] = wf[g].z; w[3] = wf[g].w;
+      for (int q = 0; q < 4; ++q) {
+        uint32_t U = pb[q];
+        if (!U) continue;
+        const uint32_t T = s_T[tq[q]];
+        const float* xs = s_tab[tq[q]];
+        float y = w[q];
+        while (U) {
+          const uint32_t b = 31u - __clz(U);
+          y = clampw(y + d.neg_a_minus * xs[T - b - 1u], d.w_min, d.w_max);
+          if (BF16) y = bf16_bits_to_f32(f32_to_bf16_bits(y));
+          U &= ~(1u << b);
         }
-        uint32_t t = t0[g];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          uint32_t U = pb[g][q];
-          if (!U) continue;
-          const uint64_t e = e0 + q;
-          while (t + 1 < nrows && s_beg[t + 1] <= e) ++t;
-          const uint32_t Tr = s_T[t];
-          const float* xs = s_tab[t];
-          float y = w[q];
-          while (U) {
-            const uint32_t b = 31u - __clz(U);
-            y = clampw(y + d.neg_a_minus * xs[Tr - b - 1u], d.w_min, d.w_max);
-            if (BF16) y = bf16_bits_to_f32(f32_to_bf16_bits(y));
-            U &= ~(1u << b);
-          }
-          if (BF16) d.w16[e] = f32_to_bf16_bits(y);
-          else d.w32[e] = y;
-        }
+        if (BF16) d.w16[e0 + q] = f32_to_bf16_bits(y);
+        else d.w32[e0 + q] = y;
       }
     }
     __syncthreads();
