@@ -1007,7 +1007,7 @@ ns_status get_graph(ns_handle* h, uint32_t S, uint32_t sched, cudaGraphExec_t* o
     return fail(h, NS_ERR_CUDA, std::string("graph capture: ") +
                                     cudaGetErrorString(ce != cudaSuccess ? ce : ee));
   cudaGraphExec_t ex;
-  cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
+  cudaError_t e = cudaGraphInstantiateWithFlags(&ex, g, cudaGraphInstantiateFlagUseNodePriority);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return fail(h, NS_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
   h->graphs[key] = ex;
@@ -1388,11 +1388,17 @@ ns_status ns_create(const ns_config* cfg, ns_handle** out) {
   h->dev = c.device;
   h->sched = c.step_schedule;
   cudaError_t e = cudaSetDevice(h->dev);
-  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking);
-  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->st2, cudaStreamNonBlocking);
+  // the step's critical path (neuron update, row walks) on the highest
+  // priority, the flush and the next step's drive beside it on the lowest:
+  // the block scheduler hands freed SMs to the critical path first (graphs
+  // are instantiated with per-node priorities)
+  int pr_lo = 0, pr_hi = 0;
+  if (e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&pr_lo, &pr_hi);
+  if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&h->st, cudaStreamNonBlocking, pr_hi);
+  if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&h->st2, cudaStreamNonBlocking, pr_lo);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_rows, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_ltd, cudaEventDisableTiming);
-  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->st3, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&h->st3, cudaStreamNonBlocking, pr_lo);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_nrn, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_drv, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, h->dev);
