@@ -70,7 +70,6 @@ struct ns_handle {
   // deferred LTD (schedule 5): LTDs wait in the spike histories of the trace
   // records (pending); the rows' trace starts match the last step (synced)
   bool defer_pending = false, defer_synced = false;
-  int flush_blocks = 0;
   int homeo_blocks = 0;
   int ntypes_acc = 1;
   // batch of networks: per-neuron network ids, per-network seeds and bases
@@ -641,6 +640,13 @@ prop_fn pick_prop_defer(uint32_t mode, uint32_t wf) {
   return bf ? ns::k_rows<false, true, false, true> : ns::k_rows<false, false, false, true>;
 }
 
+// Grid of the row-block flush: one block per task of ns::kFlushRows rows of
+// the largest row block.
+unsigned flush_grid(const ns_handle* h) {
+  const uint64_t per = (h->n + 31) / 32;
+  return (unsigned)std::max<uint64_t>((per + ns::kFlushRows - 1) / ns::kFlushRows, 1);
+}
+
 ltd_fn pick_flush(uint32_t wf) {
   return wf == NS_WEIGHT_BF16 ? ns::k_flush<true> : ns::k_flush<false>;
 }
@@ -833,7 +839,7 @@ cudaError_t enqueue_step(ns_handle* h, uint32_t j, bool* ltd_pending, uint32_t s
     e = cudaEventRecord(h->ev_rows, h->st);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(h->st2, h->ev_rows, 0);
     if (e != cudaSuccess) return e;
-    pick_flush(h->cfg.weight_format)<<<h->flush_blocks, 256, 0, h->st2>>>(dd, j);
+    pick_flush(h->cfg.weight_format)<<<flush_grid(h), 256, 0, h->st2>>>(dd, j);
     e = cudaEventRecord(h->ev_ltd, h->st2);
     if (e != cudaSuccess) return e;
     *ltd_pending = true;
@@ -1424,9 +1430,6 @@ ns_status ns_create(const ns_config* cfg, ns_handle** out) {
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pick_ltd(c.weight_format, ext), 256, 0) != cudaSuccess || nb < 1) nb = 4;
     h->ltd_blocks = h->sms * nb;
     h->ltd_narrow_blocks = h->sms * 2;
-    nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pick_flush(c.weight_format), 256, 0) != cudaSuccess || nb < 1) nb = 4;
-    h->flush_blocks = h->sms * nb;
     h->drive_blocks = h->sms * 4;
     // the neuron kernels may stage two sub-tile buffers in shared memory
     for (uint32_t mo = 0; mo < 3; ++mo)
@@ -2782,7 +2785,7 @@ ns_status ns_profile_steps(ns_handle* h, uint32_t n_steps, double* kernel_ms, ui
   prop_fn pf = dfr ? pick_prop_defer(h->cfg.input_mode, h->cfg.weight_format)
                    : pick_prop(h->cfg.input_mode, h->cfg.weight_format, ext);
   ltd_fn lf = dfr ? pick_flush(h->cfg.weight_format) : pick_ltd(h->cfg.weight_format, ext);
-  const int lblocks = dfr ? h->flush_blocks : h->ltd_blocks;
+  const int lblocks = dfr ? (int)flush_grid(h) : h->ltd_blocks;
   // kernels in order neuron, rows, ltd (+ the R-STDP / consolidation tail),
   // homeostasis, drive; serial, one event pair each
   const bool on[5] = {true, true, h->cfg.stdp_enabled != 0 || tail_on(h), homeo_or_rates(h), pre};

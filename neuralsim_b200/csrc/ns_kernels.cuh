@@ -1431,6 +1431,8 @@ __device__ __forceinline__ void flush_row(const NsDev& d, uint64_t k, const floa
 // (the rows of step k's spikers are skipped) and the neuron update of step
 // k+1; the row walks of step k+1 wait for it.
 //
+// The grid is one block per task (flush_grid): short-lived blocks let the
+// higher-priority neuron update and row walks take SMs as they free up.
 // A block takes tasks of kFlushRows consecutive rows. First one thread per
 // row reads the row's metadata, computes its pre-trace chain table into
 // shared memory and moves its trace start to step k; then the block streams
@@ -1439,7 +1441,7 @@ __device__ __forceinline__ void flush_row(const NsDev& d, uint64_t k, const floa
 // pointers, gathering its target's spike bits and applying the pending LTDs
 // with its row's table. Only changed weights are written, so a 4-entry group
 // at a task's edge or over a spiking row touches nothing it does not own.
-constexpr uint32_t kFlushRows = 32;
+constexpr uint32_t kFlushRows = 16;
 
 template <bool BF16>
 __global__ void __launch_bounds__(256) k_flush(NsDev d, uint32_t jstep) {
