@@ -35,7 +35,6 @@ struct ns_handle {
   cudaStream_t st3 = nullptr;       // drive of step k+1 beside the walks of step k
   cudaEvent_t ev_rows = nullptr, ev_ltd = nullptr;
   cudaEvent_t ev_nrn = nullptr, ev_drv = nullptr;
-  int drive_blocks = 0;
   std::string err;
   bool have_neurons = false, have_csr = false;
   uint64_t n = 0, n_pad = 0, m = 0, m_pad = 0;
@@ -640,6 +639,12 @@ prop_fn pick_prop_defer(uint32_t mode, uint32_t wf) {
   return bf ? ns::k_rows<false, true, false, true> : ns::k_rows<false, false, false, true>;
 }
 
+// Grid of the drive kernel: one neuron pair per thread, so that its blocks,
+// on the low-priority stream, are short-lived.
+unsigned drive_grid(const ns_handle* h) {
+  return (unsigned)std::max<uint64_t>((h->n_pad / 2 + 255) / 256, 1);
+}
+
 // Grid of the row-block flush: one block per task of ns::kFlushRows rows of
 // the largest row block.
 unsigned flush_grid(const ns_handle* h) {
@@ -786,7 +791,7 @@ bool precompute_drive(const ns_handle* h) {
 NsDev with_drive(ns_handle* h, const NsDev& d, uint32_t j) {
   NsDev dd = d;
   if (precompute_drive(h)) {
-    ns::k_drive<<<h->drive_blocks, 256, 0, h->st>>>(dd, j);
+    ns::k_drive<<<drive_grid(h), 256, 0, h->st>>>(dd, j);
     h->launches += 1;
   }
   return dd;
@@ -820,7 +825,7 @@ cudaError_t enqueue_step(ns_handle* h, uint32_t j, bool* ltd_pending, uint32_t s
     cudaError_t r = cudaEventRecord(h->ev_nrn, h->st);
     if (r == cudaSuccess) r = cudaStreamWaitEvent(h->st3, h->ev_nrn, 0);
     if (r != cudaSuccess) return r;
-    ns::k_drive<<<h->drive_blocks, 256, 0, h->st3>>>(x, j + 1);
+    ns::k_drive<<<drive_grid(h), 256, 0, h->st3>>>(x, j + 1);
     r = cudaEventRecord(h->ev_drv, h->st3);
     if (r == cudaSuccess) *drv_pending = true;
     return r;
@@ -1001,7 +1006,7 @@ ns_status get_graph(ns_handle* h, uint32_t S, uint32_t sched, cudaGraphExec_t* o
     // next one beside its walks
     const bool pre = precompute_drive(h);
     bool dpend = false;
-    if (pre) ns::k_drive<<<h->drive_blocks, 256, 0, h->st>>>(h->d, 0);
+    if (pre) ns::k_drive<<<drive_grid(h), 256, 0, h->st>>>(h->d, 0);
     for (uint32_t j = 0; j < S && ce == cudaSuccess; ++j)
       ce = enqueue_step(h, j, &pending, sched, false,
                         !pre ? kDriveEager : (j + 1 < S ? kDriveNext : kDriveLast), &dpend);
@@ -1430,7 +1435,6 @@ ns_status ns_create(const ns_config* cfg, ns_handle** out) {
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pick_ltd(c.weight_format, ext), 256, 0) != cudaSuccess || nb < 1) nb = 4;
     h->ltd_blocks = h->sms * nb;
     h->ltd_narrow_blocks = h->sms * 2;
-    h->drive_blocks = h->sms * 4;
     // the neuron kernels may stage two sub-tile buffers in shared memory
     for (uint32_t mo = 0; mo < 3; ++mo)
       for (uint32_t md = 0; md < 5; ++md)
@@ -2794,7 +2798,7 @@ ns_status ns_profile_steps(ns_handle* h, uint32_t n_steps, double* kernel_ms, ui
   for (uint32_t j = 0; j < n_steps; ++j) {
     cudaEvent_t* e = &ev[(size_t)j * 10];
     CK(cudaEventRecord(e[8], h->st));
-    if (pre) ns::k_drive<<<h->drive_blocks, 256, 0, h->st>>>(dd, j);
+    if (pre) ns::k_drive<<<drive_grid(h), 256, 0, h->st>>>(dd, j);
     CK(cudaEventRecord(e[9], h->st));
     CK(cudaEventRecord(e[0], h->st));
     launch_neuron_kernel(h, j == 0 ? nf0 : nf, dd, j, h->st);
