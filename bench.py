@@ -756,17 +756,20 @@ def run_e2e(a, net, cfg, drive, local, dist):
            pnet.inhibitory.nbytes)
     eng = SimulationEngine(pnet, cfg, drive)   # allocations done once
     stream = torch.cuda.ExternalStream(eng.stream(), device=local)
-    times, events, d2h = [], [], []
+    times, events, d2h, parts = [], [], [], []
     raster_buf = None   # pinned, sized after the warm-up job
     for job in range(a.e2e_jobs + 1):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        eu, er = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
         e0.record(stream)
         eng._upload(pnet)
+        eu.record(stream)
         c0 = eng.counters()
         eng.run(job_steps)
+        er.record(stream)
         c1 = eng.counters()
         idx, off = eng.read_raster(c0[0], job_steps, out=raster_buf)
         st = eng.download_state(with_weights=False)
@@ -777,6 +780,7 @@ def run_e2e(a, net, cfg, drive, local, dist):
             raster_buf = pin(np.zeros(2 * max(int(idx.size), 1), np.uint32))
             continue
         times.append(e0.elapsed_time(e1))
+        parts.append([e0.elapsed_time(eu), eu.elapsed_time(er), er.elapsed_time(e1)])
         events.append(c1[3] - c0[3])
         d2h.append(idx.nbytes + off.nbytes + st["v"].nbytes)
     eng.close()
@@ -793,7 +797,8 @@ def run_e2e(a, net, cfg, drive, local, dist):
             "d2h_bytes_per_step": int(statistics.mean(d2h)),
             "step": "one job: upload network + initial state, 10,000 simulation steps, "
                     "read back raster + final v", "jobs": len(times),
-            "ms_per_job": ms / max(len(times), 1)}
+            "ms_per_job": ms / max(len(times), 1),
+            "ms_upload_run_readback_per_job": [[round(x, 2) for x in p] for p in parts]}
 
 
 def run_cpu_baseline(net, cfg, drive, seconds, warm=None, events_per_step=None):
