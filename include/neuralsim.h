@@ -299,7 +299,10 @@ ns_status ns_clear_spike_log(ns_handle* h);
 ns_status ns_spike_log_range(ns_handle* h, uint64_t* first_step, uint64_t* n_steps);
 
 /* --- state: checkpoint / resume (io/checkpoint.rs keeps the Network only;
- *     here the device state round-trips exactly, step counter included) --- */
+ *     here the device state round-trips exactly, step counter included) ---
+ * ns_download_state copies the fields of `out` that are not NULL; with w_out
+ * not NULL it first applies every pending deferred LTD (schedule 5), which
+ * the neuron state does not depend on. */
 ns_status ns_download_state(ns_handle* h, ns_neuron_soa* out, float* w_out);
 ns_status ns_upload_state(ns_handle* h, const ns_neuron_soa* in, const float* w_in,
                           uint64_t step);

@@ -2310,7 +2310,9 @@ ns_status ns_download_state(ns_handle* h, ns_neuron_soa* o, float* w_out) {
   ns_status r = ready(h);
   if (r) return r;
   CK(cudaSetDevice(h->dev));
-  if ((r = defer_settle(h))) return r;
+  // pending deferred LTDs change weights only: a read of the neuron state
+  // alone leaves them pending
+  if (w_out && (r = defer_settle(h))) return r;
   CK(cudaStreamSynchronize(h->st));
   const uint64_t n = h->n;
   NsDev& d = h->d;

@@ -313,7 +313,9 @@ class SimulationEngine:
         self._check(self.lib.ns_clear_spike_log(self._h))
 
     # -- state --
-    def download_state(self, with_weights=True):
+    def download_state(self, with_weights=True, fields=None):
+        """The neuron state (and the weights): every field of ns_neuron_soa,
+        or only those named in `fields` (e.g. ("v",))."""
         n = self.network.n
         ppn = PARAMS_PER_NEURON[self.config.model]
         cond = self.config.input_mode in (A.INPUT_CONDUCTANCE_REF, A.INPUT_CONDUCTANCE_FRESH)
@@ -329,6 +331,11 @@ class SimulationEngine:
             "pending_input": np.zeros(ntypes * self.config.delay_steps * n, np.int64),
             "conductance": np.zeros(4 * n, np.float32), "firing_rate": np.zeros(n, np.float64),
         }
+        if fields is not None:
+            unknown = set(fields) - set(st)
+            if unknown:
+                raise ValueError(f"unknown state fields {sorted(unknown)}")
+            st = {k: v for k, v in st.items() if k in fields}
         soa = A.NsNeuronSoa()
         for name, arr in st.items():
             setattr(soa, name, _ptr(arr))

@@ -166,3 +166,23 @@ def test_deferred_schedule_falls_back_where_it_does_not_apply(lib):
     o.step(100)
     assert nets.rasters_equal(eng.read_raster(0, 100), o.raster())
     assert np.allclose(eng.download_state()["w"], o.weights(), rtol=1e-5, atol=1e-6)
+
+
+def test_state_read_without_weights_leaves_ltds_pending(lib):
+    # a read of the neuron state alone does not flush the pending LTDs; the
+    # state it returns and everything after it equal the oracle
+    net, cfg, drive = nets.izh_stdp(n=12_000, k=80)
+    eng = _engine(net, cfg, drive)
+    o = FastOracle(net, cfg, drive, precision=32)
+    eng.run(45)
+    o.step(45)
+    st = eng.download_state(with_weights=False, fields=("v", "u", "pre_trace", "post_trace"))
+    so = o.state()
+    for k, ok in (("v", "v"), ("u", "u"), ("pre_trace", "pre"), ("post_trace", "post")):
+        assert np.array_equal(st[k].astype(np.float64), so[ok]), k
+    assert set(st) == {"v", "u", "pre_trace", "post_trace"}
+    eng.run(45)
+    o.step(45)
+    assert np.array_equal(eng.download_state()["w"].astype(np.float64), o.weights())
+    assert nets.rasters_equal(eng.read_raster(0, 90), o.raster())
+
